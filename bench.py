@@ -1,0 +1,320 @@
+"""Benchmark: RK3 steps/s of the channel at 192x129x192 (FP64) on B200.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                [--poisson fp64|mixed] [--no-cpu-baseline]
+
+A step is one compute_time_step_RK3 of the 192x129x192 Re_tau=180 channel
+(nx_global=194, ny_global=129, nz_global=194; Lx=4pi, Lz=4pi/3, tanh y grid
+with stretching 2.0, nu=1/5600, dt=1e-3, constant mass flow) from the seeded
+laminar+perturbation state.  The working set (~0.5 GB of FP64 fields) is
+larger than L2, so no flush is needed between steps.
+
+value : steps/s from CUDA events on the library's stream around K steps
+        (fields resident in HBM), max over ranks, summed over ranks (replicas).
+e2e   : the same metric through the C-ABI with host buffers: every step
+        uploads U, V, W from pinned host memory, advances one step and
+        downloads U, V, W.
+--impl reference: the CPU restatement of the reference algorithm (oracle
+        port) on this host's cores, one full RK3 step of the same workload
+        per timed step.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 194, 129, 194
+LX, LZ = 4.0 * math.pi, 4.0 * math.pi / 3.0
+NU = 1.0 / 5600.0
+DT = 1e-3
+WORKLOAD = "channel Re_tau=180 192x129x192 (nx_global=194, ny_global=129, nz_global=194), RK3, dt=1e-3"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        return d["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_channel(poisson):
+    import channel3d_parallel_b200 as c3d
+    ch = c3d.Channel(nx_global=NX, ny_global=NY, nz_global=NZ, Lxp=LX, Lzp=LZ, nu=NU,
+                     CFL=-DT, x_mass_cte=1, grid_type=1, alpha_stretch=2.0, dPdx=3.0 * NU)
+    if poisson == "mixed":
+        ch.set_mode(poisson=c3d.lib.POISSON_MIXED)
+    c3d.seeded_initial_state(ch, 3.0 * NU, NU)
+    return ch
+
+
+def cpu_baseline_sample(nsteps=1):
+    """Oracle port (FP64 NumPy/SciPy) on the host: seconds per RK3 step."""
+    import numpy as np  # noqa: F401
+    from oracle import channel_oracle as co
+    p = co.channel_params(NX, NY, NZ, LX, LZ, NU)
+    g = co.Grid(p)
+    st = co.seeded_initial_state(g, p["dpdx"])
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        co.compute_time_step_RK3(g, st, DT)
+    return (time.perf_counter() - t0) / nsteps
+
+
+def cores_used():
+    try:
+        import threadpoolctl
+        info = threadpoolctl.threadpool_info()
+        n = max([i.get("num_threads", 1) for i in info] or [1])
+        return int(n)
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        pass   # the CPU port has no warm-up state; every step is a full step
+    from oracle import channel_oracle as co
+    p = co.channel_params(NX, NY, NZ, LX, LZ, NU)
+    g = co.Grid(p)
+    st = co.seeded_initial_state(g, p["dpdx"])
+    co.compute_time_step_RK3(g, st, DT)           # one untimed step
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        co.compute_time_step_RK3(g, st, DT)
+    sec = (time.perf_counter() - t0) / args.steps
+    val = 1.0 / sec
+    line = {
+        "impl": "reference", "metric": "RK3 steps/s at 192x129x192 (FP64)", "value": val,
+        "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": [NX, NY, NZ], "poisson": "fp64",
+                   "l2": "working set > L2"},
+        "cpu_baseline": {"value": val, "unit": "steps/s", "cores": cores_used(), "kind": "port",
+                         "sample": f"{args.steps} full RK3 steps of the workload on the CPU restatement"},
+        "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    ch = make_channel(args.poisson)
+    dims = ch.dims
+    # warm-up (also captures the step graph)
+    ch.compute_time_step_RK3(args.warmup)
+    ch.synchronize()
+    l0 = ch.kernel_launches()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
+    ch.compute_time_step_RK3(args.steps)     # CUDA events inside the library
+    ms_step = ch.last_step_time_ms()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = ch.kernel_launches() - l0
+    if pg:
+        t = torch.tensor([ms_step], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_step = float(t.item())
+        pg.barrier()
+    value = ws / (ms_step * 1e-3)
+    div = ch.check_divergence()
+
+    # ---- per-kernel device times (roofline of the dominant kernel)
+    prof = ch.profile_kernels(nrep=10)
+    N = (NX - 2) * (NY - 1) * (NZ - 2)
+    bytes_per_cell = {"rhs_stage": 72.0, "grad_sub": 8.0 * 7, "div_xfft": 8.0 * 3 + 8.0 * 97 / 96,
+                      "xfft_inv": 8.0 * 97 / 96 + 8.0, "zfft_fwd": 16.0 * 97 / 96,
+                      "zfft_inv": 16.0 * 97 / 96, "tridiag": 16.0 * 97 / 96 * 2}
+    # time share per step: rhs, ghosts, spectral parts, grad_sub run 3x per step
+    dom = max(("rhs_stage", "grad_sub", "div_xfft", "xfft_inv"), key=lambda k: prof[k])
+    alg = bytes_per_cell[dom] * N
+    peak, peak_kind = measured_peaks()
+    achieved = alg / (prof[dom] * 1e-3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get(dom)
+        except Exception:
+            traffic = None
+
+    # ---- end to end through the C-ABI with pinned host buffers
+    pin = {}
+    for name in ("U", "V", "W"):
+        a = ch.download(name)
+        t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+        t.numpy()[:] = a.reshape(-1, order="F")
+        pin[name] = (t, t.numpy().reshape(a.shape, order="F"))
+    nbytes = sum(v[1].nbytes for v in pin.values())
+    e2e_steps = max(3, min(args.steps, 20))
+    for _ in range(2):
+        for name in ("U", "V", "W"):
+            ch.upload(name, pin[name][1])
+        ch.compute_time_step_RK3(1)
+        for name in ("U", "V", "W"):
+            ch.download(name)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for name in ("U", "V", "W"):
+            ch.upload(name, pin[name][1])
+        ch.compute_time_step_RK3(1)
+        for name in ("U", "V", "W"):
+            out = pin[name][1]
+            lb, ub = ch.bounds(name)
+            import ctypes
+            from channel3d_parallel_b200 import lib as L
+            cl, cu = L.box(lb, ub)
+            L.check(ch._lib.c3d_download(ch.handle, L.FIELD[name], L.dptr(out), cl, cu), ch.handle)
+    e2e_sec = (time.perf_counter() - t0) / e2e_steps
+    if pg:
+        t = torch.tensor([e2e_sec], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_sec = float(t.item())
+    e2e_val = ws / e2e_sec
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        sec = cpu_baseline_sample(1)
+        cpu = {"value": 1.0 / sec, "unit": "steps/s", "cores": cores_used(), "kind": "port",
+               "sample": "1 full RK3 step of the workload on the CPU restatement (NumPy/SciPy FP64)"}
+    ch.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": "RK3 steps/s at 192x129x192 (FP64)" if args.poisson == "fp64"
+        else "RK3 steps/s at 192x129x192 (mixed-precision Poisson)",
+        "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.poisson == "fp64" else "f64+f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": [NX, NY, NZ], "cells": N, "poisson": args.poisson,
+                   "parallelism": f"replicas x{ws}", "l2": "working set > L2 (no flush)"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "alg_bytes_per_launch": alg,
+                     "kernel_ms": prof[dom]},
+        "kernel_ms": prof,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_val, "unit": "steps/s", "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nbytes},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "max_div": div,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--poisson", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        if args.steps > 20:
+            args.steps = 10     # each CPU step is a full RK3 step (seconds)
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,267 @@
+// Constant-mass-flow correction and device reductions.
+//
+// compute_dPx_for_constant_mass_flow (src/mass_flow.f90:144-175) and its use
+// at the end of compute_time_step_RK3 (src/time_integration.f90:187-193):
+//   Int_U = sum_{k=2}^{nzg-1} sum_{j=3}^{nyg-1} sum_{i=2}^{nx-1}
+//              (Hu(j) U(j) + Hu(j-1) U(j-1)) * 0.5*(yg(j)-yg(j-1))
+//   norm  = same with U = 1
+//   shift = Qflow_x_0 - Int_U/norm;  U(interior) += shift;  BC;
+//   dPdx  = 0.5*(dPdx_prev + shift/dt).
+// The z range includes plane nzg-1, the periodic duplicate of plane 2, exactly
+// as the reference's last rank does.  Reductions are deterministic: a fixed
+// grid writes per-block partials that one block sums in a fixed order.
+#include "c3d_internal.cuh"
+
+namespace c3d {
+
+static const int kRedBlocks = 148 * 4;
+static const int kRedThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double2 block_sum2(double2 v) {
+  __shared__ double sx[32], sy[32];
+  v.x = warp_sum(v.x);
+  v.y = warp_sum(v.y);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { sx[wid] = v.x; sy[wid] = v.y; }
+  __syncthreads();
+  double2 r = make_double2(0.0, 0.0);
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    r.x = lane < nw ? sx[lane] : 0.0;
+    r.y = lane < nw ? sy[lane] : 0.0;
+    r.x = warp_sum(r.x);
+    r.y = warp_sum(r.y);
+  }
+  __syncthreads();
+  return r;
+}
+
+// partial sums of (Int_U, norm); Hu may be null (H = 1)
+__global__ void __launch_bounds__(kRedThreads) k_massflow_partial(Dims d, Metric m,
+                                                                 const double* __restrict__ U,
+                                                                 const double* __restrict__ Hu,
+                                                                 double2* __restrict__ part) {
+  const int ni = d.Nx, nj = d.nyg - 3, nk = d.Nz + 1;   // i 2..nx-1, j 3..nyg-1, k 2..nzg-1
+  const int64_t tot = (int64_t)ni * nj * nk;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = 2 + (int)(t % ni);
+    const int j = 3 + (int)((t / ni) % nj);
+    const int k = 2 + (int)(t / ((int64_t)ni * nj));
+    const double w = m.wq[j];
+    const int64_t a = idxU(d, i, j, k), b = idxU(d, i, j - 1, k);
+    if (Hu) {
+      const double ha = Hu[a], hb = Hu[b];
+      acc.x += (ha * U[a] + hb * U[b]) * w;
+      acc.y += (ha + hb) * w;
+    } else {
+      acc.x += (U[a] + U[b]) * w;
+      acc.y += 2.0 * w;
+    }
+  }
+  double2 s = block_sum2(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// final sum; mode 0: qflow only; mode 1: constant-flux correction update
+__global__ void k_massflow_final(const double2* __restrict__ part, int np, DevScalars* sc,
+                                 double q0, double dt, int mode) {
+  double2 acc = make_double2(0.0, 0.0);
+  for (int t = threadIdx.x; t < np; t += blockDim.x) {
+    acc.x += part[t].x;
+    acc.y += part[t].y;
+  }
+  double2 s = block_sum2(acc);
+  if (threadIdx.x == 0) {
+    const double q = s.x / s.y;
+    sc->qflow = q;
+    if (mode == 1) {
+      const double shift = q0 - s.x / s.y;
+      sc->shift = shift;
+      sc->dpdx_prev = sc->dPdx;
+      sc->dPdx = 0.5 * (sc->dpdx_prev + shift / dt);
+    }
+  }
+}
+
+// U(2:nx-1,2:nyg-1,2:nzg-1) += shift followed by the boundary conditions is,
+// entry for entry, U += shift on every copy of an interior value and
+// U -= shift on the odd y ghosts.
+__global__ void k_shift_u(Dims d, double* __restrict__ U, const DevScalars* sc) {
+  const double s = sc->shift;
+  const int64_t tot = (int64_t)d.nx * d.nyg * d.nzg;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int j = 1 + (int)((t / d.nx) % d.nyg);
+    U[t] = (j == 1 || j == d.nyg) ? U[t] - s : U[t] + s;
+  }
+}
+
+int launch_massflow_correction(Handle* h, double dt) {
+  k_massflow_partial<<<kRedBlocks, kRedThreads, 0, h->stream>>>(h->d, h->m, h->U, nullptr,
+                                                                (double2*)h->red);
+  C3D_LAUNCH_CHECK(h);
+  k_massflow_final<<<1, 1024, 0, h->stream>>>((const double2*)h->red, kRedBlocks, h->sc,
+                                              h->Qflow_x_0, dt, 1);
+  C3D_LAUNCH_CHECK(h);
+  k_shift_u<<<148 * 8, 256, 0, h->stream>>>(h->d, h->U, h->sc);
+  C3D_LAUNCH_CHECK(h);
+  return 0;
+}
+
+int massflow_u(Handle* h, const double* U, const double* Hu, double* q_out) {
+  k_massflow_partial<<<kRedBlocks, kRedThreads, 0, h->stream>>>(h->d, h->m, U, Hu, (double2*)h->red);
+  C3D_LAUNCH_CHECK(h);
+  k_massflow_final<<<1, 1024, 0, h->stream>>>((const double2*)h->red, kRedBlocks, h->sc, 0.0, 1.0, 0);
+  C3D_LAUNCH_CHECK(h);
+  double q = 0;
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(&q, &h->sc->qflow, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  *q_out = q;
+  return 0;
+}
+
+// ---- max |div u| over cells (i,j,k) in 2..nxg-1 x 2..nyg-1 x 2..nzg-1 ----
+__global__ void __launch_bounds__(kRedThreads) k_maxdiv(Dims d, Metric m, const double* __restrict__ U,
+                                                       const double* __restrict__ V,
+                                                       const double* __restrict__ W,
+                                                       double* __restrict__ part) {
+  const int ni = d.nxg - 2, nj = d.nyg - 2, nk = d.nzg - 2;
+  const int64_t tot = (int64_t)ni * nj * nk;
+  double mx = 0.0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = 2 + (int)(t % ni);
+    const int j = 2 + (int)((t / ni) % nj);
+    const int k = 2 + (int)(t / ((int64_t)ni * nj));
+    const double v = (U[idxU(d, i, j, k)] - U[idxU(d, i - 1, j, k)]) * m.rdx[i]
+                   + (V[idxV(d, i, j, k)] - V[idxV(d, i, j - 1, k)]) * m.rdy[j]
+                   + (W[idxW(d, i, j, k)] - W[idxW(d, i, j, k - 1)]) * m.rdz[k];
+    mx = fmax(mx, fabs(v));
+  }
+  __shared__ double sm[kRedThreads];
+  sm[threadIdx.x] = mx;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sm[0];
+}
+
+int max_abs_divergence(Handle* h, const double* U, const double* V, const double* W, double* out) {
+  k_maxdiv<<<kRedBlocks, kRedThreads, 0, h->stream>>>(h->d, h->m, U, V, W, h->red);
+  C3D_LAUNCH_CHECK(h);
+  std::vector<double> part(kRedBlocks);
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(part.data(), h->red, sizeof(double) * kRedBlocks,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  double mx = 0.0;
+  for (double v : part) mx = v > mx ? v : mx;
+  *out = mx;
+  return 0;
+}
+
+// ---- finiteness scan of U, V, W ----
+__global__ void k_finite(const double* __restrict__ a, int64_t n, int* flag) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    if (!isfinite(a[t])) { *flag = 1; return; }
+  }
+}
+
+int check_finite(Handle* h, bool* ok) {
+  int* flag = (int*)(h->red + 2 * kRedBlocks + 8);
+  C3D_CUDA_TRY(h, cudaMemsetAsync(flag, 0, sizeof(int), h->stream));
+  k_finite<<<148 * 4, 256, 0, h->stream>>>(h->U, sizeU(h->d), flag);
+  C3D_LAUNCH_CHECK(h);
+  k_finite<<<148 * 4, 256, 0, h->stream>>>(h->V, sizeV(h->d), flag);
+  C3D_LAUNCH_CHECK(h);
+  k_finite<<<148 * 4, 256, 0, h->stream>>>(h->W, sizeW(h->d), flag);
+  C3D_LAUNCH_CHECK(h);
+  int f = 0;
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(&f, flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  *ok = (f == 0);
+  return 0;
+}
+
+// ---- compute_dt with CFL > 0 (src/time_integration.f90:227-262) ----
+__global__ void __launch_bounds__(kRedThreads) k_cfl(Dims d, const double* __restrict__ xg,
+                                                    const double* __restrict__ yg,
+                                                    const double* __restrict__ zg,
+                                                    const double* __restrict__ U,
+                                                    const double* __restrict__ V,
+                                                    const double* __restrict__ W,
+                                                    double* __restrict__ part) {
+  const int ni = d.nxg - 2, nj = d.nyg - 2, nk = d.nzg - 2;
+  const int64_t tot = (int64_t)ni * nj * nk;
+  double mu = 0.0, mv = 0.0, mw = 0.0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = 2 + (int)(t % ni);
+    const int j = 2 + (int)((t / ni) % nj);
+    const int k = 2 + (int)(t / ((int64_t)ni * nj));
+    mu = fmax(mu, (xg[i + 1] - xg[i]) / fabs(U[idxU(d, i, j, k)]));
+    mv = fmax(mv, (yg[j + 1] - yg[j]) / fabs(V[idxV(d, i, j, k)]));
+    mw = fmax(mw, (zg[k + 1] - zg[k]) / fabs(W[idxW(d, i, j, k)]));
+  }
+  __shared__ double s[3][kRedThreads];
+  s[0][threadIdx.x] = mu; s[1][threadIdx.x] = mv; s[2][threadIdx.x] = mw;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int c = 0; c < 3; ++c) s[c][threadIdx.x] = fmax(s[c][threadIdx.x], s[c][threadIdx.x + st]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < 3; ++c) part[3 * blockIdx.x + c] = s[c][0];
+}
+
+int compute_dt_cfl(Handle* h, double* dt) {
+  const Params& p = h->p;
+  if (p.CFL < 0) { *dt = -p.CFL; return 0; }
+  double* xg = nullptr;
+  // grids on device: reuse the tail of the reduction buffer for xg, yg, zg
+  const Dims& d = h->d;
+  double* g = h->red + 4 * kRedBlocks;
+  xg = g;
+  double* yg = xg + d.nxg + 2;
+  double* zg = yg + d.nyg + 2;
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(xg, h->xg.data(), sizeof(double) * (d.nxg + 1), cudaMemcpyHostToDevice, h->stream));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(yg, h->yg.data(), sizeof(double) * (d.nyg + 1), cudaMemcpyHostToDevice, h->stream));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(zg, h->zg.data(), sizeof(double) * (d.nzg + 1), cudaMemcpyHostToDevice, h->stream));
+  k_cfl<<<kRedBlocks, kRedThreads, 0, h->stream>>>(d, xg, yg, zg, h->U, h->V, h->W, h->red);
+  C3D_LAUNCH_CHECK(h);
+  std::vector<double> part(3 * kRedBlocks);
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(part.data(), h->red, sizeof(double) * 3 * kRedBlocks,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  double lu = 0, lv = 0, lw = 0;
+  for (int b = 0; b < kRedBlocks; ++b) {
+    lu = part[3 * b] > lu ? part[3 * b] : lu;
+    lv = part[3 * b + 1] > lv ? part[3 * b + 1] : lv;
+    lw = part[3 * b + 2] > lw ? part[3 * b + 2] : lw;
+  }
+  double dtc = p.CFL * lu;
+  dtc = p.CFL * lv < dtc ? p.CFL * lv : dtc;
+  dtc = p.CFL * lw < dtc ? p.CFL * lw : dtc;
+  double dtv = p.CFL * h->dxmin * h->dxmin / p.nu;
+  double t2 = p.CFL * h->dymin * h->dymin / p.nu;
+  double t3 = p.CFL * h->dzmin * h->dzmin / p.nu;
+  dtv = t2 < dtv ? t2 : dtv;
+  dtv = t3 < dtv ? t3 : dtv;
+  double r = dtc < dtv ? dtc : dtv;
+  *dt = r < 0.1 ? r : 0.1;
+  return 0;
+}
+
+}  // namespace c3d

@@ -1,0 +1,223 @@
+// Right-hand sides and RK3 stage update.
+//
+// compute_rhs_u/v/w (src/equations.f90:24-423) evaluated point-wise for all
+// three components in one kernel, fused with the stage update of
+// compute_time_step_RK3 (src/time_integration.f90:105-107, 134-136, 163-168).
+//
+// Interpolations are the reference's midpoint averages (src/interpolation.f90);
+// every metric division is a precomputed reciprocal factor (Metric).  The
+// RK3 tableau a21 = a31 = 1/4 is exploited by keeping one accumulator
+// G = Uo + dt/4 F1 instead of Uo and F1:
+//   stage 1:  U* = U + dt*8/15*F1,   G = U + dt/4*F1
+//   stage 2:  U* = G + dt*5/12*F2
+//   stage 3:  U* = G + dt*3/4 *F3     (a32 = 0)
+// which is the reference's update up to FP64 rounding order.
+#include "c3d_internal.cuh"
+
+namespace c3d {
+
+struct RhsArgs {
+  Dims d;
+  Metric m;
+  const double* __restrict__ U;
+  const double* __restrict__ V;
+  const double* __restrict__ W;
+  const double* __restrict__ Gu;   // accumulators in (stages 2,3)
+  const double* __restrict__ Gv;
+  const double* __restrict__ Gw;
+  double* __restrict__ Us;         // stage outputs (interior)
+  double* __restrict__ Vs;
+  double* __restrict__ Ws;
+  double* __restrict__ Gu_out;     // accumulators out (stage 1)
+  double* __restrict__ Gv_out;
+  double* __restrict__ Gw_out;
+  const double* __restrict__ Hu;   // exterior pressure-gradient masks (IB) or null
+  const double* __restrict__ Hv;
+  const double* __restrict__ Hw;
+  const DevScalars* sc;
+  double cs;   // coefficient of F for U*
+  double cg;   // coefficient of F for G (stage 1)
+  int comp_mask;  // rhs-only mode: which components to write (bit0 u, bit1 v, bit2 w)
+};
+
+// MODE 0: write F into rhs_u/v/w arrays (fine entries), incl. the duplicated
+// periodic planes the reference also computes.  MODE 1: stage 1.  MODE 2: stage 2/3.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_rhs(RhsArgs a) {
+  const Dims& d = a.d;
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = 2 + blockIdx.z * blockDim.z + threadIdx.z;
+  if (i > d.Nx + 1 || j > d.Ny + 1 || k > d.Nz + 1) return;
+  const Metric& m = a.m;
+  const double* __restrict__ U = a.U;
+  const double* __restrict__ V = a.V;
+  const double* __restrict__ W = a.W;
+#define LU(ii, jj, kk) __ldg(U + idxU(d, ii, jj, kk))
+#define LV(ii, jj, kk) __ldg(V + idxV(d, ii, jj, kk))
+#define LW(ii, jj, kk) __ldg(W + idxW(d, ii, jj, kk))
+  const double dPdx = a.sc->dPdx, dPdy = a.sc->dPdy, dPdz = a.sc->dPdz;
+
+  // ---- shared loads
+  const double u0 = LU(i, j, k), uxm = LU(i - 1, j, k), uxp = LU(i + 1, j, k);
+  const double uym = LU(i, j - 1, k), uyp = LU(i, j + 1, k);
+  const double uzm = LU(i, j, k - 1), uzp = LU(i, j, k + 1);
+  const double v0 = LV(i, j, k), vxp = LV(i + 1, j, k), vym = LV(i, j - 1, k);
+  const double w0 = LW(i, j, k), wxp = LW(i + 1, j, k), wzm = LW(i, j, k - 1);
+
+  // ---------------- Fu (src/equations.f90:40-151)
+  double Fu;
+  {
+    const double v1m = LV(i + 1, j - 1, k);
+    const double w1m = LW(i + 1, j, k - 1);
+    const double ap = u0 + uxp, am = uxm + u0;
+    double r = (am * am - ap * ap) * (0.25 * m.rdxg[i]);
+    r += ((uym + u0) * (vym + v1m) - (u0 + uyp) * (v0 + vxp)) * (0.25 * m.rdy[j]);
+    r += ((uzm + u0) * (wzm + w1m) - (u0 + uzp) * (w0 + wxp)) * (0.25 * m.rdz[k]);
+    const double visc = m.cxpF[i] * (uxp - u0) - m.cxmF[i] * (u0 - uxm)
+                      + m.cypC[j] * (uyp - u0) - m.cymC[j] * (u0 - uym)
+                      + m.czpC[k] * (uzp - u0) - m.czmC[k] * (u0 - uzm);
+    r += visc;
+    r += a.Hu ? dPdx * __ldg(a.Hu + idxU(d, i, j, k)) : dPdx;
+    Fu = r;
+  }
+  // ---------------- Fw (src/equations.f90:309-421)
+  double Fw;
+  {
+    const double wxm = LW(i - 1, j, k), wym = LW(i, j - 1, k), wyp = LW(i, j + 1, k);
+    const double wzp = LW(i, j, k + 1);
+    const double umzp = LU(i - 1, j, k + 1);
+    const double vzp = LV(i, j, k + 1), vymzp = LV(i, j - 1, k + 1);
+    const double am = wzm + w0, ap = w0 + wzp;
+    double r = (am * am - ap * ap) * (0.25 * m.rdzg[k]);
+    r += ((uxm + umzp) * (wxm + w0) - (u0 + uzp) * (w0 + wxp)) * (0.25 * m.rdx[i]);
+    r += ((vym + vymzp) * (wym + w0) - (v0 + vzp) * (w0 + wyp)) * (0.25 * m.rdy[j]);
+    const double visc = m.cxpC[i] * (wxp - w0) - m.cxmC[i] * (w0 - wxm)
+                      + m.cypC[j] * (wyp - w0) - m.cymC[j] * (w0 - wym)
+                      + m.czpF[k] * (wzp - w0) - m.czmF[k] * (w0 - wzm);
+    r += visc;
+    r += a.Hw ? dPdz * __ldg(a.Hw + idxW(d, i, j, k)) : dPdz;
+    Fw = r;
+  }
+  // ---------------- Fv (src/equations.f90:174-286), faces j = 2..ny-1
+  const bool hasv = (j <= d.Ny);
+  double Fv = 0.0;
+  if (hasv) {
+    const double vxm = LV(i - 1, j, k), vyp = LV(i, j + 1, k);
+    const double vzm = LV(i, j, k - 1), vzp = LV(i, j, k + 1);
+    const double um1 = LU(i - 1, j + 1, k);
+    const double wyp = LW(i, j + 1, k), wypzm = LW(i, j + 1, k - 1);
+    const double am = vym + v0, ap = v0 + vyp;
+    double r = (am * am - ap * ap) * (0.25 * m.rdyg[j]);
+    r += ((uxm + um1) * (vxm + v0) - (u0 + uyp) * (v0 + vxp)) * (0.25 * m.rdx[i]);
+    r += ((vzm + v0) * (wzm + wypzm) - (v0 + vzp) * (w0 + wyp)) * (0.25 * m.rdz[k]);
+    const double visc = m.cxpC[i] * (vxp - v0) - m.cxmC[i] * (v0 - vxm)
+                      + m.cypF[j] * (vyp - v0) - m.cymF[j] * (v0 - vym)
+                      + m.czpC[k] * (vzp - v0) - m.czmC[k] * (v0 - vzm);
+    r += visc;
+    r += a.Hv ? dPdy * __ldg(a.Hv + idxV(d, i, j, k)) : dPdy;
+    Fv = r;
+  }
+#undef LU
+#undef LV
+#undef LW
+
+  if (MODE == 0) {
+    // rhs_u(2:nx-1, 2:nyg-1, 2:nzg-1): x 2..Nx+1, z 2..Nz+2 (plane Nz+2 duplicates 2)
+    const int nu1 = d.nx - 2, nu2 = d.nyg - 2;
+    if (a.comp_mask & 1) {
+      double* R = a.Us;
+      R[(i - 2) + (int64_t)nu1 * ((j - 2) + (int64_t)nu2 * (k - 2))] = Fu;
+      if (k == 2) R[(i - 2) + (int64_t)nu1 * ((j - 2) + (int64_t)nu2 * (d.Nz))] = Fu;
+    }
+    // rhs_v(2:nxg-1, 2:ny-1, 2:nzg-1): x 2..Nx+2
+    if ((a.comp_mask & 2) && hasv) {
+      double* R = a.Vs;
+      const int n1 = d.nxg - 2, n2 = d.ny - 2;
+      const int64_t o = (int64_t)n1 * n2;
+      R[(i - 2) + (int64_t)n1 * (j - 2) + o * (k - 2)] = Fv;
+      if (i == 2) R[(d.Nx) + (int64_t)n1 * (j - 2) + o * (k - 2)] = Fv;
+      if (k == 2) {
+        R[(i - 2) + (int64_t)n1 * (j - 2) + o * d.Nz] = Fv;
+        if (i == 2) R[(d.Nx) + (int64_t)n1 * (j - 2) + o * d.Nz] = Fv;
+      }
+    }
+    // rhs_w(2:nxg-1, 2:nyg-1, 2:nz-1): x 2..Nx+2
+    if (a.comp_mask & 4) {
+      double* R = a.Ws;
+      const int n1 = d.nxg - 2, n2 = d.nyg - 2;
+      const int64_t o = (int64_t)n1 * n2;
+      R[(i - 2) + (int64_t)n1 * (j - 2) + o * (k - 2)] = Fw;
+      if (i == 2) R[(d.Nx) + (int64_t)n1 * (j - 2) + o * (k - 2)] = Fw;
+    }
+    return;
+  }
+
+  const int64_t iu = idxU(d, i, j, k), iw = idxW(d, i, j, k);
+  if (MODE == 1) {
+    a.Us[iu] = u0 + a.cs * Fu;
+    a.Gu_out[iu] = u0 + a.cg * Fu;
+    a.Ws[iw] = w0 + a.cs * Fw;
+    a.Gw_out[iw] = w0 + a.cg * Fw;
+    if (hasv) {
+      const int64_t iv = idxV(d, i, j, k);
+      a.Vs[iv] = v0 + a.cs * Fv;
+      a.Gv_out[iv] = v0 + a.cg * Fv;
+    }
+  } else {
+    a.Us[iu] = __ldg(a.Gu + iu) + a.cs * Fu;
+    a.Ws[iw] = __ldg(a.Gw + iw) + a.cs * Fw;
+    if (hasv) {
+      const int64_t iv = idxV(d, i, j, k);
+      a.Vs[iv] = __ldg(a.Gv + iv) + a.cs * Fv;
+    }
+  }
+}
+
+static RhsArgs base_args(Handle* h) {
+  RhsArgs a{};
+  a.d = h->d;
+  a.m = h->m;
+  a.U = h->U; a.V = h->V; a.W = h->W;
+  a.sc = h->sc;
+  if (h->p.exterior_pressure_gradient && h->ib != nullptr) {
+    a.Hu = ib_hu(h); a.Hv = ib_hv(h); a.Hw = ib_hw(h);
+  }
+  return a;
+}
+
+static dim3 rhs_block() { return dim3(32, 4, 2); }
+static dim3 rhs_grid(const Dims& d) {
+  dim3 b = rhs_block();
+  return dim3((d.Nx + b.x - 1) / b.x, (d.Ny + b.y - 1) / b.y, (d.Nz + b.z - 1) / b.z);
+}
+
+// stage = 1, 2, 3; U,V,W (with valid ghosts) -> Us,Vs,Ws interior (+ G at stage 1)
+int launch_rhs_stage(Handle* h, int stage, double dt) {
+  RhsArgs a = base_args(h);
+  a.Us = h->Us; a.Vs = h->Vs; a.Ws = h->Ws;
+  if (stage == 1) {
+    a.Gu_out = h->Gu; a.Gv_out = h->Gv; a.Gw_out = h->Gw;
+    a.cs = dt * (8.0 / 15.0);
+    a.cg = dt * (1.0 / 4.0);
+    k_rhs<1><<<rhs_grid(h->d), rhs_block(), 0, h->stream>>>(a);
+  } else {
+    a.Gu = h->Gu; a.Gv = h->Gv; a.Gw = h->Gw;
+    a.cs = (stage == 2) ? dt * (5.0 / 12.0) : dt * (3.0 / 4.0);
+    k_rhs<2><<<rhs_grid(h->d), rhs_block(), 0, h->stream>>>(a);
+  }
+  C3D_LAUNCH_CHECK(h);
+  return 0;
+}
+
+// fine entries: component 1/2/3 -> rhsU/rhsV/rhsW
+int launch_rhs_only(Handle* h, int component) {
+  RhsArgs a = base_args(h);
+  a.Us = h->rhsU; a.Vs = h->rhsV; a.Ws = h->rhsW;
+  a.comp_mask = 1 << (component - 1);
+  k_rhs<0><<<rhs_grid(h->d), rhs_block(), 0, h->stream>>>(a);
+  C3D_LAUNCH_CHECK(h);
+  return 0;
+}
+
+}  // namespace c3d

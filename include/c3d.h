@@ -1,0 +1,214 @@
+/*
+ * c3d.h -- C-ABI of the B200 (sm_100a) channel3D RK3 fractional-step path.
+ *
+ * Every entry point replaces one Fortran module procedure of
+ * MetamaterialFSI/channel3D_parallel; the citation beside each declaration
+ * names the reference interface (file:line).  The unchanged Fortran driver
+ * (app/main.f90) binds these through an ISO_C_BINDING interface module
+ * (shown in INTEGRATION.md).
+ *
+ * Conventions
+ *  - Every function returns int: 0 = OK, < 0 = error (C3D_ERR_*), > 0 =
+ *    warning (C3D_WARN_*).  c3d_last_error() returns the message of the last
+ *    non-zero status on that handle.  Nothing is thrown across the ABI and
+ *    nothing calls exit().
+ *  - Fields live in device memory owned by the library for the lifetime of
+ *    the handle; they move to and from the host only through
+ *    c3d_upload / c3d_download.  Host buffers are caller-owned, FP64,
+ *    Fortran (column-major) order, and hold exactly the box lb..ub (inclusive,
+ *    Fortran indices of the field, see C3D_FIELD_* below).
+ *  - The domain is the reference's global array set for one z slab:
+ *    nx = nx_global, ny = ny_global, nz = nz_global, nxg = nx+1, nyg = ny+1,
+ *    nzg = nz+1 (src/initialization.f90:60-94 with nprocs = 1).
+ *  - One host thread per handle; each handle owns one CUDA stream.
+ */
+#ifndef C3D_H
+#define C3D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define C3D_OK                  0
+#define C3D_ERR_PARAM          -1   /* bad argument / namelist value          */
+#define C3D_ERR_CUDA           -2   /* CUDA runtime error                     */
+#define C3D_ERR_NAN            -3   /* non-finite value found in a field      */
+#define C3D_ERR_HANDLE         -4   /* unknown or destroyed handle            */
+#define C3D_ERR_IO             -5   /* file could not be read                 */
+#define C3D_ERR_UNSUPPORTED    -6   /* option not available for this set-up  */
+#define C3D_ERR_NO_DEVICE      -7   /* no CUDA device visible                 */
+#define C3D_WARN_NOT_CONVERGED  1   /* BiCGSTAB stopped at cg_max_iter        */
+
+/* ---- field identifiers (Fortran extents, lower bound 1 unless stated) ---- */
+#define C3D_FIELD_U             1   /* U(nx, nyg, nzg)        src/global.f90:106 */
+#define C3D_FIELD_V             2   /* V(nxg, ny, nzg)                           */
+#define C3D_FIELD_W             3   /* W(nxg, nyg, nz)                           */
+#define C3D_FIELD_P             4   /* P(nxg, nyg, nzg)                          */
+#define C3D_FIELD_RHS_P         5   /* rhs_p(2:nxg-1, 2:nyg-1, 2:nzg)  src/initialization.f90:155 */
+#define C3D_FIELD_P_INTERIM     6   /* P_interim, rhs_p extents  src/projection.f90:36 */
+#define C3D_FIELD_RHS_U         7   /* rhs_u(2:nx-1, 2:nyg-1, 2:nzg-1) src/equations.f90:29 */
+#define C3D_FIELD_RHS_V         8   /* rhs_v(2:nxg-1, 2:ny-1, 2:nzg-1) */
+#define C3D_FIELD_RHS_W         9   /* rhs_w(2:nxg-1, 2:nyg-1, 2:nz-1) */
+#define C3D_FIELD_U_WORK       10   /* U-shaped work field (e.g. U_interim)      */
+#define C3D_FIELD_V_WORK       11
+#define C3D_FIELD_W_WORK       12
+/* immersed-boundary fields */
+#define C3D_FIELD_U_REG        13   /* U_reg (U extents)  src/global.f90:107 */
+#define C3D_FIELD_V_REG        14
+#define C3D_FIELD_W_REG        15
+#define C3D_FIELD_HU_INTERIOR  16   /* Heaviside fields   src/global.f90:255-259 */
+#define C3D_FIELD_HV_INTERIOR  17
+#define C3D_FIELD_HW_INTERIOR  18
+#define C3D_FIELD_HC_EXTERIOR  19   /* Hc_exterior, rhs_p extents */
+/* Lagrangian (marker) arrays: 1-D, lb[0]..ub[0] index the vector */
+#define C3D_MARKER_FB          40   /* fb(4*nb)       src/global.f90:238 */
+#define C3D_MARKER_UB          41   /* ub(3*nb)       src/global.f90:232 */
+#define C3D_MARKER_XB          42   /* xb(nb)  */
+#define C3D_MARKER_YB          43   /* yb(nb)  */
+#define C3D_MARKER_ZB          44   /* zb(nb)  */
+#define C3D_MARKER_NORMALS     45   /* normals(3*nb)  */
+#define C3D_MARKER_SB          46   /* sb(nb)  */
+#define C3D_MARKER_E1NH_EXT    47   /* E1nH_exterior(3*nb) */
+#define C3D_MARKER_E1NHC_EXT   48   /* E1nHc_exterior(nb)  */
+
+/* ---- solver options ------------------------------------------------------ */
+#define C3D_POISSON_FP64        0   /* plain FP64 spectral Poisson solve        */
+#define C3D_POISSON_MIXED       1   /* FP32 spectral solve + FP64 refinement    */
+#define C3D_PRECOND_NONE        0   /* reference BiCGSTAB (unpreconditioned)    */
+#define C3D_PRECOND_JACOBI      1   /* diagonal (Jacobi) preconditioner         */
+#define C3D_PRECOND_LEARNED     2   /* learned preconditioner + warm start      */
+
+typedef struct c3d_dims {
+  int32_t nx, ny, nz;          /* nx_global, ny_global, nz_global            */
+  int32_t nxg, nyg, nzg;       /* centre extents incl. ghosts                 */
+  int32_t nxp, nzp, nym;       /* periodic cells in x, z; cells in y          */
+  int32_t nb;                  /* Lagrangian markers (0 without IB)          */
+} c3d_dims;
+
+typedef struct c3d_stats {
+  int64_t steps;               /* RK3 steps taken                             */
+  int64_t poisson_solves;      /* Poisson solves issued                       */
+  int64_t bicgstab_solves;     /* IB Schur solves                             */
+  int64_t bicgstab_iters;      /* accumulated BiCGSTAB iterations (cg_accum_iter) */
+  int32_t last_bicgstab_iters; /* iterations of the last Schur solve          */
+  int32_t refinement_sweeps;   /* mixed-precision refinement sweeps, last solve */
+  int64_t precond_fallbacks;   /* learned-preconditioner stalls -> Jacobi     */
+  double  last_residual;       /* ||r||_2 at exit of the last Schur solve     */
+  double  dPdx, dPdy, dPdz;    /* current mean pressure gradients             */
+  double  t, dt;               /* simulation time and last dt                 */
+  double  qflow_x_0;           /* target bulk flow                            */
+  int32_t status;              /* last status code                            */
+} c3d_stats;
+
+/* ---- lifecycle ------------------------------------------------------------
+ * c3d_create: read the &params namelist (src/input_output.f90:21-132), build
+ * the grid (create_grid, src/input_output.f90:140-206), metrics, Fourier and
+ * tridiagonal set-up (initialize, src/initialization.f90:24-460) and allocate
+ * the device fields.  The fields start at zero (init_type 1); upload a state
+ * with c3d_upload or a snapshot grid with c3d_set_grid.                      */
+int c3d_create(const char* namelist_path, int* handle);
+/* same, from namelist text in memory */
+int c3d_create_from_text(const char* namelist_text, int* handle);
+/* finalize, src/finalization.f90:19-33 */
+int c3d_destroy(int handle);
+/* replace the face grids (read_input_data mesh, src/input_output.f90:347-358) */
+int c3d_set_grid(int handle, const double* x, const double* y, const double* z);
+int c3d_get_dims(int handle, c3d_dims* dims);
+/* read back the grids: x(nx), y(ny), z(nz), xg(nxg), yg(nyg), zg(nzg) */
+int c3d_get_grid(int handle, double* x, double* y, double* z,
+                 double* xg, double* yg, double* zg);
+const char* c3d_last_error(int handle);
+
+/* ---- field transfer ------------------------------------------------------ */
+int c3d_upload(int handle, int field_id, const double* host,
+               const int64_t lb[3], const int64_t ub[3]);
+int c3d_download(int handle, int field_id, double* host,
+                 const int64_t lb[3], const int64_t ub[3]);
+/* scalars: dPdx, dPdy, dPdz, t, Qflow_x_0 (module globals, src/global.f90:167-173) */
+int c3d_set_scalars(int handle, double dPdx, double dPdy, double dPdz,
+                    double t, double qflow_x_0);
+int c3d_synchronize(int handle);
+
+/* ---- coarse entries (hot path) -------------------------------------------- */
+/* compute_time_step_RK3, src/time_integration.f90:86-213; nsteps steps, each
+ * preceded by compute_dt (src/time_integration.f90:219-267).               */
+int c3d_time_step_rk3(int handle, int nsteps);
+/* compute_dt, src/time_integration.f90:219-267 */
+int c3d_compute_dt(int handle, double* dt);
+/* compute_mean_mass_flow_U with Hu, src/mass_flow.f90:24-53 (app/main.f90:90) */
+int c3d_compute_mean_mass_flow_u(int handle, double* qflow);
+
+/* ---- fine entries mirroring the module interfaces ------------------------- */
+/* compute_rhs_u/v/w(U,V,W,rhs), src/equations.f90:24,160,295: reads the
+ * current U,V,W fields, writes C3D_FIELD_RHS_U/V/W.                         */
+int c3d_compute_rhs_u(int handle);
+int c3d_compute_rhs_v(int handle);
+int c3d_compute_rhs_w(int handle);
+/* solve_poisson_equation(rhs), src/poisson.f90:33-101: in place on
+ * C3D_FIELD_RHS_P; rk_step == 1 also sets P (src/poisson.f90:91-99).        */
+int c3d_solve_poisson_equation(int handle, int rk_step);
+/* divergence(rhs_p, U, V, W), src/differential_operators.f90:54-74 */
+int c3d_divergence(int handle);
+/* compute_non_IB_projection, src/projection.f90:22-46 */
+int c3d_compute_non_IB_projection(int handle, int rk_step);
+/* apply_boundary_conditions(U,V,W), src/boundary_conditions.f90:20-55;
+ * which: 0 = U,V,W; 1 = U_reg,V_reg,W_reg; 2 = the U/V/W work fields       */
+int c3d_apply_boundary_conditions(int handle, int which);
+/* compute_dPx_for_constant_mass_flow(U, dPdx), src/mass_flow.f90:144-175 */
+int c3d_compute_dPx_for_constant_mass_flow(int handle, double* dPdx);
+/* compute_pressure, src/pressure.f90:21-29 -- interface kept; the reference
+ * never calls it (src/statistics.f90:37) and it returns C3D_ERR_UNSUPPORTED. */
+int c3d_compute_pressure(int handle);
+
+/* ---- immersed boundary ---------------------------------------------------- */
+/* setup_IB_geometry (src/immersed_boundary_geometry.f90:70-398) at time t   */
+int c3d_setup_IB_geometry(int handle);
+/* setup_IB_operators, src/immersed_boundary_operators.f90:19-256 */
+int c3d_setup_IB_operators(int handle);
+/* compute_heaviside, src/heaviside.f90:20-54 */
+int c3d_compute_heaviside(int handle);
+/* regT(Eu, U, V, W), src/immersed_boundary_operators.f90:296-318: host out (3*nb) */
+int c3d_regT(int handle, double* Eu);
+/* regTc_1n(E1np, P_interim), src/immersed_boundary_operators.f90:344-357 (nb) */
+int c3d_regTc_1n(int handle, int field_id, double* E1np);
+/* regT_1n(E1nu, U, V, W), src/immersed_boundary_operators.f90:320-342 (3*nb) */
+int c3d_regT_1n(int handle, double* E1nu);
+/* regu/regv/regw(F, f), src/immersed_boundary_operators.f90:359-400:
+ * component 1/2/3 spread of f (nb) into U_reg/V_reg/W_reg                 */
+int c3d_reg(int handle, int component, const double* f);
+/* schur(Sf, f), src/projection.f90:98-144 (host vectors of 4*nb) */
+int c3d_schur(int handle, const double* f, double* Sf);
+/* bicgstab(fb, rhs_ib), src/projection.f90:146-186: solves for the device
+ * fb (warm start = current fb) with right-hand side rhs (4*nb, host).       */
+int c3d_bicgstab(int handle, const double* rhs);
+/* compute_IB_projection, src/projection.f90:48-96 */
+int c3d_compute_IB_projection(int handle);
+
+/* ---- options and telemetry ------------------------------------------------ */
+int c3d_set_mode(int handle, int poisson_mode, int precond_mode);
+int c3d_get_stats(int handle, c3d_stats* stats);
+/* max |div u| over interior cells, src/monitor.f90:210-221 */
+int c3d_check_divergence(int handle, double* max_divergence);
+/* NaN scan of U,V,W (statistics NaN stop, src/statistics.f90:142-144):
+ * returns C3D_ERR_NAN if any entry is not finite.                           */
+int c3d_check_finite(int handle);
+
+/* ---- timing support (kernel-level evidence) ------------------------------- */
+/* device time in ms of the last c3d_time_step_rk3 call, from CUDA events     */
+int c3d_last_step_time_ms(int handle, double* ms);
+/* number of kernels launched by the library since the handle was created   */
+int c3d_kernel_launches(int handle, int64_t* count);
+/* time every kernel class of one RK3 stage separately, each launched nrep
+ * times between CUDA events on the handle's stream (the fields are used as
+ * scratch); ms[c] = average device time of class c in the order
+ * rhs_stage, ghosts, div_xfft, zfft_fwd, tridiag, zfft_inv, xfft_inv,
+ * grad_sub, massflow.  Writes min(nmax, 9) entries.                          */
+int c3d_profile_kernels(int handle, int nrep, double* ms, int nmax);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* C3D_H */

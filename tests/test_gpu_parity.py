@@ -1,0 +1,208 @@
+"""GPU parity of the FP64 path against the CPU oracle, through the C-ABI.
+
+Tolerances (max-norm error relative to the max-norm of the oracle field):
+  copies (boundary conditions)            bit-exact
+  right-hand sides, divergence            1e-12
+  Poisson solve, projection               1e-11  (Thomas vs LAPACK zgtsv, FFT rounding)
+  RK3 steps (1 and 10)                    1e-10  (north-star bar)
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import channel_oracle as co
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    # name: (nx_global, ny_global, nz_global, Lxp, Lzp, grid_type)
+    "cfg0_34x65x34": (34, 65, 34, math.pi, math.pi / 2, 1),
+    "odd_ny_radix3": (50, 34, 26, 2.0, 1.0, 1),
+    "uniform_small": (18, 17, 14, 1.0, 0.7, 0),
+}
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def make_pair(case, amplitude=0.1, seed=0):
+    import channel3d_parallel_b200 as c3d
+    nx, ny, nz, lx, lz, gt = CASES[case]
+    nu = 1.0 / 5600.0
+    p = co.channel_params(nx, ny, nz, lx, lz, nu, grid_type=gt)
+    g = co.Grid(p)
+    st = co.seeded_initial_state(g, p["dpdx"], amplitude=amplitude, seed=seed)
+    ch = c3d.Channel(nx_global=nx, ny_global=ny, nz_global=nz, Lxp=lx, Lzp=lz, nu=nu,
+                     CFL=-1e-3, x_mass_cte=1, grid_type=gt, alpha_stretch=2.0, dPdx=p["dpdx"])
+    ch.set_grid(g.x[1:], g.y[1:], g.z[1:])
+    ch.upload("U", st.U[1:, 1:, 1:])
+    ch.upload("V", st.V[1:, 1:, 1:])
+    ch.upload("W", st.W[1:, 1:, 1:])
+    ch.set_scalars(dPdx=st.dPdx, t=0.0, Qflow_x_0=st.Qflow_x_0)
+    ch.compute_dt()
+    return p, g, st, ch
+
+
+@pytest.fixture(params=list(CASES))
+def pair(request):
+    p, g, st, ch = make_pair(request.param)
+    yield p, g, st, ch
+    ch.close()
+
+
+def test_library_grid_matches_oracle():
+    import channel3d_parallel_b200 as c3d
+    p = co.channel_params(34, 65, 34, math.pi, math.pi / 2, 1 / 5600)
+    g = co.Grid(p)
+    with c3d.Channel(nx_global=34, ny_global=65, nz_global=34, Lxp=math.pi, Lzp=math.pi / 2,
+                     nu=1 / 5600, CFL=-1e-3, grid_type=1, alpha_stretch=2.0) as ch:
+        gr = ch.grid()
+    for k in ("x", "y", "z", "xg", "yg", "zg"):
+        ref = getattr(g, k)[1:]
+        assert np.abs(gr[k] - ref).max() <= 4e-16 * max(1.0, np.abs(ref).max()), k
+
+
+def test_boundary_conditions_bit_exact(pair):
+    p, g, st, ch = pair
+    rng = np.random.default_rng(11)
+    U, V, W = (rng.standard_normal(a.shape) for a in (st.U, st.V, st.W))
+    ch.upload("U", U[1:, 1:, 1:]); ch.upload("V", V[1:, 1:, 1:]); ch.upload("W", W[1:, 1:, 1:])
+    ch.apply_boundary_conditions("UVW")
+    co.apply_boundary_conditions(g, U, V, W)
+    assert np.array_equal(ch.download("U"), U[1:, 1:, 1:])
+    assert np.array_equal(ch.download("V"), V[1:, 1:, 1:])
+    assert np.array_equal(ch.download("W"), W[1:, 1:, 1:])
+
+
+def test_rhs(pair):
+    p, g, st, ch = pair
+    ru = co.compute_rhs_u(g, st.U, st.V, st.W, st.dPdx)
+    rv = co.compute_rhs_v(g, st.U, st.V, st.W, st.dPdy)
+    rw = co.compute_rhs_w(g, st.U, st.V, st.W, st.dPdz)
+    assert rel(ch.compute_rhs_u(), ru) < 1e-12
+    assert rel(ch.compute_rhs_v(), rv) < 1e-12
+    assert rel(ch.compute_rhs_w(), rw) < 1e-12
+
+
+def test_divergence_and_poisson(pair):
+    p, g, st, ch = pair
+    # perturb so the field is not divergence-free
+    rng = np.random.default_rng(2)
+    U = st.U.copy(); U[2:g.nx, 2:g.nyg, 2:g.nzg] += 0.01 * rng.standard_normal(U[2:g.nx, 2:g.nyg, 2:g.nzg].shape)
+    co.apply_boundary_conditions(g, U, st.V, st.W)
+    ch.upload("U", U[1:, 1:, 1:])
+    ch.divergence()
+    d_ref = co.divergence(g, U, st.V, st.W)
+    d_gpu = ch.download("RHS_P")
+    assert rel(d_gpu, d_ref[2:, 2:, 2:]) < 1e-12
+    ch.solve_poisson_equation(rk_step=1)
+    s_ref = co.solve_poisson_equation(g, d_ref.copy(), st, rk_step=1, dt=1e-3)
+    s_gpu = ch.download("RHS_P")
+    assert rel(s_gpu, s_ref[2:, 2:, 2:]) < 1e-11
+    assert rel(ch.download("P"), st.P[1:, 1:, 1:]) < 1e-11
+
+
+def test_non_IB_projection(pair):
+    p, g, st, ch = pair
+    rng = np.random.default_rng(4)
+    U = st.U.copy(); U[2:g.nx, 2:g.nyg, 2:g.nzg] += 0.01 * rng.standard_normal(U[2:g.nx, 2:g.nyg, 2:g.nzg].shape)
+    co.apply_boundary_conditions(g, U, st.V, st.W)
+    st.U = U
+    ch.upload("U", U[1:, 1:, 1:])
+    ch.compute_non_IB_projection(rk_step=0)
+    co.compute_non_IB_projection(g, st, 1e-3)
+    for name, ref in (("U", st.U), ("V", st.V), ("W", st.W)):
+        assert rel(ch.download(name), ref[1:, 1:, 1:]) < 1e-11, name
+    assert rel(ch.download("P_INTERIM"), st.P_interim[2:, 2:, 2:]) < 1e-11
+
+
+@pytest.mark.parametrize("nsteps", [1, 10])
+def test_rk3_steps(pair, nsteps):
+    p, g, st, ch = pair
+    ch.compute_time_step_RK3(nsteps)
+    for _ in range(nsteps):
+        co.compute_time_step_RK3(g, st, 1e-3)
+    errs = {name: rel(ch.download(name), ref[1:, 1:, 1:])
+            for name, ref in (("U", st.U), ("V", st.V), ("W", st.W), ("P", st.P))}
+    assert max(errs.values()) < 1e-10, errs
+    s = ch.stats()
+    assert abs(s["dPdx"] - st.dPdx) <= 1e-9 * abs(st.dPdx) + 1e-14
+    assert s["steps"] == nsteps
+    assert ch.check_divergence() < 1e-12
+    assert ch.check_finite() == 0
+
+
+def test_mass_flow_entries(pair):
+    p, g, st, ch = pair
+    q, n = co.mean_mass_flow_u(g, st.U)
+    assert abs(ch.compute_mean_mass_flow_U() - q / n) < 1e-14
+    assert abs(ch.compute_dPx_for_constant_mass_flow() - (st.Qflow_x_0 - q / n)) < 1e-14
+
+
+def test_product_initial_state_matches_oracle():
+    import channel3d_parallel_b200 as c3d
+    nx, ny, nz, lx, lz, gt = CASES["cfg0_34x65x34"]
+    p = co.channel_params(nx, ny, nz, lx, lz, 1 / 5600, grid_type=gt)
+    g = co.Grid(p)
+    st = co.seeded_initial_state(g, p["dpdx"])
+    with c3d.Channel(nx_global=nx, ny_global=ny, nz_global=nz, Lxp=lx, Lzp=lz, nu=1 / 5600,
+                     CFL=-1e-3, x_mass_cte=1, grid_type=gt, alpha_stretch=2.0) as ch:
+        ch.set_grid(g.x[1:], g.y[1:], g.z[1:])
+        q0 = c3d.seeded_initial_state(ch, p["dpdx"], 1 / 5600)
+        assert abs(q0 - st.Qflow_x_0) < 1e-13
+        for name, ref in (("U", st.U), ("V", st.V), ("W", st.W)):
+            assert rel(ch.download(name), ref[1:, 1:, 1:]) < 1e-12
+
+
+def test_nan_is_reported():
+    """A non-finite value uploaded from the host comes back as C3D_ERR_NAN."""
+    import channel3d_parallel_b200 as c3d
+    p, g, st, ch = make_pair("uniform_small")
+    try:
+        U = st.U.copy()
+        U[5, 5, 5] = np.nan
+        ch.upload("U", U[1:, 1:, 1:])
+        with pytest.raises(c3d.C3DError) as e:
+            ch.check_finite()
+        assert e.value.code == -3
+    finally:
+        ch.close()
+
+
+def test_partial_box_transfer():
+    p, g, st, ch = make_pair("uniform_small")
+    try:
+        full = ch.download("V")
+        sub = ch.download("V", lb=(3, 2, 4), ub=(9, 7, 8))
+        assert np.array_equal(sub, full[2:9, 1:7, 3:8])
+        ch.upload("V", np.zeros((7, 6, 5)), lb=(3, 2, 4))
+        full2 = ch.download("V")
+        assert np.all(full2[2:9, 1:7, 3:8] == 0.0)
+    finally:
+        ch.close()
+
+
+def test_full_size_one_step_parity():
+    """192x129x192 (the throughput configuration): one RK3 step against the
+    oracle, plus size-independent properties over further steps."""
+    import channel3d_parallel_b200 as c3d
+    nu = 1.0 / 5600.0
+    p = co.channel_params(194, 129, 194, 4 * math.pi, 4 * math.pi / 3, nu)
+    g = co.Grid(p)
+    st = co.seeded_initial_state(g, p["dpdx"])
+    with c3d.Channel(nx_global=194, ny_global=129, nz_global=194, Lxp=4 * math.pi,
+                     Lzp=4 * math.pi / 3, nu=nu, CFL=-1e-3, x_mass_cte=1, grid_type=1,
+                     alpha_stretch=2.0, dPdx=p["dpdx"]) as ch:
+        ch.set_grid(g.x[1:], g.y[1:], g.z[1:])
+        for name, ref in (("U", st.U), ("V", st.V), ("W", st.W)):
+            ch.upload(name, ref[1:, 1:, 1:])
+        ch.set_scalars(dPdx=st.dPdx, Qflow_x_0=st.Qflow_x_0)
+        ch.compute_time_step_RK3(1)
+        co.compute_time_step_RK3(g, st, 1e-3)
+        for name, ref in (("U", st.U), ("V", st.V), ("W", st.W), ("P", st.P)):
+            assert rel(ch.download(name), ref[1:, 1:, 1:]) < 1e-10, name
+        ch.compute_time_step_RK3(4)
+        assert ch.check_divergence() < 1e-12
+        assert abs(ch.compute_mean_mass_flow_U() - st.Qflow_x_0) < 1e-13
