@@ -207,6 +207,15 @@ def run_ours(args):
         pg.barrier()
     value = ws / (ms_step * 1e-3)
     div = ch.check_divergence()
+    if args.device_only:
+        ch.close()
+        if pg:
+            pg.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"metric": "RK3 steps/s at 192x129x192", "value": value,
+                              "unit": "steps/s", "ms_per_step": ms_step,
+                              "gpu_launches": launches, "max_div": div}), flush=True)
+        return
 
     # ---- per-kernel device times (roofline of the dominant kernel)
     prof = ch.profile_kernels(nrep=10)
@@ -305,6 +314,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--poisson", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--device-only", action="store_true",
+                    help="only the device-timed step loop (used for profiler captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
