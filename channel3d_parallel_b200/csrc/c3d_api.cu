@@ -19,6 +19,11 @@ static std::map<int, Handle*> g_handles;
 static int g_next = 1;
 static std::string g_global_error;
 
+void set_global_error(const std::string& msg) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_global_error = msg;
+}
+
 static Handle* lookup(int id) {
   std::lock_guard<std::mutex> lk(g_mu);
   auto it = g_handles.find(id);

@@ -121,6 +121,8 @@ struct Params {
 };
 
 int parse_namelist(const std::string& text, Params& p, std::string& err);
+// message returned by c3d_last_error for calls that have no handle
+void set_global_error(const std::string& msg);
 
 struct IbState;   // immersed-boundary state (k_ib.cu)
 struct MixedState;  // mixed-precision work buffers (k_poisson.cu)

@@ -89,6 +89,8 @@ PROTOTYPES = {
     "c3d_last_step_time_ms": [_INT, _D],
     "c3d_kernel_launches": [_INT, C.POINTER(C.c_int64)],
     "c3d_profile_kernels": [_INT, _INT, _D, _INT],
+    "c3d_mean_mass_flow_u_noalloc": [C.c_void_p, _INT, _INT, _INT, C.c_void_p, C.c_void_p,
+                                     C.c_void_p],
 }
 KERNEL_CLASSES = ("rhs_stage", "ghosts", "div_xfft", "zfft_fwd", "tridiag", "zfft_inv",
                   "xfft_inv", "grad_sub", "massflow")

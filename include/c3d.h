@@ -208,6 +208,26 @@ int c3d_kernel_launches(int handle, int64_t* count);
  * grad_sub, massflow.  Writes min(nmax, 9) entries.                          */
 int c3d_profile_kernels(int handle, int nrep, double* ms, int nmax);
 
+/* ---- allocation-free entry ------------------------------------------------
+ * No counterpart in the reference.  Bulk flux of U, the value of
+ * c3d_compute_mean_mass_flow_u for a field without immersed body (Hu = 1),
+ * for callers that must not allocate device memory -- a driver that checks
+ * the flux inside its own time loop, where cudaMalloc would synchronise the
+ * device, or a program whose device memory belongs to another runtime's
+ * fixed pool.  No handle is needed and nothing is allocated: the per-plane
+ * partial sums live in a static device array of 4096 z planes (64 KiB per
+ * GPU that loads the library, held until exit); nzg-2 > 4096 is rejected
+ * with C3D_ERR_PARAM.  The first call on a device looks up that array's
+ * address, so make it before any stream capture.  Calls share the array:
+ * calls that overlap on the GPU race, so serialise them (one stream).
+ *   U      device pointer, U(nx, nyg, nzg) in Fortran order
+ *   yg     device pointer, yg(1:nyg)
+ *   qflow  device pointer to one double: Int_U / norm
+ *   stream cudaStream_t to launch on (NULL: the legacy default stream)
+ * Errors are reported through c3d_last_error(0).                            */
+int c3d_mean_mass_flow_u_noalloc(const double* U, int nx, int nyg, int nzg,
+                                 const double* yg, double* qflow, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
