@@ -23,7 +23,8 @@ _NAMELIST_ORDER = [
     "y_mass_cte", "z_mass_cte", "nsteps", "nsave", "nstats", "nmonitor", "filein", "fileout",
     "nstep_init", "t_init", "init_type", "grid_type", "body_type",
     "exterior_pressure_gradient", "body_param_3", "body_param_1", "body_param_2",
-    "body_ramp_up_time", "min_buffer_width", "cg_tol", "cg_max_iter", "perturb_scale"]
+    "body_ramp_up_time", "min_buffer_width", "cg_tol", "cg_max_iter", "perturb_scale",
+    "body_param_4"]
 
 
 def namelist_text(**params):

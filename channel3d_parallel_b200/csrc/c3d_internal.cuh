@@ -115,6 +115,9 @@ struct Params {
   std::string body_type = "none";
   bool exterior_pressure_gradient = true;
   double body_param_1 = 0, body_param_2 = 0, body_param_3 = 0, body_ramp_up_time = 0;
+  // extension (no reference counterpart): mean y of the single plane of
+  // body_type 'wall_standing_wave'
+  double body_param_4 = 0;
   double min_buffer_width = 0, cg_tol = (double)1e-8f;
   int cg_max_iter = 50;
   double perturb_scale = 0.5;

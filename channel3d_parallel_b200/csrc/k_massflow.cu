@@ -106,7 +106,9 @@ __global__ void k_shift_u(Dims d, double* __restrict__ U, const DevScalars* sc) 
 }
 
 int launch_massflow_correction(Handle* h, double dt) {
-  k_massflow_partial<<<kRedBlocks, kRedThreads, 0, h->stream>>>(h->d, h->m, h->U, nullptr,
+  // with an immersed body the flux is H-weighted (src/mass_flow.f90:160-163)
+  const double* Hu = h->ib ? ib_hu(h) : nullptr;
+  k_massflow_partial<<<kRedBlocks, kRedThreads, 0, h->stream>>>(h->d, h->m, h->U, Hu,
                                                                 (double2*)h->red);
   C3D_LAUNCH_CHECK(h);
   k_massflow_final<<<1, 1024, 0, h->stream>>>((const double2*)h->red, kRedBlocks, h->sc,

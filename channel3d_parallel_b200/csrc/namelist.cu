@@ -144,6 +144,7 @@ int parse_namelist(const std::string& text, Params& p, std::string& err) {
     else if (key == "body_param_1") rc = need_real(p.body_param_1);
     else if (key == "body_param_2") rc = need_real(p.body_param_2);
     else if (key == "body_param_3") rc = need_real(p.body_param_3);
+    else if (key == "body_param_4") rc = need_real(p.body_param_4);   // extension
     else if (key == "body_ramp_up_time") rc = need_real(p.body_ramp_up_time);
     else if (key == "min_buffer_width") rc = need_real(p.min_buffer_width);
     else if (key == "cg_tol") rc = need_real(p.cg_tol);

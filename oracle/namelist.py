@@ -41,6 +41,9 @@ DEFAULTS = {
     "nmonitor": 0, "filein": "", "fileout": "", "nstep_init": 0,
     "init_type": 1, "grid_type": 0, "body_param_1": 0.0,
     "body_param_2": 0.0, "body_param_3": 0.0,
+    # extension (no reference counterpart): mean y of the plane of
+    # body_type 'wall_standing_wave'
+    "body_param_4": 0.0,
 }
 
 INT_KEYS = {"nx_global", "ny_global", "nz_global", "nxb", "nzb", "x_mass_cte",

@@ -1,0 +1,145 @@
+"""GPU parity of the immersed-boundary path against the CPU oracle.
+
+Tolerances (max-norm relative): E / E1n / R and Heaviside fields 1e-12
+(R uses FP64 atomics, so sums are order-dependent at round-off); Schur
+operator 1e-11; BiCGSTAB solution and IB RK3 steps 1e-9 (the Krylov
+iterates amplify round-off by the conditioning of the Schur operator).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import channel_oracle as co
+from oracle import ib_oracle as ibo
+
+pytestmark = pytest.mark.gpu
+
+NU = 3.076923076923077e-04
+
+CASES = {
+    # planar static wall at y = Ly/2 on a uniform grid (examples/input_parameters_ib_planar_wall)
+    "center_wall": dict(nx_global=18, ny_global=33, nz_global=18, Lxp=1.718, Lzp=0.859,
+                        grid_type=0, alpha_stretch=0.0, body_type="center_wall", nxb=16, nzb=16,
+                        cfl=-0.01),
+    # one plane at y = 0.2 with a standing wave inside the uniform wall buffer of grid type 2
+    "wall_standing_wave": dict(nx_global=34, ny_global=49, nz_global=14, Lxp=2.0, Lzp=0.6,
+                               grid_type=2, alpha_stretch=2.0, min_buffer_width=0.3,
+                               body_type="wall_standing_wave", nxb=32, nzb=12,
+                               body_param_1=0.02, body_param_2=2 * math.pi / 5.0,
+                               body_param_3=1.0, body_param_4=0.2, cfl=-1e-3),
+    # two concentric z cylinders on a uniform grid (examples/input_parameters_ib_double_rotating_cylinders)
+    "double_cylinders_z": dict(nx_global=34, ny_global=33, nz_global=14, Lxp=2.0, Lzp=1.0,
+                               grid_type=0, alpha_stretch=0.0, body_type="double_cylinders_z",
+                               nxb=0, nzb=6, body_param_1=0.15, body_param_2=0.3,
+                               body_param_3=0.015, cfl=-0.01),
+    # both walls with a standing wave (examples/input_parameters_ib_standing_wave)
+    "standing_wave": dict(nx_global=34, ny_global=65, nz_global=10, Lxp=2.0, Lzp=0.5,
+                          grid_type=2, alpha_stretch=2.0, min_buffer_width=0.1,
+                          body_type="standing_wave", nxb=16, nzb=3, body_param_1=0.05,
+                          body_param_2=0.5, body_param_3=1.0, cfl=-0.02),
+}
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def build(case, cg_tol=1e-12, cg_max_iter=200, x_mass_cte=1):
+    import channel3d_parallel_b200 as c3d
+    kw = dict(CASES[case])
+    nx, ny, nz = kw.pop("nx_global"), kw.pop("ny_global"), kw.pop("nz_global")
+    lx, lz = kw.pop("Lxp"), kw.pop("Lzp")
+    gt, al = kw.pop("grid_type"), kw.pop("alpha_stretch")
+    cfl = kw.pop("cfl")
+    p = co.channel_params(nx, ny, nz, lx, lz, NU, alpha=al, grid_type=gt, cfl=cfl,
+                          x_mass_cte=x_mass_cte, cg_tol=cg_tol, cg_max_iter=cg_max_iter,
+                          **{k.lower(): v for k, v in kw.items()})
+    g = co.Grid(p)
+    st = co.seeded_initial_state(g, p["dpdx"], amplitude=0.05, dt=-cfl)
+    ib = ibo.IBState(g, p, t=0.0)
+    ibo.compute_heaviside(g, ib)
+    q, n = co.mean_mass_flow_u(g, st.U, ib.Hu)
+    st.Qflow_x_0 = q / n
+    ch = c3d.Channel(nx_global=nx, ny_global=ny, nz_global=nz, Lxp=lx, Lzp=lz, nu=NU, CFL=cfl,
+                     x_mass_cte=x_mass_cte, grid_type=gt, alpha_stretch=al, dPdx=p["dpdx"],
+                     cg_tol=cg_tol, cg_max_iter=cg_max_iter, **kw)
+    ch.set_grid(g.x[1:], g.y[1:], g.z[1:])
+    for name, ref in (("U", st.U), ("V", st.V), ("W", st.W)):
+        ch.upload(name, ref[1:, 1:, 1:])
+    ch.compute_dt()
+    ch.compute_heaviside()
+    ch.set_scalars(dPdx=st.dPdx, t=0.0, Qflow_x_0=st.Qflow_x_0)
+    return p, g, st, ib, ch
+
+
+@pytest.fixture(params=list(CASES))
+def setup(request):
+    p, g, st, ib, ch = build(request.param)
+    yield request.param, p, g, st, ib, ch
+    ch.close()
+
+
+def test_marker_geometry(setup):
+    case, p, g, st, ib, ch = setup
+    b = ib.body
+    assert ch.dims["nb"] == b.nb
+    for name, ref in (("XB", b.xb), ("YB", b.yb), ("ZB", b.zb), ("SB", b.sb),
+                      ("NORMALS", b.normals), ("UB", b.ub)):
+        got = ch.download(name)
+        assert np.abs(got - ref).max() <= 1e-14 * max(1.0, np.abs(ref).max()), name
+
+
+def test_interpolation_and_spreading(setup):
+    case, p, g, st, ib, ch = setup
+    rng = np.random.default_rng(7)
+    U, V, W = (rng.standard_normal(a.shape) for a in (st.U, st.V, st.W))
+    co.apply_boundary_conditions(g, U, V, W)
+    for name, A in (("U", U), ("V", V), ("W", W)):
+        ch.upload(name, A[1:, 1:, 1:])
+    assert rel(ch.regT(), ib.ops.E(U, V, W)) < 1e-12
+    assert rel(ch.regT_1n(), ib.ops.E1n(U, V, W)) < 1e-12
+    Pr = g.rhs_p_array()
+    Pr[2:, 2:, 2:] = rng.standard_normal(Pr[2:, 2:, 2:].shape)
+    ch.upload("P_INTERIM", Pr[2:, 2:, 2:])
+    assert rel(ch.regTc_1n("P_INTERIM"), ib.ops.E1n_c(Pr)) < 1e-12
+    nb = ib.body.nb
+    f = rng.standard_normal(nb)
+    for comp, (fname, shape) in enumerate((("U_REG", st.U.shape), ("V_REG", st.V.shape),
+                                           ("W_REG", st.W.shape))):
+        ch.reg(comp + 1, f)
+        ref = ib.ops.R(comp, f, shape)
+        assert rel(ch.download(fname), ref[1:, 1:, 1:]) < 1e-12, fname
+
+
+def test_heaviside(setup):
+    case, p, g, st, ib, ch = setup
+    for name, ref in (("HU_INTERIOR", ib.Hu), ("HV_INTERIOR", ib.Hv), ("HW_INTERIOR", ib.Hw)):
+        assert np.abs(ch.download(name) - ref[1:, 1:, 1:]).max() < 1e-11, name
+    assert np.abs(ch.download("HC_EXTERIOR") - ib.Hc_ext[2:, 2:, 2:]).max() < 1e-11
+    assert rel(ch.download("E1NHC_EXT"), ib.E1nHc_ext) < 1e-10
+    assert rel(ch.download("E1NH_EXT"), ib.E1nH_ext) < 1e-10
+
+
+def test_schur_operator(setup):
+    case, p, g, st, ib, ch = setup
+    rng = np.random.default_rng(9)
+    f = rng.standard_normal(4 * ib.body.nb)
+    dt = -p["cfl"]
+    assert rel(ch.schur(f), ibo.schur(g, ib, f, dt)) < 1e-11
+
+
+@pytest.mark.parametrize("nsteps", [1, 2])
+def test_ib_rk3_steps(setup, nsteps):
+    case, p, g, st, ib, ch = setup
+    dt = -p["cfl"]
+    ch.compute_time_step_RK3(nsteps)
+    for _ in range(nsteps):
+        ibo.compute_time_step_RK3_ib(g, st, ib, dt)
+    errs = {name: rel(ch.download(name), ref[1:, 1:, 1:])
+            for name, ref in (("U", st.U), ("V", st.V), ("W", st.W))}
+    assert max(errs.values()) < 1e-9, errs
+    assert rel(ch.download("FB"), ib.fb) < 1e-7
+    s = ch.stats()
+    assert s["bicgstab_solves"] == 3 * nsteps
+    assert s["last_residual"] < p["cg_tol"] or s["last_bicgstab_iters"] == p["cg_max_iter"]
