@@ -307,6 +307,7 @@ static int build(Handle* h, const std::vector<double>* xg_in = nullptr) {
   if ((rc = dev_alloc(h, &h->red, h->red_len))) return rc;
   if ((rc = dev_alloc(h, &h->sc, 1))) return rc;
   if ((rc = poisson_setup(h))) return rc;
+  if ((rc = rhs_setup(h))) return rc;
   // module scalars
   h->t = p.t_init;
   h->dPdx = p.dPdx;
@@ -444,6 +445,10 @@ static int sync_scalars_from_device(Handle* h) {
   C3D_CUDA_TRY(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->stream));
   C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   h->dPdx = s.dPdx; h->dPdy = s.dPdy; h->dPdz = s.dPdz;
+  if (s.err) {
+    h->last_error = "a kernel gave up waiting for an asynchronous copy (device state is suspect)";
+    return C3D_ERR_CUDA;
+  }
   return 0;
 }
 
@@ -743,12 +748,15 @@ int c3d_compute_pressure(int id) {
 
 int c3d_set_mode(int id, int poisson_mode, int precond_mode) {
   GET_HANDLE(id);
-  if (poisson_mode != C3D_POISSON_FP64 && poisson_mode != C3D_POISSON_MIXED) RET(h, C3D_ERR_PARAM);
+  if (poisson_mode != C3D_POISSON_FP64 && poisson_mode != C3D_POISSON_MIXED &&
+      poisson_mode != C3D_POISSON_MIXED_UNREFINED) RET(h, C3D_ERR_PARAM);
   if (precond_mode < C3D_PRECOND_NONE || precond_mode > C3D_PRECOND_LEARNED) RET(h, C3D_ERR_PARAM);
-  if (poisson_mode == C3D_POISSON_MIXED) {
+  if (poisson_mode != C3D_POISSON_FP64) {
     int rc = mixed_setup(h);
     if (rc) RET(h, rc);
   }
+  h->refine_sweeps = (poisson_mode == C3D_POISSON_MIXED_UNREFINED) ? 0 : 1;
+  if (poisson_mode == C3D_POISSON_MIXED_UNREFINED) poisson_mode = C3D_POISSON_MIXED;
   h->poisson_mode = poisson_mode;
   h->precond_mode = precond_mode;
   if (h->step_exec) { cudaGraphExecDestroy(h->step_exec); h->step_exec = nullptr; }
@@ -800,8 +808,9 @@ int c3d_profile_kernels(int id, int nrep, double* ms, int nmax) {
   if (!ms || nrep <= 0) return C3D_ERR_PARAM;
   if (h->step_exec) { cudaGraphExecDestroy(h->step_exec); h->step_exec = nullptr; }
   const double dt = h->dt > 0 ? h->dt : 1e-3;
-  double out[9] = {0};
-  for (int c = 0; c < 9; ++c) {
+  const int ncls = 7;
+  double out[ncls] = {0};
+  for (int c = 0; c < ncls; ++c) {
     int rc = 0;
     // one untimed launch, then nrep timed ones
     for (int r = 0; r <= nrep; ++r) {
@@ -809,9 +818,9 @@ int c3d_profile_kernels(int id, int nrep, double* ms, int nmax) {
       switch (c) {
         case 0: rc = launch_rhs_stage(h, 2, dt); break;
         case 1: rc = launch_fill_ghosts3(h, h->Us, h->Vs, h->Ws); break;
-        case 2: case 3: case 4: case 5: case 6: rc = profile_spectral(h, c - 2); break;
-        case 7: rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W); break;
-        case 8: rc = launch_massflow_correction(h, dt); break;
+        case 2: case 3: case 4: rc = profile_spectral(h, c - 2); break;
+        case 5: rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W); break;
+        case 6: rc = launch_massflow_correction(h, dt); break;
       }
       if (rc) RET(h, rc);
     }
@@ -821,7 +830,7 @@ int c3d_profile_kernels(int id, int nrep, double* ms, int nmax) {
     C3D_CUDA_TRY(h, cudaEventElapsedTime(&t, h->ev0, h->ev1));
     out[c] = t / nrep;
   }
-  for (int c = 0; c < 9 && c < nmax; ++c) ms[c] = out[c];
+  for (int c = 0; c < ncls && c < nmax; ++c) ms[c] = out[c];
   RET(h, 0);
 }
 

@@ -79,25 +79,33 @@ struct DevScalars {
   double shift;          // last constant-mass-flow correction
   double qflow;          // last bulk flux (Int_U / norm)
   double dpdx_prev;
-  double pad[2];
+  unsigned long long err;   // sticky kernel error bits (bit 0: a bounded copy wait gave up)
+  double pad;
 };
 
-// FFT plan for one length N = 2^a 3^b
-struct FftPlan {
-  int n = 0;
-  int npass = 0;
-  int radix[16];
-  double2* tw = nullptr;     // exp(-2 pi i m / n), m = 0..n-1 (device)
-};
-
-// precomputed Thomas factor for every (kz', kx) mode: 1/d'_j
-struct TriTable {
-  double* rdp = nullptr;     // [(j*nkzs + kzs)*nkx + m]
-  float* rdp32 = nullptr;    // FP32 copy for the mixed-precision solve
-  double* mult = nullptr;    // [(j*nkzs + kzs)*nkx + m] : DL_j / d'_j
-  float* mult32 = nullptr;
-  double *dl = nullptr, *du = nullptr;   // Dyy(j+1,j), Dyy(j,j+1) (j = 0..Ny-1)
+// Spectral Poisson state: twiddles, Thomas factor tables and spectra for the
+// FP64 path and the FP32 (mixed-precision) path.
+struct SpectralState {
+  double2 *twx = nullptr, *twz = nullptr;    // exp(-2 pi i m / n) (device)
+  float2 *twx32 = nullptr, *twz32 = nullptr;
+  // Thomas factors of every (kx, kz') mode, layout [(m*Ny + j)*nkzs + kz']:
+  // multipliers DL(j)/D'(j) and reciprocal pivots 1/D'(j)
+  double *mult = nullptr, *rdp = nullptr;
+  float *mult32 = nullptr, *rdp32 = nullptr;
+  double *dl = nullptr, *du = nullptr;       // Dyy(j+1, j) and Dyy(j, j+1), j = 0..Ny-1 (0 past the end)
   float *dl32 = nullptr, *du32 = nullptr;
+  // spectra, layout [m][j][k] = [(m*Ny + (j-2))*pz + (k-2)]: one kx slab is
+  // Ny rows of pz complex values (pz*sizeof(complex) a multiple of 16 bytes)
+  double2* spec = nullptr;
+  float2* spec32 = nullptr;
+  int pz64 = 0, pz32 = 0;
+  // FP64 kx = kz = 0 mode of the FP32 path
+  double* linesum = nullptr;                 // per (j, k) line sum of the right-hand side
+  double* phi00 = nullptr;                   // mean solution / (Nx*Nz) per j
+  // cluster decomposition of a kx slab: cs CTAs of jc rows of j, shared
+  // memory row stride rs complex values, nt threads, smem bytes
+  int cs64 = 1, jc64 = 1, rs64 = 0, nt64 = 256, smem64 = 0;
+  int cs32 = 1, jc32 = 1, rs32 = 0, nt32 = 256, smem32 = 0;
 };
 
 struct Params {
@@ -152,12 +160,11 @@ struct Handle {
   double *P_interim = nullptr;
   double *phi1 = nullptr;                                   // stage-1 phi for P
   double *rhsU = nullptr, *rhsV = nullptr, *rhsW = nullptr; // fine-entry rhs arrays
-  double2* spec = nullptr;                                  // spectrum [j][k][m]
   double* red = nullptr;                                    // reduction partials
   int red_len = 0;
   DevScalars* sc = nullptr;
-  FftPlan fx, fz;
-  TriTable tri;
+  SpectralState sp;
+  int refine_sweeps = 1;          // mixed precision: refinement projections per stage
   // state
   double t = 0, dt = 0;
   double dPdx = 0, dPdy = 0, dPdz = 0, Qflow_x_0 = 0;
@@ -179,6 +186,7 @@ struct Handle {
   int64_t graph_solves = 0;       // Poisson solves per captured step
   bool use_graph = true;
   bool write_pinterim = false;   // projection also stores P_interim = phi/dt
+  int rhs_kernel = 0;             // 0: shared-memory tiled stage kernel, 1: per-point kernel
 };
 
 const double* ib_hu(Handle* h);
@@ -217,6 +225,7 @@ enum FieldKind { KIND_U = 0, KIND_V = 1, KIND_W = 2 };
 int launch_fill_ghosts(Handle* h, double* F, FieldKind kind);
 int launch_fill_ghosts3(Handle* h, double* U, double* V, double* W);
 // rhs (k_rhs.cu)
+int rhs_setup(Handle* h);
 int launch_rhs_stage(Handle* h, int stage, double dt);
 int launch_rhs_only(Handle* h, int component);
 // poisson + projection (k_poisson.cu)
@@ -227,7 +236,7 @@ int launch_projection_step(Handle* h, int rk_step, double dt);
 int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, const double* Wi,
                              const double* phi, double dt, double* Uo, double* Vo, double* Wo);
 int rebuild_pressure(Handle* h);
-int profile_spectral(Handle* h, int part);   // 0 div_xfft, 1 zfft fwd, 2 tridiag, 3 zfft inv, 4 xfft inv
+int profile_spectral(Handle* h, int part);   // 0 div_xfft, 1 spectral_yz, 2 xfft inv
 int mixed_setup(Handle* h);
 void mixed_free(Handle* h);
 // mass flow and reductions (k_massflow.cu)

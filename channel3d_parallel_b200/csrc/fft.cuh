@@ -107,4 +107,132 @@ __device__ typename cplx<T>::t* fft_lines(typename cplx<T>::t* buf0, typename cp
   return src;
 }
 
+// Radix-R butterfly on v[0..R-1] (R = 2, 3, 4), forward or inverse.
+template <typename T, bool INV, int R>
+__device__ __forceinline__ void butterfly(typename cplx<T>::t* v) {
+  using C = typename cplx<T>::t;
+  if (R == 4) {
+    C a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    C a2 = cadd(v[1], v[3]), d = csub(v[1], v[3]);
+    C a3;
+    if (INV) { a3.x = -d.y; a3.y = d.x; }
+    else     { a3.x = d.y;  a3.y = -d.x; }
+    v[0] = cadd(a0, a2);
+    v[1] = cadd(a1, a3);
+    v[2] = csub(a0, a2);
+    v[3] = csub(a1, a3);
+  } else if (R == 2) {
+    C a0 = cadd(v[0], v[1]), a1 = csub(v[0], v[1]);
+    v[0] = a0; v[1] = a1;
+  } else {
+    const T s3 = (T)0.86602540378443864676;
+    C s = cadd(v[1], v[2]);
+    C d = csub(v[1], v[2]);
+    C m;
+    m.x = v[0].x - (T)0.5 * s.x;
+    m.y = v[0].y - (T)0.5 * s.y;
+    C id;
+    if (INV) { id.x = -s3 * d.y; id.y = s3 * d.x; }
+    else     { id.x = s3 * d.y;  id.y = -s3 * d.x; }
+    v[0] = cadd(v[0], s);
+    v[1] = cadd(m, id);
+    v[2] = csub(m, id);
+  }
+}
+
+// In-place mixed-radix FFT of shared-memory rows (Cooley-Tukey, no
+// reordering pass).  With radices R_0..R_{P-1} and spans L_p = N/(R_0..R_{p-1}),
+// stage p combines, in every block of L_p elements, the R_p elements
+// q + r*M (M = L_p/R_p, q < M).
+//   forward (decimation in frequency): DFT_R of the R inputs, output s scaled
+//     by w_L^(q*s), w = exp(-2 pi i/L); stages p = 0..P-1; natural-order
+//     input, X[k] left at the digit-reversed position dr(k);
+//   inverse (decimation in time): input r scaled by conj(w_L^(q*r)), inverse
+//     DFT_R; stages p = P-1..0; takes the digit-reversed spectrum back to
+//     natural order, unnormalised.
+// A butterfly reads and writes the same R addresses, so a stage needs one
+// barrier and no staging.  Consecutive threads take consecutive q when runs
+// of q are at least `run` long (conflict-free rows), else consecutive rows
+// (conflict-free when the row stride is chosen for it).
+template <typename T, bool INV, int R>
+__device__ __forceinline__ void ct_stage(typename cplx<T>::t* data, int nrows, int rs,
+                                         const typename cplx<T>::t* tw, int N, int L, int run) {
+  using C = typename cplx<T>::t;
+  const int M = L / R, nb = N / R, tws = N / L;
+  const int total = nrows * nb;
+  const bool rowmajor = M < run;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    int l, bb;
+    if (rowmajor) { bb = t / nrows; l = t - bb * nrows; }
+    else { l = t / nb; bb = t - l * nb; }
+    const int blk = bb / M, q = bb - blk * M;
+    C* p = data + l * rs + blk * L + q;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = p[r * M];
+    if (INV && q > 0) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        C w = tw[q * r * tws];
+        w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    butterfly<T, INV, R>(v);
+    if (!INV && q > 0) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[q * r * tws]);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) p[r * M] = v[r];
+  }
+  __syncthreads();
+}
+
+template <typename T, bool INV>
+__device__ __forceinline__ void ct_stage_any(typename cplx<T>::t* data, int nrows, int rs,
+                                             const typename cplx<T>::t* tw, int N, int L, int R,
+                                             int run) {
+  if (R == 4) ct_stage<T, INV, 4>(data, nrows, rs, tw, N, L, run);
+  else if (R == 2) ct_stage<T, INV, 2>(data, nrows, rs, tw, N, L, run);
+  else ct_stage<T, INV, 3>(data, nrows, rs, tw, N, L, run);
+}
+
+// forward transform of nrows rows; output in digit-reversed order
+template <typename T>
+__device__ void fft_rows_dif(typename cplx<T>::t* data, int nrows, int rs,
+                             const typename cplx<T>::t* tw, const FftPasses& P, int run) {
+  int L = P.n;
+  for (int p = 0; p < P.npass; ++p) {
+    ct_stage_any<T, false>(data, nrows, rs, tw, P.n, L, P.radix[p], run);
+    L /= P.radix[p];
+  }
+}
+
+// inverse transform of nrows digit-reversed rows; output in natural order
+template <typename T>
+__device__ void fft_rows_dit_inv(typename cplx<T>::t* data, int nrows, int rs,
+                                 const typename cplx<T>::t* tw, const FftPasses& P, int run) {
+  int L = 1;
+  for (int p = P.npass - 1; p >= 0; --p) {
+    L *= P.radix[p];
+    ct_stage_any<T, true>(data, nrows, rs, tw, P.n, L, P.radix[p], run);
+  }
+}
+
+// wavenumber index k whose coefficient the forward transform leaves at
+// position pos (inverse of the digit reversal)
+__host__ __device__ inline int dif_position_to_k(int pos, const FftPasses& P) {
+  int k = 0, mult = 1, rem = pos, span = P.n;
+  for (int p = 0; p < P.npass; ++p) {
+    const int M = span / P.radix[p];
+    const int s = rem / M;
+    rem -= s * M;
+    k += s * mult;
+    mult *= P.radix[p];
+    span = M;
+  }
+  return k;
+}
+
 }  // namespace c3d

@@ -1,27 +1,41 @@
 // Pseudo-pressure Poisson solve and projection.
 //
 // solve_poisson_equation (src/poisson.f90:33-101) restated for one GPU:
-//   per y-plane 2-D DFT over (x, z)      -> x real-to-complex FFT of each
-//                                           (j, k) line (pairs of real lines
-//                                           packed as one complex line) and a
-//                                           complex FFT of each (j, kx) z-line;
-//   per (kx, kz) tridiagonal in y        -> Thomas elimination with the
-//                                           factorisation of every mode
-//                                           precomputed once (the matrix is
-//                                           fixed: Dyy + kxx + kzz, with the
-//                                           00-mode pin D(2) *= 3/2);
-//   inverse DFT / (nxp*nzp), real part   -> inverse z FFT, complex-to-real x
-//                                           FFT of the Hermitian half spectrum.
-// divergence (src/differential_operators.f90:54-74) is fused into the first
-// FFT kernel; gradient (:16-52) and the projection update
-// (src/projection.f90:22-46) are one kernel.
+//   per y-plane 2-D DFT over (x, z)   -> k_xfft_fwd: x real-to-complex FFT of
+//                                        each (j, k) line (two real lines per
+//                                        complex FFT), divergence fused in;
+//   per (kx, kz) tridiagonal in y     -> k_spectral_yz: one thread-block
+//   (Zgtsv, :50-75)                      cluster per kx slab; each CTA brings
+//                                        its rows of the slab into shared
+//                                        memory with bulk copies, does the z
+//                                        FFT in place, the Thomas elimination
+//                                        in j (carried across the cluster's
+//                                        CTAs through distributed shared
+//                                        memory), the inverse z FFT, and
+//                                        copies the rows back;
+//   inverse DFT / (nxp*nzp), real     -> k_xfft_inv: complex-to-real x FFT of
+//   part, periodic copies (:78-88)       the Hermitian half spectrum.
+// gradient (src/differential_operators.f90:16-52) and the projection update
+// (src/projection.f90:22-46) are k_grad_sub.
 //
-// Spectrum layout in HBM: spec[((j-2)*Nz + (k-2))*nkx + m], m = 0..Nx/2.
+// Two precisions share the kernels (template T): FP64, and FP32 for the
+// mixed-precision solve, where the kx = kz = 0 wall-normal mode is computed
+// in FP64 (line sums of the right-hand side and an FP64 Thomas solve of the
+// pinned mean mode) and the FP32 result is refined by re-projecting with the
+// FP64 residual div(u).
+//
+// Spectrum layout in HBM: spec[(m*Ny + (j-2))*pz + (k-2)], m = 0..Nx/2: a kx
+// slab is Ny contiguous rows of pz >= Nz complex values.
+#include <cooperative_groups.h>
+
 #include <cmath>
 #include <vector>
 
+#include "bulk.cuh"
 #include "c3d_internal.cuh"
 #include "fft.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace c3d {
 
@@ -38,43 +52,53 @@ static bool make_passes(int n, FftPasses& P) {
   return m == 1 && n >= 2;
 }
 
-static int make_twiddles(Handle* h, int n, double2** out) {
-  std::vector<double2> t(n);
+static FftPasses get_passes(int n) {
+  FftPasses P{};
+  make_passes(n, P);
+  return P;
+}
+
+template <typename C>
+static int make_twiddles(Handle* h, int n, C** out) {
+  std::vector<C> t(n);
   const long double pi = 3.141592653589793238462643383279502884L;
   for (int m = 0; m < n; ++m) {
     long double a = -2.0L * pi * (long double)m / (long double)n;
-    t[m].x = (double)cosl(a);
-    t[m].y = (double)sinl(a);
+    t[m].x = (decltype(t[m].x))cosl(a);
+    t[m].y = (decltype(t[m].y))sinl(a);
   }
-  double2* d = nullptr;
-  int rc = dev_alloc(h, &d, n);
-  if (rc) return rc;
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(d, t.data(), sizeof(double2) * n, cudaMemcpyHostToDevice, h->stream));
-  *out = d;
+  if (*out == nullptr) {
+    int rc = dev_alloc(h, out, n);
+    if (rc) return rc;
+  }
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(*out, t.data(), sizeof(C) * n, cudaMemcpyHostToDevice, h->stream));
   return 0;
 }
 
-// Thomas factorisation of every mode, exactly the no-pivot path of the
-// reference's LAPACK zgtsv call (src/poisson.f90:72): MULT = DL(k)/D(k),
-// D(k+1) -= MULT*DU(k).  Stored: mult_j and 1/d'_j.
+// Thomas factorisation of every mode, the no-pivot path of the reference's
+// LAPACK zgtsv call (src/poisson.f90:72): MULT = DL(k)/D(k), D(k+1) -= MULT*DU(k).
+// Stored: mult_j and 1/d'_j, layout [(m*Ny + j)*nkzs + kz'].
 static int build_tri_table(Handle* h) {
   const Dims& d = h->d;
+  SpectralState& S = h->sp;
   const int Ny = d.Ny, nkx = d.nkx, nkzs = d.nkzs;
   const int64_t nt = (int64_t)Ny * nkzs * nkx;
   std::vector<double> rdp(nt), mult(nt);
   std::vector<float> rdp32(nt), mult32(nt);
-  std::vector<double> D(Ny);
-  std::vector<double> dl(Ny, 0.0), du(Ny, 0.0);
+  std::vector<double> D(Ny), dl(Ny, 0.0), du(Ny, 0.0);
+  std::vector<float> dl32(Ny, 0.0f), du32(Ny, 0.0f);
   for (int jj = 0; jj + 1 < Ny; ++jj) {
     dl[jj] = h->Dl[jj + 3];   // Dyy(j+1, j), j = jj+2
     du[jj] = h->Du[jj + 2];   // Dyy(j, j+1)
+    dl32[jj] = (float)dl[jj];
+    du32[jj] = (float)du[jj];
   }
-  for (int kzs = 0; kzs < nkzs; ++kzs) {
-    for (int m = 0; m < nkx; ++m) {
+  for (int m = 0; m < nkx; ++m) {
+    for (int kzs = 0; kzs < nkzs; ++kzs) {
       for (int jj = 0; jj < Ny; ++jj) D[jj] = (h->Dd[jj + 2] + h->kxx[m]) + h->kzz[kzs];
-      if (m == 0 && kzs == 0) D[0] = 3.0 / 2.0 * D[0];
+      if (m == 0 && kzs == 0) D[0] = 3.0 / 2.0 * D[0];       // src/poisson.f90:69
       for (int jj = 0; jj < Ny; ++jj) {
-        const int64_t o = ((int64_t)jj * nkzs + kzs) * nkx + m;
+        const int64_t o = ((int64_t)m * Ny + jj) * nkzs + kzs;
         double mu = 0.0;
         if (jj + 1 < Ny) {
           mu = dl[jj] / D[jj];
@@ -88,269 +112,403 @@ static int build_tri_table(Handle* h) {
     }
   }
   int rc;
-  if (h->tri.rdp == nullptr) {
-    if ((rc = dev_alloc(h, &h->tri.rdp, nt))) return rc;
-    if ((rc = dev_alloc(h, &h->tri.mult, nt))) return rc;
-    if ((rc = dev_alloc(h, &h->tri.rdp32, nt))) return rc;
-    if ((rc = dev_alloc(h, &h->tri.mult32, nt))) return rc;
-    if ((rc = dev_alloc(h, &h->tri.dl, Ny))) return rc;
-    if ((rc = dev_alloc(h, &h->tri.du, Ny))) return rc;
-    if ((rc = dev_alloc(h, &h->tri.dl32, Ny))) return rc;
-    if ((rc = dev_alloc(h, &h->tri.du32, Ny))) return rc;
+  if (S.rdp == nullptr) {
+    if ((rc = dev_alloc(h, &S.rdp, nt))) return rc;
+    if ((rc = dev_alloc(h, &S.mult, nt))) return rc;
+    if ((rc = dev_alloc(h, &S.rdp32, nt))) return rc;
+    if ((rc = dev_alloc(h, &S.mult32, nt))) return rc;
+    if ((rc = dev_alloc(h, &S.dl, Ny))) return rc;
+    if ((rc = dev_alloc(h, &S.du, Ny))) return rc;
+    if ((rc = dev_alloc(h, &S.dl32, Ny))) return rc;
+    if ((rc = dev_alloc(h, &S.du32, Ny))) return rc;
   }
-  std::vector<float> dl32(Ny), du32(Ny);
-  for (int jj = 0; jj < Ny; ++jj) { dl32[jj] = (float)dl[jj]; du32[jj] = (float)du[jj]; }
   cudaStream_t s = h->stream;
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(h->tri.rdp, rdp.data(), nt * 8, cudaMemcpyHostToDevice, s));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(h->tri.mult, mult.data(), nt * 8, cudaMemcpyHostToDevice, s));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(h->tri.rdp32, rdp32.data(), nt * 4, cudaMemcpyHostToDevice, s));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(h->tri.mult32, mult32.data(), nt * 4, cudaMemcpyHostToDevice, s));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(h->tri.dl, dl.data(), Ny * 8, cudaMemcpyHostToDevice, s));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(h->tri.du, du.data(), Ny * 8, cudaMemcpyHostToDevice, s));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(h->tri.dl32, dl32.data(), Ny * 4, cudaMemcpyHostToDevice, s));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(h->tri.du32, du32.data(), Ny * 4, cudaMemcpyHostToDevice, s));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(S.rdp, rdp.data(), nt * 8, cudaMemcpyHostToDevice, s));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(S.mult, mult.data(), nt * 8, cudaMemcpyHostToDevice, s));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(S.rdp32, rdp32.data(), nt * 4, cudaMemcpyHostToDevice, s));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(S.mult32, mult32.data(), nt * 4, cudaMemcpyHostToDevice, s));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(S.dl, dl.data(), Ny * 8, cudaMemcpyHostToDevice, s));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(S.du, du.data(), Ny * 8, cudaMemcpyHostToDevice, s));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(S.dl32, dl32.data(), Ny * 4, cudaMemcpyHostToDevice, s));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(S.du32, du32.data(), Ny * 4, cudaMemcpyHostToDevice, s));
   return cudaStreamSynchronize(s) == cudaSuccess ? 0 : C3D_ERR_CUDA;
-}
-
-static FftPasses get_passes(int n) {
-  FftPasses P{};
-  make_passes(n, P);
-  return P;
 }
 
 // ---------------------------------------------------------------------------
 // kernel 1: (divergence |) x real-to-complex FFT of (j, k) lines
 // ---------------------------------------------------------------------------
+constexpr int kMaxLines = 16;   // complex lines per block (upper bound)
+constexpr int kLinesX = 4;      // complex x-lines per block
+
+template <typename T>
 struct XfwdArgs {
   Dims d;
   Metric m;
   const double* __restrict__ U;
   const double* __restrict__ V;
   const double* __restrict__ W;
-  const double* __restrict__ rhs;   // FROM_RHS mode input
-  double2* __restrict__ spec;
-  const double2* __restrict__ tw;
+  const double* __restrict__ rhs;             // right-hand side when not fused with div
+  typename cplx<T>::t* __restrict__ spec;
+  const typename cplx<T>::t* __restrict__ tw;
+  double* __restrict__ linesum;               // FP64 line sums (mixed path) or null
   FftPasses P;
-  int lpb;                          // complex lines per block
+  int lpb;
+  int pz;                                     // spectrum row pitch
 };
 
-// one complex line = two real lines r = 2p, 2p+1 with r = (j-2) + Ny*(k-2)
-template <bool FROM_DIV>
-__global__ void __launch_bounds__(256) k_xfft_fwd(XfwdArgs a) {
-  extern __shared__ double2 smem[];
+// real x-line r = (k-2) + Nz*(j-2); its spectrum goes to slab offset
+// (j-2)*pz + (k-2)
+__device__ __forceinline__ void line_info(const Dims& d, int pz, int64_t r, int* j, int* k, int* off) {
+  const int jj = (int)(r / d.Nz), kk = (int)(r - (int64_t)jj * d.Nz);
+  *j = 2 + jj;
+  *k = 2 + kk;
+  *off = jj * pz + kk;
+}
+
+// one complex line = two real lines r = 2p, 2p+1
+template <bool FROM_DIV, typename T>
+__global__ void __launch_bounds__(128) k_xfft_fwd(XfwdArgs<T> a) {
+  using C = typename cplx<T>::t;
+  extern __shared__ __align__(16) unsigned char xf_smem[];
+  __shared__ int s_j[2 * kMaxLines], s_k[2 * kMaxLines], s_off[2 * kMaxLines];
   const Dims& d = a.d;
   const int N = d.Nx;
   const int L = a.lpb;
-  double2* tw = smem;
-  double2* b0 = smem + N;
-  double2* b1 = b0 + L * N;
+  C* tw = reinterpret_cast<C*>(xf_smem);
+  C* b0 = tw + N;
+  C* b1 = b0 + L * N;
+  double* sval = reinterpret_cast<double*>(b1 + L * N);   // FP64 copy (line sums)
   for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = a.tw[t];
   const int64_t nreal = (int64_t)d.Ny * d.Nz;
-  const int64_t p0 = (int64_t)blockIdx.x * L;   // first complex line
-  // gather
+  const int64_t r0 = (int64_t)blockIdx.x * L * 2;
+  if (threadIdx.x < 2 * L) {
+    const int64_t r = r0 + threadIdx.x;
+    int j = -1, k = -1, off = 0;
+    if (r < nreal) line_info(d, a.pz, r, &j, &k, &off);
+    s_j[threadIdx.x] = j;
+    s_k[threadIdx.x] = k;
+    s_off[threadIdx.x] = off;
+  }
+  __syncthreads();
   for (int t = threadIdx.x; t < 2 * L * N; t += blockDim.x) {
-    const int ii = t % N;
-    const int rl = t / N;                       // local real line 0..2L-1
-    const int64_t r = 2 * p0 + rl;
+    const int rl = t / N;
+    const int ii = t - rl * N;
+    const int j = s_j[rl], k = s_k[rl];
     double val = 0.0;
-    if (r < nreal) {
-      const int j = 2 + (int)(r % d.Ny);
-      const int k = 2 + (int)(r / d.Ny);
+    if (j > 0) {
       const int i = 2 + ii;
       if (FROM_DIV) {
-        val = (a.U[idxU(d, i, j, k)] - a.U[idxU(d, i - 1, j, k)]) * a.m.rdx[i]
-            + (a.V[idxV(d, i, j, k)] - a.V[idxV(d, i, j - 1, k)]) * a.m.rdy[j]
-            + (a.W[idxW(d, i, j, k)] - a.W[idxW(d, i, j, k - 1)]) * a.m.rdz[k];
+        const int64_t iu = idxU(d, i, j, k), iv = idxV(d, i, j, k), iw = idxW(d, i, j, k);
+        val = (a.U[iu] - a.U[iu - 1]) * a.m.rdx[i]
+            + (a.V[iv] - a.V[iv - d.nxg]) * a.m.rdy[j]
+            + (a.W[iw] - a.W[iw - (int64_t)d.nxg * d.nyg]) * a.m.rdz[k];
       } else {
         val = a.rhs[idxR(d, i, j, k)];
       }
     }
-    double2& z = b0[(rl >> 1) * N + ii];
-    if (rl & 1) z.y = val; else z.x = val;
+    C& z = b0[(rl >> 1) * N + ii];
+    if (rl & 1) z.y = (T)val; else z.x = (T)val;
+    if (a.linesum) sval[t] = val;
   }
   __syncthreads();
-  double2* res = fft_lines<double, false>(b0, b1, L, tw, a.P);
-  // split the two real transforms, write m = 0..N/2
+  if (a.linesum && threadIdx.x < 2 * L) {   // FP64 line sum in a fixed order
+    const int64_t r = r0 + threadIdx.x;
+    if (r < nreal) {
+      double sum = 0.0;
+      for (int ii = 0; ii < N; ++ii) sum += sval[threadIdx.x * N + ii];
+      a.linesum[r] = sum;
+    }
+  }
+  C* res = fft_lines<T, false>(b0, b1, L, tw, a.P);
   const int nk = d.nkx;
   for (int t = threadIdx.x; t < L * nk; t += blockDim.x) {
-    const int mm = t % nk;
-    const int pl = t / nk;
-    const int64_t r0 = 2 * (p0 + pl);
-    if (r0 >= nreal) continue;
-    const double2 Z = res[pl * N + mm];
-    const double2 Zr = res[pl * N + ((N - mm) % N)];
+    const int pl = t % L;
+    const int mm = t / L;
+    const int64_t ra = r0 + 2 * pl;
+    if (ra >= nreal) continue;
+    const C Z = res[pl * N + mm];
+    const C Zr = res[pl * N + ((N - mm) % N)];
     // A = (Z + conj(Zr))/2,  B = (Z - conj(Zr))/(2i)
-    double2 A, B;
-    A.x = 0.5 * (Z.x + Zr.x);
-    A.y = 0.5 * (Z.y - Zr.y);
-    const double dx_ = Z.x - Zr.x, dy_ = Z.y + Zr.y;
-    B.x = 0.5 * dy_;
-    B.y = -0.5 * dx_;
-    // spectrum index: line r -> (j-2) = r % Ny, (k-2) = r / Ny
-    const int64_t l0 = (r0 % d.Ny) * (int64_t)d.Nz + (r0 / d.Ny);
-    const int64_t r1 = r0 + 1;
-    const int64_t l1 = (r1 % d.Ny) * (int64_t)d.Nz + (r1 / d.Ny);
-    a.spec[l0 * nk + mm] = A;
-    if (r1 < nreal) a.spec[l1 * nk + mm] = B;
+    C A, B;
+    A.x = (T)0.5 * (Z.x + Zr.x);
+    A.y = (T)0.5 * (Z.y - Zr.y);
+    B.x = (T)0.5 * (Z.y + Zr.y);
+    B.y = (T)-0.5 * (Z.x - Zr.x);
+    C* out = a.spec + (int64_t)mm * d.Ny * a.pz;
+    out[s_off[2 * pl]] = A;
+    if (ra + 1 < nreal) out[s_off[2 * pl + 1]] = B;
   }
 }
 
 // ---------------------------------------------------------------------------
-// kernel 2: complex FFT along z of (j, m) lines, in place in the spectrum
+// kernel 2: z FFT, Thomas in y, inverse z FFT of one kx slab per cluster
 // ---------------------------------------------------------------------------
-struct ZfftArgs {
+// rows of j per CTA (register-resident pivots of one column)
+template <typename T>
+__host__ __device__ constexpr int yz_jmax() { return sizeof(T) == 8 ? 32 : 64; }
+constexpr int kYzThreads = 256;
+
+template <typename T>
+struct YzArgs {
   Dims d;
-  double2* spec;
-  const double2* tw;
+  typename cplx<T>::t* __restrict__ spec;
+  const typename cplx<T>::t* __restrict__ tw;
+  const T* __restrict__ rdp;     // 1/D'(j) per (m, j, kz')
+  const T* __restrict__ dl;      // Dyy(j+1, j)
+  const T* __restrict__ du;      // Dyy(j, j+1)
+  unsigned long long* err;       // sticky error bits
   FftPasses P;
-  int mc;   // m values per block
+  int cs;        // CTAs per cluster
+  int jc;        // j rows per CTA
+  int rs;        // shared-memory row stride (complex values)
+  int pz;        // HBM row pitch (complex values)
+  int zero00;    // 1: leave the kx = kz = 0 column to the FP64 mean-mode solve
 };
 
-template <bool INV>
-__global__ void __launch_bounds__(256) k_zfft(ZfftArgs a) {
-  extern __shared__ double2 smem[];
+// CTA c of the cluster owns rows j0 = c*jc .. j0+jn-1 of the slab.  Shared
+// memory: rows [jc][rs] (the z FFT runs along a row), twiddles, DL and DU.
+// The Thomas sweeps walk a column (one kz per thread) down the rows, CTA by
+// CTA: forward elimination from CTA 0 to cs-1, back substitution from cs-1 to
+// 0, each CTA starting from the neighbour row read through distributed
+// shared memory.  After the forward transform column `col` holds wavenumber
+// kz = dif_position_to_k(col); the inverse transform takes that order back.
+template <typename T>
+__global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
+  using C = typename cplx<T>::t;
+  constexpr int JM = yz_jmax<T>();
+  constexpr int kRun = 128 / (int)sizeof(C);   // q-runs that fill a shared-memory wavefront
+  extern __shared__ __align__(128) unsigned char yz_smem[];
+  __shared__ __align__(8) uint64_t bar;
+  cg::cluster_group cl = cg::this_cluster();
   const Dims& d = a.d;
-  const int N = d.Nz, nk = d.nkx, MC = a.mc;
-  double2* tw = smem;
-  double2* b0 = smem + N;
-  double2* b1 = b0 + MC * N;
-  for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = a.tw[t];
-  const int jj = blockIdx.y;
-  const int m0 = blockIdx.x * MC;
-  double2* base = a.spec + (int64_t)jj * d.Nz * nk;
-  for (int t = threadIdx.x; t < MC * N; t += blockDim.x) {
-    const int mm = t % MC;
-    const int kk = t / MC;
-    double2 v = make_double2(0.0, 0.0);
-    if (m0 + mm < nk) v = base[(int64_t)kk * nk + m0 + mm];
-    b0[mm * N + kk] = v;
+  const int cs = a.cs;
+  const int crank = (int)cl.block_rank();
+  const int m = blockIdx.x / cs;
+  const int Ny = d.Ny, Nz = d.Nz, nkzs = d.nkzs;
+  const int RS = a.rs, Jc = a.jc;
+  const int j0 = crank * Jc;
+  const int jn = min(Jc, Ny - j0);             // rows owned by this CTA (>= 1)
+  C* data = reinterpret_cast<C*>(yz_smem);
+  C* tw = data + (size_t)Jc * RS;
+  T* sdl = reinterpret_cast<T*>(tw + Nz);
+  T* sdu = sdl + Ny;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  C* g = a.spec + ((int64_t)m * Ny + j0) * a.pz;
+  const unsigned rowbytes = (unsigned)(a.pz * sizeof(C));
+
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
   }
   __syncthreads();
-  double2* res = fft_lines<double, INV>(b0, b1, MC, tw, a.P);
-  for (int t = threadIdx.x; t < MC * N; t += blockDim.x) {
-    const int mm = t % MC;
-    const int kk = t / MC;
-    if (m0 + mm < nk) base[(int64_t)kk * nk + m0 + mm] = res[mm * N + kk];
+  if (tid < 32) {
+    if (tid == 0) mbar_arrive_expect_tx(&bar, rowbytes * (unsigned)jn);
+    __syncwarp();
+    for (int r = tid; r < jn; r += 32) bulk_load(data + (size_t)r * RS, g + (int64_t)r * a.pz, rowbytes, &bar);
+  }
+  for (int t = tid; t < Nz; t += nt) tw[t] = a.tw[t];
+  for (int t = tid; t < Ny; t += nt) { sdl[t] = a.dl[t]; sdu[t] = a.du[t]; }
+
+  // pivots of this thread's column for rows j0-1 .. j0+jn-1 (one column per
+  // thread when Nz <= blockDim; otherwise reloaded per column below)
+  const T* rdp_m = a.rdp + (int64_t)m * Ny * nkzs;
+  const bool one_col = Nz <= nt;
+  T rdv[JM];
+  T rdm1 = (T)0;
+  auto load_pivots = [&](int col) {
+    const int kz = dif_position_to_k(col, a.P);
+    const int kzs = kz <= Nz - kz ? kz : Nz - kz;
+#pragma unroll
+    for (int jl = 0; jl < JM; ++jl)
+      rdv[jl] = jl < jn ? __ldg(rdp_m + (int64_t)(j0 + jl) * nkzs + kzs) : (T)0;
+    rdm1 = j0 > 0 ? __ldg(rdp_m + (int64_t)(j0 - 1) * nkzs + kzs) : (T)0;
+  };
+  if (one_col && tid < Nz) load_pivots(tid);
+
+  const bool loaded = mbar_wait(&bar, 0, kWaitCycles);
+  if (!loaded) atomicOr(a.err, 1ull);
+  __syncthreads();
+
+  fft_rows_dif<T>(data, jn, RS, tw, a.P, kRun);
+
+  // forward elimination B(j) -= DL(j-1)/D'(j-1) * B(j-1)
+  for (int c = 0; c < cs; ++c) {
+    if (crank == c) {
+      const C* up = c > 0 ? cl.map_shared_rank(data, c - 1) : nullptr;
+      for (int col = tid; col < Nz; col += nt) {
+        if (!one_col) load_pivots(col);
+        C prev = c > 0 ? up[(size_t)(Jc - 1) * RS + col] : data[col];
+#pragma unroll
+        for (int jl = 0; jl < JM; ++jl) {
+          if (jl < jn && (c > 0 || jl > 0)) {
+            const int j = j0 + jl;
+            const T mu = sdl[j - 1] * (jl == 0 ? rdm1 : rdv[jl > 0 ? jl - 1 : 0]);
+            C b = data[jl * RS + col];
+            b.x = b.x - mu * prev.x;
+            b.y = b.y - mu * prev.y;
+            data[jl * RS + col] = b;
+            prev = b;
+          }
+        }
+      }
+    }
+    cl.sync();
+  }
+  // back substitution x(j) = (B(j) - DU(j) x(j+1)) / D'(j), DU(Ny-1) = 0
+  for (int c = cs - 1; c >= 0; --c) {
+    if (crank == c) {
+      const C* dn = c < cs - 1 ? cl.map_shared_rank(data, c + 1) : nullptr;
+      for (int col = tid; col < Nz; col += nt) {
+        if (!one_col) load_pivots(col);
+        C xn = c < cs - 1 ? dn[col] : C{(T)0, (T)0};
+#pragma unroll
+        for (int jl = JM - 1; jl >= 0; --jl) {
+          if (jl < jn) {
+            const T u = sdu[j0 + jl];
+            C b = data[jl * RS + col];
+            b.x = (b.x - u * xn.x) * rdv[jl];
+            b.y = (b.y - u * xn.y) * rdv[jl];
+            data[jl * RS + col] = b;
+            xn = b;
+          }
+        }
+        if (a.zero00 && m == 0 && col == 0)
+          for (int jl = 0; jl < jn; ++jl) data[jl * RS] = C{(T)0, (T)0};
+      }
+    }
+    cl.sync();
+  }
+
+  fft_rows_dit_inv<T>(data, jn, RS, tw, a.P, kRun);
+
+  fence_async_shared();
+  __syncthreads();
+  if (tid < 32) {
+    if (loaded) {
+      for (int r = tid; r < jn; r += 32) bulk_store(g + (int64_t)r * a.pz, data + (size_t)r * RS, rowbytes);
+      bulk_commit();
+      bulk_wait_read_all();
+    } else {
+      // the rows never arrived: let the copies in flight finish before exit
+      mbar_wait(&bar, 0, kWaitCycles);
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
-// kernel 3: Thomas solve in y for every (kz, m) mode
+// FP64 kx = kz = 0 mode of the mixed path: plane sums and the pinned solve
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_tridiag(Dims d, double2* __restrict__ spec,
-                                                 const double* __restrict__ mult,
-                                                 const double* __restrict__ rdp,
-                                                 const double* __restrict__ du) {
-  const int nk = d.nkx;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;   // kz*nk + m
-  if (q >= d.Nz * nk) return;
-  const int kz = q / nk, m = q - kz * nk;
-  const int kzs = kz <= d.Nz - kz ? kz : d.Nz - kz;
-  const int64_t sstride = (int64_t)d.Nz * nk;
-  const int64_t tstride = (int64_t)d.nkzs * nk;
-  const int64_t t0 = (int64_t)kzs * nk + m;
-  double2* s = spec + q;
-  // forward elimination: B(j+1) -= MULT_j * B(j)
-  double2 prev = s[0];
-  for (int jj = 1; jj < d.Ny; ++jj) {
-    const double mu = __ldg(mult + (jj - 1) * tstride + t0);
-    double2 b = s[jj * sstride];
-    b.x = b.x - mu * prev.x;
-    b.y = b.y - mu * prev.y;
-    s[jj * sstride] = b;
-    prev = b;
+__global__ void k_mode00(Dims d, const double* __restrict__ linesum, const double* __restrict__ mult,
+                         const double* __restrict__ rdp, const double* __restrict__ du,
+                         double* __restrict__ phi00) {
+  extern __shared__ double b00[];
+  const int Ny = d.Ny, Nz = d.Nz, nkzs = d.nkzs;
+  for (int j = threadIdx.x; j < Ny; j += blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < Nz; ++k) s += linesum[(int64_t)j * Nz + k];   // fixed order
+    b00[j] = s;
   }
-  // back substitution: x(j) = (B(j) - DU(j) x(j+1)) / D'(j)
-  const int jl = d.Ny - 1;
-  double rd = __ldg(rdp + jl * tstride + t0);
-  double2 xn;
-  xn.x = prev.x * rd;
-  xn.y = prev.y * rd;
-  s[jl * sstride] = xn;
-  for (int jj = jl - 1; jj >= 0; --jj) {
-    const double u = __ldg(du + jj);
-    rd = __ldg(rdp + jj * tstride + t0);
-    double2 b = s[jj * sstride];
-    b.x = (b.x - u * xn.x) * rd;
-    b.y = (b.y - u * xn.y) * rd;
-    s[jj * sstride] = b;
-    xn = b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // mode (0, 0): table entries (m = 0, kz' = 0)
+    for (int j = 1; j < Ny; ++j) b00[j] = b00[j] - mult[(int64_t)(j - 1) * nkzs] * b00[j - 1];
+    double xn = b00[Ny - 1] * rdp[(int64_t)(Ny - 1) * nkzs];
+    b00[Ny - 1] = xn;
+    for (int j = Ny - 2; j >= 0; --j) {
+      xn = (b00[j] - du[j] * xn) * rdp[(int64_t)j * nkzs];
+      b00[j] = xn;
+    }
   }
+  __syncthreads();
+  const double sd = (double)d.Nx * (double)d.Nz;
+  for (int j = threadIdx.x; j < Ny; j += blockDim.x) phi00[j] = b00[j] / sd;
 }
 
 // ---------------------------------------------------------------------------
-// kernel 4: x complex-to-real inverse FFT, write phi into rhs_p layout
+// kernel 3: x complex-to-real inverse FFT, write phi into rhs_p layout
 // ---------------------------------------------------------------------------
+template <typename T>
 struct XinvArgs {
   Dims d;
-  const double2* __restrict__ spec;
-  const double2* __restrict__ tw;
-  double* __restrict__ rhs;    // output phi (rhs_p layout)
-  double* __restrict__ phi1;   // optional second copy (P side effect)
+  const typename cplx<T>::t* __restrict__ spec;
+  const typename cplx<T>::t* __restrict__ tw;
+  double* __restrict__ rhs;      // output phi (rhs_p layout)
+  double* __restrict__ phi1;     // optional second copy (P side effect)
+  const double* __restrict__ phi00;   // FP64 mean mode added to the output (mixed path)
+  int accumulate;                // 1: rhs += result (refinement)
   FftPasses P;
   int lpb;
-  double scale_div;            // nxp*nzp
+  int pz;                        // spectrum row pitch
+  double scale_div;              // nxp*nzp
 };
 
-__global__ void __launch_bounds__(256) k_xfft_inv(XinvArgs a) {
-  extern __shared__ double2 smem[];
+template <typename T>
+__global__ void __launch_bounds__(128) k_xfft_inv(XinvArgs<T> a) {
+  using C = typename cplx<T>::t;
+  extern __shared__ __align__(16) unsigned char xi_smem[];
+  __shared__ int s_j[2 * kMaxLines], s_k[2 * kMaxLines], s_off[2 * kMaxLines];
   const Dims& d = a.d;
   const int N = d.Nx, L = a.lpb, nk = d.nkx;
-  double2* tw = smem;
-  double2* b0 = smem + N;
-  double2* b1 = b0 + L * N;
+  C* tw = reinterpret_cast<C*>(xi_smem);
+  C* b0 = tw + N;
+  C* b1 = b0 + L * N;
   for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = a.tw[t];
   const int64_t nreal = (int64_t)d.Ny * d.Nz;
-  const int64_t p0 = (int64_t)blockIdx.x * L;
-  // build Z = A + iB on the full circle from the two half spectra
+  const int64_t r0 = (int64_t)blockIdx.x * L * 2;
+  if (threadIdx.x < 2 * L) {
+    const int64_t r = r0 + threadIdx.x;
+    int j = -1, k = -1, off = 0;
+    if (r < nreal) line_info(d, a.pz, r, &j, &k, &off);
+    s_j[threadIdx.x] = j;
+    s_k[threadIdx.x] = k;
+    s_off[threadIdx.x] = off;
+  }
+  __syncthreads();
+  // Z = A + iB on the full circle from the two half spectra
   for (int t = threadIdx.x; t < L * nk; t += blockDim.x) {
-    const int mm = t % nk;
-    const int pl = t / nk;
-    const int64_t r0 = 2 * (p0 + pl), r1 = r0 + 1;
-    double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
-    if (r0 < nreal) {
-      const int64_t l0 = (r0 % d.Ny) * (int64_t)d.Nz + (r0 / d.Ny);
-      A = a.spec[l0 * nk + mm];
-    }
-    if (r1 < nreal) {
-      const int64_t l1 = (r1 % d.Ny) * (int64_t)d.Nz + (r1 / d.Ny);
-      B = a.spec[l1 * nk + mm];
-    }
-    if (mm == 0 || 2 * mm == N) { A.y = 0.0; B.y = 0.0; }   // Hermitian projection
-    double2 Z;
+    const int pl = t % L;
+    const int mm = t / L;
+    const int64_t ra = r0 + 2 * pl;
+    const C* in = a.spec + (int64_t)mm * d.Ny * a.pz;
+    C A = C{(T)0, (T)0}, B = C{(T)0, (T)0};
+    if (ra < nreal) A = in[s_off[2 * pl]];
+    if (ra + 1 < nreal) B = in[s_off[2 * pl + 1]];
+    if (mm == 0 || 2 * mm == N) { A.y = (T)0; B.y = (T)0; }   // Hermitian projection
+    C Z;
     Z.x = A.x - B.y;
     Z.y = A.y + B.x;
     b0[pl * N + mm] = Z;
     if (mm > 0 && 2 * mm < N) {
-      double2 Zc;
+      C Zc;
       Zc.x = A.x + B.y;
       Zc.y = -A.y + B.x;
       b0[pl * N + (N - mm)] = Zc;
     }
   }
   __syncthreads();
-  double2* res = fft_lines<double, true>(b0, b1, L, tw, a.P);
+  C* res = fft_lines<T, true>(b0, b1, L, tw, a.P);
   const double sd = a.scale_div;
   for (int t = threadIdx.x; t < 2 * L * N; t += blockDim.x) {
-    const int ii = t % N;
     const int rl = t / N;
-    const int64_t r = 2 * p0 + rl;
-    if (r >= nreal) continue;
-    const double2 z = res[(rl >> 1) * N + ii];
-    const double v = ((rl & 1) ? z.y : z.x) / sd;
-    const int j = 2 + (int)(r % d.Ny);
-    const int k = 2 + (int)(r / d.Ny);
+    const int ii = t - rl * N;
+    const int j = s_j[rl], k = s_k[rl];
+    if (j < 0) continue;
+    const C z = res[(rl >> 1) * N + ii];
+    double v = (double)((rl & 1) ? z.y : z.x) / sd;
+    if (a.phi00) v += a.phi00[j - 2];
     const int i = 2 + ii;
+    const int64_t o = idxR(d, i, j, k);
+    if (a.accumulate) v += a.rhs[o];
     // apply_periodic_xz_centers (src/poisson.f90:106-125): x plane nxg-1 and
     // z plane nzp+2 duplicate plane 2
-    a.rhs[idxR(d, i, j, k)] = v;
+    a.rhs[o] = v;
     if (i == 2) a.rhs[idxR(d, d.Nx + 2, j, k)] = v;
     if (k == 2) {
       a.rhs[idxR(d, i, j, d.Nz + 2)] = v;
       if (i == 2) a.rhs[idxR(d, d.Nx + 2, j, d.Nz + 2)] = v;
     }
     if (a.phi1) {
-      a.phi1[idxR(d, i, j, k)] = v;
+      a.phi1[o] = v;
       if (i == 2) a.phi1[idxR(d, d.Nx + 2, j, k)] = v;
       if (k == 2) {
         a.phi1[idxR(d, i, j, d.Nz + 2)] = v;
@@ -363,85 +521,133 @@ __global__ void __launch_bounds__(256) k_xfft_inv(XinvArgs a) {
 // ---------------------------------------------------------------------------
 // host drivers
 // ---------------------------------------------------------------------------
-static const int kLinesX = 8;   // complex x-lines per block
-static const int kLinesZ = 8;   // z-lines per block
+template <typename T>
+static int xfft_smem(const Dims& d, bool linesum) {
+  return (int)(sizeof(typename cplx<T>::t) * (d.Nx + 2 * kLinesX * d.Nx) +
+               (linesum ? sizeof(double) * 2 * kLinesX * d.Nx : 0));
+}
 
-static int set_fft_smem_limits(Handle* h) {
+// cluster decomposition of a kx slab: smallest power-of-two cluster whose
+// CTAs own at most yz_jmax rows and fit two CTAs per SM (16-CTA clusters may
+// use up to one SM each).  Row stride: FP64 rows of 16-byte values padded to
+// rs = 1 (mod 8) make row-to-row steps conflict-free; FP32 rows stay 16-byte
+// aligned for the bulk copies (rs even) with rs = 2 (mod 4).
+template <typename T>
+static bool choose_cluster(const Dims& d, int pz, int& cs, int& jc, int& rs, int& nt, int& smem) {
+  const size_t esz = sizeof(typename cplx<T>::t);
+  rs = pz;
+  if (sizeof(T) == 8) { while (rs % 8 != 1) ++rs; }
+  else { while (rs % 4 != 2) ++rs; }
+  nt = kYzThreads;
+  for (cs = 1; cs <= 16; cs *= 2) {
+    jc = (d.Ny + cs - 1) / cs;
+    if ((cs - 1) * jc >= d.Ny) continue;      // every CTA must own a row
+    if (jc > yz_jmax<T>()) continue;
+    const size_t bytes = esz * ((size_t)jc * rs + d.Nz) + 2 * sizeof(T) * d.Ny;
+    if (bytes <= 112 * 1024 || (cs == 16 && bytes <= 224 * 1024)) {
+      smem = (int)bytes;
+      return true;
+    }
+  }
+  return false;
+}
+
+template <typename T>
+static int launch_yz(Handle* h, typename cplx<T>::t* spec, const typename cplx<T>::t* tw, const T* rdp,
+                     const T* dl, const T* du, int cs, int jc, int rs, int pz, int nt, int smem,
+                     int zero00) {
   const Dims& d = h->d;
-  const int smx = (int)(sizeof(double2) * (d.Nx + 2 * kLinesX * d.Nx));
-  const int smz = (int)(sizeof(double2) * (d.Nz + 2 * kLinesZ * d.Nz));
-  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_xfft_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
-  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_xfft_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
-  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_xfft_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
-  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_zfft<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smz));
-  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_zfft<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smz));
+  YzArgs<T> a{};
+  a.d = d; a.spec = spec; a.tw = tw; a.rdp = rdp; a.dl = dl; a.du = du;
+  a.err = &h->sc->err;
+  a.P = get_passes(d.Nz); a.cs = cs; a.jc = jc; a.rs = rs; a.pz = pz; a.zero00 = zero00;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)(cs * d.nkx), 1, 1);
+  cfg.blockDim = dim3((unsigned)nt, 1, 1);
+  cfg.dynamicSmemBytes = (size_t)smem;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  C3D_CUDA_TRY(h, cudaLaunchKernelEx(&cfg, k_spectral_yz<T>, a));
+  C3D_LAUNCH_CHECK(h);
   return 0;
 }
 
-static int run_spectral_parts(Handle* h, bool from_div, const double* U, const double* V,
-                              const double* W, double* rhs, double* phi1, int only);
+template <typename T>
+static int set_limits(Handle* h, int smem_yz, int cs) {
+  const Dims& d = h->d;
+  const int smx = xfft_smem<T>(d, sizeof(T) == 4);
+  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_xfft_fwd<true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
+  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_xfft_fwd<false, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
+  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_xfft_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
+  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_spectral_yz<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_yz));
+  if (cs > 8)
+    C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_spectral_yz<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  return 0;
+}
 
-static int run_spectral(Handle* h, bool from_div, const double* U, const double* V,
-                        const double* W, double* rhs, double* phi1) {
-  return run_spectral_parts(h, from_div, U, V, W, rhs, phi1, -1);
+// parts: bit0 x FFT, bit1 yz, bit2 inverse x FFT
+template <typename T>
+static int run_spectral_t(Handle* h, bool from_div, const double* U, const double* V, const double* W,
+                          const double* rhs_in, double* out, double* phi1, int accumulate, int parts) {
+  const Dims& d = h->d;
+  SpectralState& S = h->sp;
+  cudaStream_t s = h->stream;
+  const bool f32 = sizeof(T) == 4;
+  using C = typename cplx<T>::t;
+  C* spec;
+  const C *twx, *twz;
+  const T *rdp, *dl, *du;
+  int cs, jc, rs, pz, nt, smem;
+  if (f32) {
+    spec = (C*)S.spec32; twx = (const C*)S.twx32; twz = (const C*)S.twz32;
+    rdp = (const T*)S.rdp32; dl = (const T*)S.dl32; du = (const T*)S.du32;
+    cs = S.cs32; jc = S.jc32; rs = S.rs32; pz = S.pz32; nt = S.nt32; smem = S.smem32;
+  } else {
+    spec = (C*)S.spec; twx = (const C*)S.twx; twz = (const C*)S.twz;
+    rdp = (const T*)S.rdp; dl = (const T*)S.dl; du = (const T*)S.du;
+    cs = S.cs64; jc = S.jc64; rs = S.rs64; pz = S.pz64; nt = S.nt64; smem = S.smem64;
+  }
+  const FftPasses Px = get_passes(d.Nx);
+  const int64_t npairs = ((int64_t)d.Ny * d.Nz + 1) / 2;
+  const unsigned nbx = (unsigned)((npairs + kLinesX - 1) / kLinesX);
+  const int smx = xfft_smem<T>(d, f32);
+  if (parts & 1) {
+    XfwdArgs<T> a{};
+    a.d = d; a.m = h->m; a.U = U; a.V = V; a.W = W; a.rhs = rhs_in;
+    a.spec = spec; a.tw = twx; a.P = Px; a.lpb = kLinesX; a.pz = pz;
+    a.linesum = f32 ? S.linesum : nullptr;
+    if (from_div) k_xfft_fwd<true, T><<<nbx, 128, smx, s>>>(a);
+    else k_xfft_fwd<false, T><<<nbx, 128, smx, s>>>(a);
+    C3D_LAUNCH_CHECK(h);
+    if (f32) {
+      k_mode00<<<1, 256, sizeof(double) * d.Ny, s>>>(d, S.linesum, S.mult, S.rdp, S.du, S.phi00);
+      C3D_LAUNCH_CHECK(h);
+    }
+  }
+  if (parts & 2) {
+    int rc = launch_yz<T>(h, spec, twz, rdp, dl, du, cs, jc, rs, pz, nt, smem, f32 ? 1 : 0);
+    if (rc) return rc;
+  }
+  if (parts & 4) {
+    XinvArgs<T> a{};
+    a.d = d; a.spec = spec; a.tw = twx; a.rhs = out; a.phi1 = phi1;
+    a.phi00 = f32 ? S.phi00 : nullptr; a.accumulate = accumulate;
+    a.P = Px; a.lpb = kLinesX; a.pz = pz; a.scale_div = (double)d.Nx * (double)d.Nz;
+    k_xfft_inv<T><<<nbx, 128, smx, s>>>(a);
+    C3D_LAUNCH_CHECK(h);
+  }
+  if (parts == 7) h->stats.poisson_solves++;
+  return 0;
 }
 
 int profile_spectral(Handle* h, int part) {
-  return run_spectral_parts(h, true, h->Us, h->Vs, h->Ws, h->rhs_p, nullptr, part);
-}
-
-static int run_spectral_parts(Handle* h, bool from_div, const double* U, const double* V,
-                              const double* W, double* rhs, double* phi1, int only) {
-  const Dims& d = h->d;
-  cudaStream_t s = h->stream;
-  FftPasses Px = get_passes(d.Nx), Pz = get_passes(d.Nz);
-  const int64_t npairs = ((int64_t)d.Ny * d.Nz + 1) / 2;
-  // 1: div | rhs -> x FFT
-  if (only < 0 || only == 0) {
-    XfwdArgs a{};
-    a.d = d; a.m = h->m; a.U = U; a.V = V; a.W = W; a.rhs = rhs;
-    a.spec = h->spec; a.tw = h->fx.tw; a.P = Px; a.lpb = kLinesX;
-    const size_t sm = sizeof(double2) * (d.Nx + 2 * kLinesX * d.Nx);
-    const unsigned nb = (unsigned)((npairs + kLinesX - 1) / kLinesX);
-    if (from_div) {
-      k_xfft_fwd<true><<<nb, 128, sm, s>>>(a);
-    } else {
-      k_xfft_fwd<false><<<nb, 128, sm, s>>>(a);
-    }
-    C3D_LAUNCH_CHECK(h);
-  }
-  // 2: z FFT forward
-  ZfftArgs za{};
-  za.d = d; za.spec = h->spec; za.tw = h->fz.tw; za.P = Pz; za.mc = kLinesZ;
-  const size_t smz = sizeof(double2) * (d.Nz + 2 * kLinesZ * d.Nz);
-  dim3 gz((d.nkx + kLinesZ - 1) / kLinesZ, d.Ny);
-  if (only < 0 || only == 1) {
-    k_zfft<false><<<gz, 128, smz, s>>>(za);
-    C3D_LAUNCH_CHECK(h);
-  }
-  // 3: tridiagonal
-  if (only < 0 || only == 2) {
-    const int nm = d.Nz * d.nkx;
-    k_tridiag<<<(nm + 127) / 128, 128, 0, s>>>(d, h->spec, h->tri.mult, h->tri.rdp, h->tri.du);
-    C3D_LAUNCH_CHECK(h);
-  }
-  // 4: z FFT inverse
-  if (only < 0 || only == 3) {
-    k_zfft<true><<<gz, 128, smz, s>>>(za);
-    C3D_LAUNCH_CHECK(h);
-  }
-  // 5: x inverse FFT -> phi
-  if (only < 0 || only == 4) {
-    XinvArgs a{};
-    a.d = d; a.spec = h->spec; a.tw = h->fx.tw; a.rhs = rhs; a.phi1 = phi1;
-    a.P = Px; a.lpb = kLinesX; a.scale_div = (double)d.Nx * (double)d.Nz;
-    const size_t sm = sizeof(double2) * (d.Nx + 2 * kLinesX * d.Nx);
-    const unsigned nb = (unsigned)((npairs + kLinesX - 1) / kLinesX);
-    k_xfft_inv<<<nb, 128, sm, s>>>(a);
-    C3D_LAUNCH_CHECK(h);
-  }
-  if (only < 0) h->stats.poisson_solves++;
-  return 0;
+  return run_spectral_t<double>(h, true, h->Us, h->Vs, h->Ws, nullptr, h->rhs_p, nullptr, 0, 1 << part);
 }
 
 // divergence only (fine entry and diagnostics): rhs_p = div(U,V,W) incl. the
@@ -472,9 +678,10 @@ int launch_divergence(Handle* h, const double* U, const double* V, const double*
   return 0;
 }
 
+// in place on an rhs_p-shaped array; always FP64 (fine entry, IB operators)
 int launch_poisson_solve(Handle* h, double* rhs, int rk_step, double dt) {
-  (void)dt;
-  int rc = run_spectral(h, false, nullptr, nullptr, nullptr, rhs, rk_step == 1 ? h->phi1 : nullptr);
+  int rc = run_spectral_t<double>(h, false, nullptr, nullptr, nullptr, rhs, rhs,
+                                  rk_step == 1 ? h->phi1 : nullptr, 0, 7);
   if (rc) return rc;
   if (rk_step == 1) { h->P_pending = true; h->P_pending_dt = dt; }
   return 0;
@@ -540,12 +747,33 @@ int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, cons
 }
 
 // compute_non_IB_projection with U* in (Us,Vs,Ws) and the result in (U,V,W),
-// ghosts filled: one div+FFT, z FFT, Thomas, z iFFT, iFFT, gradient, BC.
+// ghosts filled.  FP64: one solve.  Mixed: an FP32 solve, then refinement
+// sweeps that solve again for the FP64 residual div(U) and re-project U* with
+// the accumulated potential.
 int launch_projection_step(Handle* h, int rk_step, double dt) {
-  int rc = run_spectral(h, true, h->Us, h->Vs, h->Ws, h->rhs_p,
-                        (rk_step == 1 && h->ib == nullptr) ? h->phi1 : nullptr);
-  if (rc) return rc;
-  if (rk_step == 1 && h->ib == nullptr) { h->P_pending = true; h->P_pending_dt = dt; }
+  const bool stage1 = (rk_step == 1 && h->ib == nullptr);
+  int rc;
+  if (h->poisson_mode == C3D_POISSON_MIXED) {
+    const int sweeps = h->refine_sweeps;
+    rc = run_spectral_t<float>(h, true, h->Us, h->Vs, h->Ws, nullptr, h->rhs_p,
+                               (stage1 && sweeps == 0) ? h->phi1 : nullptr, 0, 7);
+    if (rc) return rc;
+    for (int sw = 1; sw <= sweeps; ++sw) {
+      rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W);
+      if (rc) return rc;
+      rc = launch_fill_ghosts3(h, h->U, h->V, h->W);
+      if (rc) return rc;
+      rc = run_spectral_t<float>(h, true, h->U, h->V, h->W, nullptr, h->rhs_p,
+                                 (stage1 && sw == sweeps) ? h->phi1 : nullptr, 1, 7);
+      if (rc) return rc;
+    }
+    h->stats.refinement_sweeps = sweeps;
+  } else {
+    rc = run_spectral_t<double>(h, true, h->Us, h->Vs, h->Ws, nullptr, h->rhs_p,
+                                stage1 ? h->phi1 : nullptr, 0, 7);
+    if (rc) return rc;
+  }
+  if (stage1) { h->P_pending = true; h->P_pending_dt = dt; }
   rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W);
   if (rc) return rc;
   return launch_fill_ghosts3(h, h->U, h->V, h->W);
@@ -581,6 +809,7 @@ int rebuild_pressure(Handle* h) {
 
 int poisson_setup(Handle* h) {
   const Dims& d = h->d;
+  SpectralState& S = h->sp;
   FftPasses P;
   if (!make_passes(d.Nx, P) || !make_passes(d.Nz, P)) {
     h->last_error = "nxp and nzp must be products of 2 and 3 (nx_global-2, nz_global-2)";
@@ -590,21 +819,47 @@ int poisson_setup(Handle* h) {
     h->last_error = "nx_global must be even";
     return C3D_ERR_PARAM;
   }
+  if (2 * kLinesX * d.Nx > 16 * 1024 || d.Nx > 4096) {
+    h->last_error = "nx_global too large for the x FFT kernels";
+    return C3D_ERR_UNSUPPORTED;
+  }
   int rc;
-  if (h->spec == nullptr) {
-    h->fx.n = d.Nx;
-    h->fz.n = d.Nz;
-    if ((rc = make_twiddles(h, d.Nx, &h->fx.tw))) return rc;
-    if ((rc = make_twiddles(h, d.Nz, &h->fz.tw))) return rc;
-    const int64_t ns = (int64_t)d.Ny * d.Nz * d.nkx;
-    if ((rc = dev_alloc(h, &h->spec, ns))) return rc;
-    if ((rc = set_fft_smem_limits(h))) return rc;
+  if (S.spec == nullptr) {
+    S.pz64 = d.Nz;
+    if (!choose_cluster<double>(d, S.pz64, S.cs64, S.jc64, S.rs64, S.nt64, S.smem64)) {
+      h->last_error = "ny_global too large for one 16-CTA cluster per kx slab";
+      return C3D_ERR_UNSUPPORTED;
+    }
+    if ((rc = make_twiddles(h, d.Nx, &S.twx))) return rc;
+    if ((rc = make_twiddles(h, d.Nz, &S.twz))) return rc;
+    const int64_t ns = (int64_t)d.Ny * S.pz64 * d.nkx;
+    if ((rc = dev_alloc(h, &S.spec, ns))) return rc;
+    if ((rc = set_limits<double>(h, S.smem64, S.cs64))) return rc;
   }
   return build_tri_table(h);
 }
 
+int mixed_setup(Handle* h) {
+  const Dims& d = h->d;
+  SpectralState& S = h->sp;
+  if (S.spec32 != nullptr) return 0;
+  S.pz32 = d.Nz + (d.Nz & 1);
+  if (!choose_cluster<float>(d, S.pz32, S.cs32, S.jc32, S.rs32, S.nt32, S.smem32)) {
+    h->last_error = "ny_global too large for the FP32 cluster decomposition";
+    return C3D_ERR_UNSUPPORTED;
+  }
+  int rc;
+  if ((rc = make_twiddles(h, d.Nx, &S.twx32))) return rc;
+  if ((rc = make_twiddles(h, d.Nz, &S.twz32))) return rc;
+  const int64_t ns = (int64_t)d.Ny * S.pz32 * d.nkx;
+  if ((rc = dev_alloc(h, &S.spec32, ns))) return rc;
+  if ((rc = dev_alloc(h, &S.linesum, (int64_t)d.Ny * d.Nz))) return rc;
+  if ((rc = dev_alloc(h, &S.phi00, d.Ny))) return rc;
+  if ((rc = set_limits<float>(h, S.smem32, S.cs32))) return rc;
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return 0;
+}
 
-int mixed_setup(Handle* h) { (void)h; return 0; }
 void mixed_free(Handle* h) { (void)h; }
 
 }  // namespace c3d

@@ -174,6 +174,156 @@ __global__ void __launch_bounds__(256) k_rhs(RhsArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Tiled stage kernel: a CTA owns a TX x TY tile of (i, j) columns and marches
+// over a run of KC z planes, keeping planes k-1, k, k+1 of U, V and W (tile
+// plus a one-cell halo in x and y) in a rolling shared-memory window.  Every
+// field value is read from HBM once per CTA (halo overhead (TX+2)(TY+2)/(TX*TY));
+// the arithmetic is that of k_rhs.
+// ---------------------------------------------------------------------------
+constexpr int TX = 32, TY = 8, KC = 32;
+constexpr int PX = TX + 2, PY = TY + 2, PN = PX * PY;
+constexpr int NSLOT = 8;   // planes k-1, k, k+1 in use, k+2..k+4 in flight
+constexpr int AHEAD = 3;   // planes issued beyond k+1
+
+__device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  const int n = valid ? 8 : 0;   // src-size 0 zero-fills the destination
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <int MODE>
+__global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
+  extern __shared__ double rhs_smem[];
+  double (*sU)[PN] = reinterpret_cast<double (*)[PN]>(rhs_smem);
+  double (*sV)[PN] = reinterpret_cast<double (*)[PN]>(rhs_smem + NSLOT * PN);
+  double (*sW)[PN] = reinterpret_cast<double (*)[PN]>(rhs_smem + 2 * NSLOT * PN);
+  const Dims& d = a.d;
+  const Metric& m = a.m;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * TX + tx;
+  const int i0 = 2 + blockIdx.x * TX, j0 = 2 + blockIdx.y * TY;
+  const int k0 = 2 + blockIdx.z * KC;
+  const int k1 = min(k0 + KC - 1, d.Nz + 1);
+  const int i = i0 + tx, j = j0 + ty;
+  const bool active = (i <= d.Nx + 1) && (j <= d.Ny + 1);
+  const bool hasv = active && (j <= d.Ny);
+  const double dPdx = a.sc->dPdx, dPdy = a.sc->dPdy, dPdz = a.sc->dPdz;
+
+  // asynchronous copy of plane k (tile + halo) of U, V, W into a slot
+  auto issue_plane = [&](int k) {
+    const int slot = k & (NSLOT - 1);
+    for (int t = tid; t < PN; t += TX * TY) {
+      const int li = t % PX, lj = t / PX;
+      const int gi = i0 - 1 + li, gj = j0 - 1 + lj;
+      const bool vu = gi <= d.nx && gj <= d.nyg && k <= d.nzg;
+      const bool vv = gi <= d.nxg && gj <= d.ny && k <= d.nzg;
+      const bool vw = gi <= d.nxg && gj <= d.nyg && k <= d.nz;
+      cp_async8(&sU[slot][t], vu ? a.U + idxU(d, gi, gj, k) : a.U, vu);
+      cp_async8(&sV[slot][t], vv ? a.V + idxV(d, gi, gj, k) : a.V, vv);
+      cp_async8(&sW[slot][t], vw ? a.W + idxW(d, gi, gj, k) : a.W, vw);
+    }
+    cp_async_commit();
+  };
+  issue_plane(k0 - 1);
+  issue_plane(k0);
+  for (int q = 1; q <= AHEAD; ++q) {
+    if (k0 + q <= k1 + 1) issue_plane(k0 + q);
+    else cp_async_commit();
+  }
+  const int c = (ty + 1) * PX + (tx + 1);     // own cell in the padded tile
+  for (int k = k0; k <= k1; ++k) {
+    if (k + 1 + AHEAD <= k1 + 1) issue_plane(k + 1 + AHEAD);
+    else cp_async_commit();                   // keep the group count uniform
+    cp_async_wait<AHEAD>();                   // planes up to k+1 have landed
+    __syncthreads();
+    const int sm = (k - 1) & (NSLOT - 1), s0 = k & (NSLOT - 1), sp = (k + 1) & (NSLOT - 1);
+    if (active) {
+      const int64_t iu = idxU(d, i, j, k), iw = idxW(d, i, j, k);
+      const int64_t iv = idxV(d, i, j, k);
+      double gu = 0.0, gv = 0.0, gw = 0.0;
+      if (MODE == 2) {                        // issue the accumulator loads early
+        gu = __ldg(a.Gu + iu);
+        gw = __ldg(a.Gw + iw);
+        if (hasv) gv = __ldg(a.Gv + iv);
+      }
+#define AU(s, di, dj) sU[s][c + (di) + (dj) * PX]
+#define AV(s, di, dj) sV[s][c + (di) + (dj) * PX]
+#define AW(s, di, dj) sW[s][c + (di) + (dj) * PX]
+      const double u0 = AU(s0, 0, 0), uxm = AU(s0, -1, 0), uxp = AU(s0, 1, 0);
+      const double uym = AU(s0, 0, -1), uyp = AU(s0, 0, 1);
+      const double uzm = AU(sm, 0, 0), uzp = AU(sp, 0, 0);
+      const double v0 = AV(s0, 0, 0), vxp = AV(s0, 1, 0), vym = AV(s0, 0, -1);
+      const double w0 = AW(s0, 0, 0), wxp = AW(s0, 1, 0), wzm = AW(sm, 0, 0);
+      double Fu, Fv = 0.0, Fw;
+      {
+        const double v1m = AV(s0, 1, -1);
+        const double w1m = AW(sm, 1, 0);
+        const double ap = u0 + uxp, am = uxm + u0;
+        double r = (am * am - ap * ap) * (0.25 * m.rdxg[i]);
+        r += ((uym + u0) * (vym + v1m) - (u0 + uyp) * (v0 + vxp)) * (0.25 * m.rdy[j]);
+        r += ((uzm + u0) * (wzm + w1m) - (u0 + uzp) * (w0 + wxp)) * (0.25 * m.rdz[k]);
+        r += m.cxpF[i] * (uxp - u0) - m.cxmF[i] * (u0 - uxm)
+           + m.cypC[j] * (uyp - u0) - m.cymC[j] * (u0 - uym)
+           + m.czpC[k] * (uzp - u0) - m.czmC[k] * (u0 - uzm);
+        r += a.Hu ? dPdx * __ldg(a.Hu + iu) : dPdx;
+        Fu = r;
+      }
+      {
+        const double wxm = AW(s0, -1, 0), wym = AW(s0, 0, -1), wyp = AW(s0, 0, 1);
+        const double wzp = AW(sp, 0, 0);
+        const double umzp = AU(sp, -1, 0);
+        const double vzp = AV(sp, 0, 0), vymzp = AV(sp, 0, -1);
+        const double am = wzm + w0, ap = w0 + wzp;
+        double r = (am * am - ap * ap) * (0.25 * m.rdzg[k]);
+        r += ((uxm + umzp) * (wxm + w0) - (u0 + uzp) * (w0 + wxp)) * (0.25 * m.rdx[i]);
+        r += ((vym + vymzp) * (wym + w0) - (v0 + vzp) * (w0 + wyp)) * (0.25 * m.rdy[j]);
+        r += m.cxpC[i] * (wxp - w0) - m.cxmC[i] * (w0 - wxm)
+           + m.cypC[j] * (wyp - w0) - m.cymC[j] * (w0 - wym)
+           + m.czpF[k] * (wzp - w0) - m.czmF[k] * (w0 - wzm);
+        r += a.Hw ? dPdz * __ldg(a.Hw + iw) : dPdz;
+        Fw = r;
+      }
+      if (hasv) {
+        const double vxm = AV(s0, -1, 0), vyp = AV(s0, 0, 1);
+        const double vzm = AV(sm, 0, 0), vzp = AV(sp, 0, 0);
+        const double um1 = AU(s0, -1, 1);
+        const double wyp = AW(s0, 0, 1), wypzm = AW(sm, 0, 1);
+        const double am = vym + v0, ap = v0 + vyp;
+        double r = (am * am - ap * ap) * (0.25 * m.rdyg[j]);
+        r += ((uxm + um1) * (vxm + v0) - (u0 + uyp) * (v0 + vxp)) * (0.25 * m.rdx[i]);
+        r += ((vzm + v0) * (wzm + wypzm) - (v0 + vzp) * (w0 + wyp)) * (0.25 * m.rdz[k]);
+        r += m.cxpC[i] * (vxp - v0) - m.cxmC[i] * (v0 - vxm)
+           + m.cypF[j] * (vyp - v0) - m.cymF[j] * (v0 - vym)
+           + m.czpC[k] * (vzp - v0) - m.czmC[k] * (v0 - vzm);
+        r += a.Hv ? dPdy * __ldg(a.Hv + iv) : dPdy;
+        Fv = r;
+      }
+#undef AU
+#undef AV
+#undef AW
+      if (MODE == 1) {
+        a.Us[iu] = u0 + a.cs * Fu;
+        a.Gu_out[iu] = u0 + a.cg * Fu;
+        a.Ws[iw] = w0 + a.cs * Fw;
+        a.Gw_out[iw] = w0 + a.cg * Fw;
+        if (hasv) {
+          a.Vs[iv] = v0 + a.cs * Fv;
+          a.Gv_out[iv] = v0 + a.cg * Fv;
+        }
+      } else {
+        a.Us[iu] = gu + a.cs * Fu;
+        a.Ws[iw] = gw + a.cs * Fw;
+        if (hasv) a.Vs[iv] = gv + a.cs * Fv;
+      }
+    }
+    __syncthreads();   // plane k-1's slot is refilled by the next iteration
+  }
+}
+
 static RhsArgs base_args(Handle* h) {
   RhsArgs a{};
   a.d = h->d;
@@ -192,19 +342,32 @@ static dim3 rhs_grid(const Dims& d) {
   return dim3((d.Nx + b.x - 1) / b.x, (d.Ny + b.y - 1) / b.y, (d.Nz + b.z - 1) / b.z);
 }
 
+static const int kRhsSmem = 3 * NSLOT * PN * (int)sizeof(double);
+
+int rhs_setup(Handle* h) {
+  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_rhs_tiled<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmem));
+  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_rhs_tiled<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmem));
+  return 0;
+}
+
 // stage = 1, 2, 3; U,V,W (with valid ghosts) -> Us,Vs,Ws interior (+ G at stage 1)
 int launch_rhs_stage(Handle* h, int stage, double dt) {
   RhsArgs a = base_args(h);
   a.Us = h->Us; a.Vs = h->Vs; a.Ws = h->Ws;
+  const Dims& d = h->d;
+  const dim3 tb(TX, TY, 1);
+  const dim3 tg((d.Nx + TX - 1) / TX, (d.Ny + TY - 1) / TY, (d.Nz + KC - 1) / KC);
   if (stage == 1) {
     a.Gu_out = h->Gu; a.Gv_out = h->Gv; a.Gw_out = h->Gw;
     a.cs = dt * (8.0 / 15.0);
     a.cg = dt * (1.0 / 4.0);
-    k_rhs<1><<<rhs_grid(h->d), rhs_block(), 0, h->stream>>>(a);
+    if (h->rhs_kernel == 0) k_rhs_tiled<1><<<tg, tb, kRhsSmem, h->stream>>>(a);
+    else k_rhs<1><<<rhs_grid(d), rhs_block(), 0, h->stream>>>(a);
   } else {
     a.Gu = h->Gu; a.Gv = h->Gv; a.Gw = h->Gw;
     a.cs = (stage == 2) ? dt * (5.0 / 12.0) : dt * (3.0 / 4.0);
-    k_rhs<2><<<rhs_grid(h->d), rhs_block(), 0, h->stream>>>(a);
+    if (h->rhs_kernel == 0) k_rhs_tiled<2><<<tg, tb, kRhsSmem, h->stream>>>(a);
+    else k_rhs<2><<<rhs_grid(d), rhs_block(), 0, h->stream>>>(a);
   }
   C3D_LAUNCH_CHECK(h);
   return 0;

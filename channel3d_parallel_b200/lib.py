@@ -24,7 +24,7 @@ FIELD = dict(U=1, V=2, W=3, P=4, RHS_P=5, P_INTERIM=6, RHS_U=7, RHS_V=8, RHS_W=9
              U_WORK=10, V_WORK=11, W_WORK=12, U_REG=13, V_REG=14, W_REG=15,
              HU_INTERIOR=16, HV_INTERIOR=17, HW_INTERIOR=18, HC_EXTERIOR=19)
 MARKER = dict(FB=40, UB=41, XB=42, YB=43, ZB=44, NORMALS=45, SB=46, E1NH_EXT=47, E1NHC_EXT=48)
-POISSON_FP64, POISSON_MIXED = 0, 1
+POISSON_FP64, POISSON_MIXED, POISSON_MIXED_UNREFINED = 0, 1, 2
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_LEARNED = 0, 1, 2
 
 
@@ -92,8 +92,8 @@ PROTOTYPES = {
     "c3d_mean_mass_flow_u_noalloc": [C.c_void_p, _INT, _INT, _INT, C.c_void_p, C.c_void_p,
                                      C.c_void_p],
 }
-KERNEL_CLASSES = ("rhs_stage", "ghosts", "div_xfft", "zfft_fwd", "tridiag", "zfft_inv",
-                  "xfft_inv", "grad_sub", "massflow")
+KERNEL_CLASSES = ("rhs_stage", "ghosts", "div_xfft", "spectral_yz", "xfft_inv", "grad_sub",
+                  "massflow")
 
 _lib = None
 

@@ -77,6 +77,7 @@ extern "C" {
 /* ---- solver options ------------------------------------------------------ */
 #define C3D_POISSON_FP64        0   /* plain FP64 spectral Poisson solve        */
 #define C3D_POISSON_MIXED       1   /* FP32 spectral solve + FP64 refinement    */
+#define C3D_POISSON_MIXED_UNREFINED 2 /* FP32 spectral solve, no refinement (accuracy studies) */
 #define C3D_PRECOND_NONE        0   /* reference BiCGSTAB (unpreconditioned)    */
 #define C3D_PRECOND_JACOBI      1   /* diagonal (Jacobi) preconditioner         */
 #define C3D_PRECOND_LEARNED     2   /* learned preconditioner + warm start      */
@@ -204,8 +205,8 @@ int c3d_kernel_launches(int handle, int64_t* count);
 /* time every kernel class of one RK3 stage separately, each launched nrep
  * times between CUDA events on the handle's stream (the fields are used as
  * scratch); ms[c] = average device time of class c in the order
- * rhs_stage, ghosts, div_xfft, zfft_fwd, tridiag, zfft_inv, xfft_inv,
- * grad_sub, massflow.  Writes min(nmax, 9) entries.                          */
+ * rhs_stage, ghosts, div_xfft, spectral_yz, xfft_inv, grad_sub, massflow
+ * (FP64 kernels).  Writes min(nmax, 7) entries.                              */
 int c3d_profile_kernels(int handle, int nrep, double* ms, int nmax);
 
 /* ---- allocation-free entry ------------------------------------------------

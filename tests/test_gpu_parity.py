@@ -20,6 +20,8 @@ CASES = {
     "cfg0_34x65x34": (34, 65, 34, math.pi, math.pi / 2, 1),
     "odd_ny_radix3": (50, 34, 26, 2.0, 1.0, 1),
     "uniform_small": (18, 17, 14, 1.0, 0.7, 0),
+    # 127 interior rows: a kx slab spans a 4-CTA cluster (FP64)
+    "tall_ny_clusters": (18, 129, 18, 1.0, 0.5, 1),
 }
 
 
@@ -128,7 +130,10 @@ def test_rk3_steps(pair, nsteps):
             for name, ref in (("U", st.U), ("V", st.V), ("W", st.W), ("P", st.P))}
     assert max(errs.values()) < 1e-10, errs
     s = ch.stats()
-    assert abs(s["dPdx"] - st.dPdx) <= 1e-9 * abs(st.dPdx) + 1e-14
+    # dPdx = (dPdx_prev + shift/dt)/2 with shift = Q0 - Q(U), a difference of
+    # nearly equal bulk fluxes: round-off of Q (a few eps*Q0) divided by dt
+    dt = 1e-3
+    assert abs(s["dPdx"] - st.dPdx) <= 1e-9 * abs(st.dPdx) + 50 * 2.2e-16 * abs(st.Qflow_x_0) / dt
     assert s["steps"] == nsteps
     assert ch.check_divergence() < 1e-12
     assert ch.check_finite() == 0
