@@ -80,7 +80,8 @@ struct DevScalars {
   double qflow;          // last bulk flux (Int_U / norm)
   double dpdx_prev;
   unsigned long long err;   // sticky kernel error bits (bit 0: a bounded copy wait gave up)
-  double pad;
+  unsigned int ticket;      // blocks done in the current reduction (reset by the last one)
+  unsigned int pad;
 };
 
 // Spectral Poisson state: twiddles, Thomas factor tables and spectra for the

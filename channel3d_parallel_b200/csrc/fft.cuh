@@ -189,35 +189,118 @@ __device__ __forceinline__ void ct_stage(typename cplx<T>::t* data, int nrows, i
   __syncthreads();
 }
 
-template <typename T, bool INV>
+// Same stage when blockDim.x is a multiple of N/R: every thread keeps one
+// butterfly position (q fixed, twiddles in registers) and walks the rows
+// l0, l0 + nt/(N/R), ..., kB rows per iteration.
+template <typename T, bool INV, int R, int kB>
+__device__ __forceinline__ void ct_stage_fixed(typename cplx<T>::t* data, int nrows, int rs,
+                                               const typename cplx<T>::t* tw, int N, int L) {
+  using C = typename cplx<T>::t;
+  const int M = L / R, nb = N / R, tws = N / L;
+  const int bb = threadIdx.x % nb;
+  const int l0 = threadIdx.x / nb, ls = blockDim.x / nb;
+  const int blk = bb / M, q = bb - blk * M;
+  C w[R];
+#pragma unroll
+  for (int r = 1; r < R; ++r) {
+    w[r] = tw[q * r * tws];
+    if (INV) w[r].y = -w[r].y;
+  }
+  C* p0 = data + blk * L + q;
+  // all loads of an iteration are issued before any store (the compiler
+  // cannot reorder shared-memory loads across stores to a runtime stride)
+  int l = l0;
+  for (; l + (kB - 1) * ls < nrows; l += kB * ls) {
+    C v[kB][R];
+#pragma unroll
+    for (int b = 0; b < kB; ++b)
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b][r] = p0[(l + b * ls) * rs + r * M];
+#pragma unroll
+    for (int b = 0; b < kB; ++b) {
+      if (INV) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[b][r] = cmul(v[b][r], w[r]);
+      }
+      butterfly<T, INV, R>(v[b]);
+      if (!INV) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[b][r] = cmul(v[b][r], w[r]);
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < kB; ++b)
+#pragma unroll
+      for (int r = 0; r < R; ++r) p0[(l + b * ls) * rs + r * M] = v[b][r];
+  }
+  for (; l < nrows; l += ls) {
+    C* p = p0 + l * rs;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = p[r * M];
+    if (INV) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
+    }
+    butterfly<T, INV, R>(v);
+    if (!INV) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) p[r * M] = v[r];
+  }
+  __syncthreads();
+}
+
+template <typename T, bool INV, int kB>
 __device__ __forceinline__ void ct_stage_any(typename cplx<T>::t* data, int nrows, int rs,
                                              const typename cplx<T>::t* tw, int N, int L, int R,
                                              int run) {
-  if (R == 4) ct_stage<T, INV, 4>(data, nrows, rs, tw, N, L, run);
-  else if (R == 2) ct_stage<T, INV, 2>(data, nrows, rs, tw, N, L, run);
-  else ct_stage<T, INV, 3>(data, nrows, rs, tw, N, L, run);
+  if (blockDim.x % (N / R) == 0) {
+    if (R == 4) ct_stage_fixed<T, INV, 4, kB>(data, nrows, rs, tw, N, L);
+    else if (R == 2) ct_stage_fixed<T, INV, 2, kB>(data, nrows, rs, tw, N, L);
+    else ct_stage_fixed<T, INV, 3, kB>(data, nrows, rs, tw, N, L);
+  } else {
+    if (R == 4) ct_stage<T, INV, 4>(data, nrows, rs, tw, N, L, run);
+    else if (R == 2) ct_stage<T, INV, 2>(data, nrows, rs, tw, N, L, run);
+    else ct_stage<T, INV, 3>(data, nrows, rs, tw, N, L, run);
+  }
 }
 
 // forward transform of nrows rows; output in digit-reversed order
-template <typename T>
+template <typename T, int kB>
 __device__ void fft_rows_dif(typename cplx<T>::t* data, int nrows, int rs,
                              const typename cplx<T>::t* tw, const FftPasses& P, int run) {
   int L = P.n;
   for (int p = 0; p < P.npass; ++p) {
-    ct_stage_any<T, false>(data, nrows, rs, tw, P.n, L, P.radix[p], run);
+    ct_stage_any<T, false, kB>(data, nrows, rs, tw, P.n, L, P.radix[p], run);
     L /= P.radix[p];
   }
 }
 
 // inverse transform of nrows digit-reversed rows; output in natural order
-template <typename T>
+template <typename T, int kB>
 __device__ void fft_rows_dit_inv(typename cplx<T>::t* data, int nrows, int rs,
                                  const typename cplx<T>::t* tw, const FftPasses& P, int run) {
   int L = 1;
   for (int p = P.npass - 1; p >= 0; --p) {
     L *= P.radix[p];
-    ct_stage_any<T, true>(data, nrows, rs, tw, P.n, L, P.radix[p], run);
+    ct_stage_any<T, true, kB>(data, nrows, rs, tw, P.n, L, P.radix[p], run);
   }
+}
+
+// position at which the forward transform leaves the coefficient of index k
+__host__ __device__ inline int dif_k_to_position(int k, const FftPasses& P) {
+  int pos = 0, rem = k, span = P.n;
+  for (int p = 0; p < P.npass; ++p) {
+    const int M = span / P.radix[p];
+    const int s = rem % P.radix[p];
+    rem /= P.radix[p];
+    pos += s * M;
+    span = M;
+  }
+  return pos;
 }
 
 // wavenumber index k whose coefficient the forward transform leaves at

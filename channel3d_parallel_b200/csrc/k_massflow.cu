@@ -43,76 +43,89 @@ __device__ __forceinline__ double2 block_sum2(double2 v) {
   return r;
 }
 
-// partial sums of (Int_U, norm); Hu may be null (H = 1)
-__global__ void __launch_bounds__(kRedThreads) k_massflow_partial(Dims d, Metric m,
-                                                                 const double* __restrict__ U,
-                                                                 const double* __restrict__ Hu,
-                                                                 double2* __restrict__ part) {
-  const int ni = d.Nx, nj = d.nyg - 3, nk = d.Nz + 1;   // i 2..nx-1, j 3..nyg-1, k 2..nzg-1
-  const int64_t tot = (int64_t)ni * nj * nk;
+// (Int_U, norm) over rows (j, k), j = 3..nyg-1, k = 2..nzg-1, one warp per
+// x-row (i = 2..nx-1) so that a row's index arithmetic is done once; Hu may
+// be null (H = 1).  Every block writes its partial sum; the last block to
+// finish (ticket in DevScalars) adds the partials in block order and
+//   mode 0: stores qflow = Int_U/norm;
+//   mode 1: also the constant-flux correction shift and dPdx.
+__global__ void __launch_bounds__(kRedThreads) k_massflow(Dims d, Metric m, const double* __restrict__ U,
+                                                         const double* __restrict__ Hu,
+                                                         double2* __restrict__ part, DevScalars* sc,
+                                                         double q0, double dt, int mode) {
+  const int ni = d.Nx, nj = d.nyg - 3, nk = d.Nz + 1;
+  const int nrows = nj * nk;
+  const int lane = threadIdx.x & 31;
+  const int wpb = kRedThreads / 32;
   double2 acc = make_double2(0.0, 0.0);
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int i = 2 + (int)(t % ni);
-    const int j = 3 + (int)((t / ni) % nj);
-    const int k = 2 + (int)(t / ((int64_t)ni * nj));
+  for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < nrows; row += gridDim.x * wpb) {
+    const int kk = row / nj;
+    const int j = 3 + (row - kk * nj);
+    const int k = 2 + kk;
     const double w = m.wq[j];
-    const int64_t a = idxU(d, i, j, k), b = idxU(d, i, j - 1, k);
-    if (Hu) {
-      const double ha = Hu[a], hb = Hu[b];
-      acc.x += (ha * U[a] + hb * U[b]) * w;
-      acc.y += (ha + hb) * w;
-    } else {
-      acc.x += (U[a] + U[b]) * w;
-      acc.y += 2.0 * w;
+    const int64_t a0 = idxU(d, 2, j, k), b0 = idxU(d, 2, j - 1, k);
+    for (int ii = lane; ii < ni; ii += 32) {
+      const int64_t a = a0 + ii, b = b0 + ii;
+      if (Hu) {
+        const double ha = Hu[a], hb = Hu[b];
+        acc.x += (ha * U[a] + hb * U[b]) * w;
+        acc.y += (ha + hb) * w;
+      } else {
+        acc.x += (U[a] + U[b]) * w;
+        acc.y += 2.0 * w;
+      }
     }
   }
   double2 s = block_sum2(acc);
-  if (threadIdx.x == 0) part[blockIdx.x] = s;
-}
-
-// final sum; mode 0: qflow only; mode 1: constant-flux correction update
-__global__ void k_massflow_final(const double2* __restrict__ part, int np, DevScalars* sc,
-                                 double q0, double dt, int mode) {
-  double2 acc = make_double2(0.0, 0.0);
-  for (int t = threadIdx.x; t < np; t += blockDim.x) {
-    acc.x += part[t].x;
-    acc.y += part[t].y;
-  }
-  double2 s = block_sum2(acc);
+  __shared__ bool last;
   if (threadIdx.x == 0) {
-    const double q = s.x / s.y;
+    part[blockIdx.x] = s;
+    __threadfence();
+    last = atomicAdd(&sc->ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double2 t = make_double2(0.0, 0.0);
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+    const double2 v = __ldcg(part + b);
+    t.x += v.x;
+    t.y += v.y;
+  }
+  t = block_sum2(t);
+  if (threadIdx.x == 0) {
+    const double q = t.x / t.y;
     sc->qflow = q;
     if (mode == 1) {
-      const double shift = q0 - s.x / s.y;
+      const double shift = q0 - t.x / t.y;
       sc->shift = shift;
       sc->dpdx_prev = sc->dPdx;
       sc->dPdx = 0.5 * (sc->dpdx_prev + shift / dt);
     }
+    sc->ticket = 0u;
   }
 }
 
 // U(2:nx-1,2:nyg-1,2:nzg-1) += shift followed by the boundary conditions is,
 // entry for entry, U += shift on every copy of an interior value and
-// U -= shift on the odd y ghosts.
-__global__ void k_shift_u(Dims d, double* __restrict__ U, const DevScalars* sc) {
+// U -= shift on the odd y ghosts.  One warp per x-row of the whole array.
+__global__ void __launch_bounds__(256) k_shift_u(Dims d, double* __restrict__ U, const DevScalars* sc) {
   const double s = sc->shift;
-  const int64_t tot = (int64_t)d.nx * d.nyg * d.nzg;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int j = 1 + (int)((t / d.nx) % d.nyg);
-    U[t] = (j == 1 || j == d.nyg) ? U[t] - s : U[t] + s;
+  const int nrows = d.nyg * d.nzg;
+  const int lane = threadIdx.x & 31;
+  for (int row = blockIdx.x * 8 + (threadIdx.x >> 5); row < nrows; row += gridDim.x * 8) {
+    const int j = 1 + row % d.nyg;
+    const double sr = (j == 1 || j == d.nyg) ? -s : s;
+    double* u = U + (int64_t)row * d.nx;
+    for (int i = lane; i < d.nx; i += 32) u[i] += sr;
   }
 }
 
 int launch_massflow_correction(Handle* h, double dt) {
   // with an immersed body the flux is H-weighted (src/mass_flow.f90:160-163)
   const double* Hu = h->ib ? ib_hu(h) : nullptr;
-  k_massflow_partial<<<kRedBlocks, kRedThreads, 0, h->stream>>>(h->d, h->m, h->U, Hu,
-                                                                (double2*)h->red);
-  C3D_LAUNCH_CHECK(h);
-  k_massflow_final<<<1, 1024, 0, h->stream>>>((const double2*)h->red, kRedBlocks, h->sc,
-                                              h->Qflow_x_0, dt, 1);
+  k_massflow<<<kRedBlocks, kRedThreads, 0, h->stream>>>(h->d, h->m, h->U, Hu, (double2*)h->red, h->sc,
+                                                        h->Qflow_x_0, dt, 1);
   C3D_LAUNCH_CHECK(h);
   k_shift_u<<<148 * 8, 256, 0, h->stream>>>(h->d, h->U, h->sc);
   C3D_LAUNCH_CHECK(h);
@@ -120,9 +133,8 @@ int launch_massflow_correction(Handle* h, double dt) {
 }
 
 int massflow_u(Handle* h, const double* U, const double* Hu, double* q_out) {
-  k_massflow_partial<<<kRedBlocks, kRedThreads, 0, h->stream>>>(h->d, h->m, U, Hu, (double2*)h->red);
-  C3D_LAUNCH_CHECK(h);
-  k_massflow_final<<<1, 1024, 0, h->stream>>>((const double2*)h->red, kRedBlocks, h->sc, 0.0, 1.0, 0);
+  k_massflow<<<kRedBlocks, kRedThreads, 0, h->stream>>>(h->d, h->m, U, Hu, (double2*)h->red, h->sc, 0.0,
+                                                        1.0, 0);
   C3D_LAUNCH_CHECK(h);
   double q = 0;
   C3D_CUDA_TRY(h, cudaMemcpyAsync(&q, &h->sc->qflow, sizeof(double), cudaMemcpyDeviceToHost, h->stream));

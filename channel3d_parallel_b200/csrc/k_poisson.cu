@@ -137,8 +137,12 @@ static int build_tri_table(Handle* h) {
 // ---------------------------------------------------------------------------
 // kernel 1: (divergence |) x real-to-complex FFT of (j, k) lines
 // ---------------------------------------------------------------------------
-constexpr int kMaxLines = 16;   // complex lines per block (upper bound)
-constexpr int kLinesX = 4;      // complex x-lines per block
+// Two real x-lines form one complex line; a block transforms kLinesX complex
+// lines in place (rows of stride rs in shared memory) with a thread count
+// that is a multiple of Nx, so every FFT stage keeps one butterfly position
+// per thread.
+constexpr int kLinesX = 8;      // complex x-lines per block
+constexpr int kMaxNx = 512;
 
 template <typename T>
 struct XfwdArgs {
@@ -152,8 +156,8 @@ struct XfwdArgs {
   const typename cplx<T>::t* __restrict__ tw;
   double* __restrict__ linesum;               // FP64 line sums (mixed path) or null
   FftPasses P;
-  int lpb;
   int pz;                                     // spectrum row pitch
+  int rs;                                     // shared-memory row stride
 };
 
 // real x-line r = (k-2) + Nz*(j-2); its spectrum goes to slab offset
@@ -165,38 +169,57 @@ __device__ __forceinline__ void line_info(const Dims& d, int pz, int64_t r, int*
   *off = jj * pz + kk;
 }
 
-// one complex line = two real lines r = 2p, 2p+1
+// shared-memory carve-up of the x-FFT kernels
+template <typename T>
+struct XfftSmem {
+  typename cplx<T>::t* tw;     // [N]
+  typename cplx<T>::t* buf;    // [kLinesX][rs]
+  int* pos;                    // [N] digit-reversed position of coefficient m
+  double* sval;                // [2*kLinesX][N] FP64 values for line sums (FP32 path)
+};
+
+template <typename T>
+__device__ __forceinline__ XfftSmem<T> xfft_carve(unsigned char* base, int N, int rs) {
+  using C = typename cplx<T>::t;
+  XfftSmem<T> s;
+  s.tw = reinterpret_cast<C*>(base);
+  s.buf = s.tw + N;
+  s.pos = reinterpret_cast<int*>(s.buf + (size_t)kLinesX * rs);
+  s.sval = reinterpret_cast<double*>(s.pos + N + (N & 1));   // FP32 path only
+  return s;
+}
+
 template <bool FROM_DIV, typename T>
-__global__ void __launch_bounds__(128) k_xfft_fwd(XfwdArgs<T> a) {
+__global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
   using C = typename cplx<T>::t;
   extern __shared__ __align__(16) unsigned char xf_smem[];
-  __shared__ int s_j[2 * kMaxLines], s_k[2 * kMaxLines], s_off[2 * kMaxLines];
+  __shared__ int s_j[2 * kLinesX], s_k[2 * kLinesX], s_off[2 * kLinesX];
   const Dims& d = a.d;
-  const int N = d.Nx;
-  const int L = a.lpb;
-  C* tw = reinterpret_cast<C*>(xf_smem);
-  C* b0 = tw + N;
-  C* b1 = b0 + L * N;
-  double* sval = reinterpret_cast<double*>(b1 + L * N);   // FP64 copy (line sums)
-  for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = a.tw[t];
+  const int N = d.Nx, RS = a.rs;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  XfftSmem<T> sm = xfft_carve<T>(xf_smem, N, RS);
+  for (int t = tid; t < N; t += nt) {
+    sm.tw[t] = a.tw[t];
+    sm.pos[t] = dif_k_to_position(t, a.P);
+  }
   const int64_t nreal = (int64_t)d.Ny * d.Nz;
-  const int64_t r0 = (int64_t)blockIdx.x * L * 2;
-  if (threadIdx.x < 2 * L) {
-    const int64_t r = r0 + threadIdx.x;
+  const int64_t r0 = (int64_t)blockIdx.x * kLinesX * 2;
+  if (tid < 2 * kLinesX) {
+    const int64_t r = r0 + tid;
     int j = -1, k = -1, off = 0;
     if (r < nreal) line_info(d, a.pz, r, &j, &k, &off);
-    s_j[threadIdx.x] = j;
-    s_k[threadIdx.x] = k;
-    s_off[threadIdx.x] = off;
+    s_j[tid] = j;
+    s_k[tid] = k;
+    s_off[tid] = off;
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < 2 * L * N; t += blockDim.x) {
-    const int rl = t / N;
-    const int ii = t - rl * N;
+  // nt is a multiple of N: thread -> x index ii, real lines rl0, rl0 + nt/N, ...
+  const int ii = tid % N, rls = nt / N;
+  const int i = 2 + ii;
+  for (int rl = tid / N; rl < 2 * kLinesX; rl += rls) {
     const int j = s_j[rl], k = s_k[rl];
     double val = 0.0;
     if (j > 0) {
-      const int i = 2 + ii;
       if (FROM_DIV) {
         const int64_t iu = idxU(d, i, j, k), iv = idxV(d, i, j, k), iw = idxW(d, i, j, k);
         val = (a.U[iu] - a.U[iu - 1]) * a.m.rdx[i]
@@ -206,29 +229,30 @@ __global__ void __launch_bounds__(128) k_xfft_fwd(XfwdArgs<T> a) {
         val = a.rhs[idxR(d, i, j, k)];
       }
     }
-    C& z = b0[(rl >> 1) * N + ii];
+    C& z = sm.buf[(rl >> 1) * RS + ii];
     if (rl & 1) z.y = (T)val; else z.x = (T)val;
-    if (a.linesum) sval[t] = val;
+    if (a.linesum) sm.sval[rl * N + ii] = val;
   }
   __syncthreads();
-  if (a.linesum && threadIdx.x < 2 * L) {   // FP64 line sum in a fixed order
-    const int64_t r = r0 + threadIdx.x;
+  if (a.linesum && tid < 2 * kLinesX) {   // FP64 line sum in a fixed order
+    const int64_t r = r0 + tid;
     if (r < nreal) {
       double sum = 0.0;
-      for (int ii = 0; ii < N; ++ii) sum += sval[threadIdx.x * N + ii];
+      for (int q = 0; q < N; ++q) sum += sm.sval[tid * N + q];
       a.linesum[r] = sum;
     }
   }
-  C* res = fft_lines<T, false>(b0, b1, L, tw, a.P);
+  fft_rows_dif<T, 2>(sm.buf, kLinesX, RS, sm.tw, a.P, 128 / (int)sizeof(C));
+  // split Z = A + iB of the two real lines: A = (Z_m + conj Z_{N-m})/2,
+  // B = (Z_m - conj Z_{N-m})/(2i), m = 0..N/2
   const int nk = d.nkx;
-  for (int t = threadIdx.x; t < L * nk; t += blockDim.x) {
-    const int pl = t % L;
-    const int mm = t / L;
+  for (int t = tid; t < kLinesX * nk; t += nt) {
+    const int pl = t % kLinesX;
+    const int mm = t / kLinesX;
     const int64_t ra = r0 + 2 * pl;
     if (ra >= nreal) continue;
-    const C Z = res[pl * N + mm];
-    const C Zr = res[pl * N + ((N - mm) % N)];
-    // A = (Z + conj(Zr))/2,  B = (Z - conj(Zr))/(2i)
+    const C Z = sm.buf[pl * RS + sm.pos[mm]];
+    const C Zr = sm.buf[pl * RS + sm.pos[mm == 0 ? 0 : N - mm]];
     C A, B;
     A.x = (T)0.5 * (Z.x + Zr.x);
     A.y = (T)0.5 * (Z.y - Zr.y);
@@ -309,6 +333,12 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
   for (int t = tid; t < Nz; t += nt) tw[t] = a.tw[t];
   for (int t = tid; t < Ny; t += nt) { sdl[t] = a.dl[t]; sdu[t] = a.du[t]; }
 
+  const bool loaded = mbar_wait(&bar, 0, kWaitCycles);
+  if (!loaded) atomicOr(a.err, 1ull);
+  __syncthreads();
+
+  fft_rows_dif<T, 4>(data, jn, RS, tw, a.P, kRun);
+
   // pivots of this thread's column for rows j0-1 .. j0+jn-1 (one column per
   // thread when Nz <= blockDim; otherwise reloaded per column below)
   const T* rdp_m = a.rdp + (int64_t)m * Ny * nkzs;
@@ -325,29 +355,45 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
   };
   if (one_col && tid < Nz) load_pivots(tid);
 
-  const bool loaded = mbar_wait(&bar, 0, kWaitCycles);
-  if (!loaded) atomicOr(a.err, 1ull);
-  __syncthreads();
-
-  fft_rows_dif<T>(data, jn, RS, tw, a.P, kRun);
-
+  // The sweeps take rows in chunks of kCh: loads of a chunk are issued
+  // together, the recurrence runs in registers, then the chunk is stored.
+  constexpr int kCh = 4;
   // forward elimination B(j) -= DL(j-1)/D'(j-1) * B(j-1)
   for (int c = 0; c < cs; ++c) {
     if (crank == c) {
       const C* up = c > 0 ? cl.map_shared_rank(data, c - 1) : nullptr;
       for (int col = tid; col < Nz; col += nt) {
         if (!one_col) load_pivots(col);
-        C prev = c > 0 ? up[(size_t)(Jc - 1) * RS + col] : data[col];
+        C prev = c > 0 ? up[(size_t)(Jc - 1) * RS + col] : C{(T)0, (T)0};
 #pragma unroll
-        for (int jl = 0; jl < JM; ++jl) {
-          if (jl < jn && (c > 0 || jl > 0)) {
-            const int j = j0 + jl;
-            const T mu = sdl[j - 1] * (jl == 0 ? rdm1 : rdv[jl > 0 ? jl - 1 : 0]);
-            C b = data[jl * RS + col];
-            b.x = b.x - mu * prev.x;
-            b.y = b.y - mu * prev.y;
-            data[jl * RS + col] = b;
-            prev = b;
+        for (int c0 = 0; c0 < JM; c0 += kCh) {
+          if (c0 < jn) {
+            C bv[kCh];
+            T dlv[kCh];
+#pragma unroll
+            for (int u = 0; u < kCh; ++u) {
+              const int jl = c0 + u;
+              bv[u] = C{(T)0, (T)0};
+              dlv[u] = (T)0;
+              if (jl < jn) {
+                bv[u] = data[jl * RS + col];
+                if (j0 + jl > 0) dlv[u] = sdl[j0 + jl - 1];
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < kCh; ++u) {
+              const int jl = c0 + u;
+              if (jl < jn) {
+                // row 0 of the slab has no predecessor (dlv = 0, prev = 0)
+                const T mu = dlv[u] * (jl == 0 ? rdm1 : rdv[jl > 0 ? jl - 1 : 0]);
+                bv[u].x = bv[u].x - mu * prev.x;
+                bv[u].y = bv[u].y - mu * prev.y;
+                prev = bv[u];
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < kCh; ++u)
+              if (c0 + u < jn) data[(c0 + u) * RS + col] = bv[u];
           }
         }
       }
@@ -362,14 +408,32 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
         if (!one_col) load_pivots(col);
         C xn = c < cs - 1 ? dn[col] : C{(T)0, (T)0};
 #pragma unroll
-        for (int jl = JM - 1; jl >= 0; --jl) {
-          if (jl < jn) {
-            const T u = sdu[j0 + jl];
-            C b = data[jl * RS + col];
-            b.x = (b.x - u * xn.x) * rdv[jl];
-            b.y = (b.y - u * xn.y) * rdv[jl];
-            data[jl * RS + col] = b;
-            xn = b;
+        for (int c0 = JM - kCh; c0 >= 0; c0 -= kCh) {
+          if (c0 < jn) {
+            C bv[kCh];
+            T duv[kCh];
+#pragma unroll
+            for (int u = 0; u < kCh; ++u) {
+              const int jl = c0 + u;
+              bv[u] = C{(T)0, (T)0};
+              duv[u] = (T)0;
+              if (jl < jn) {
+                bv[u] = data[jl * RS + col];
+                duv[u] = sdu[j0 + jl];
+              }
+            }
+#pragma unroll
+            for (int u = kCh - 1; u >= 0; --u) {
+              const int jl = c0 + u;
+              if (jl < jn) {
+                bv[u].x = (bv[u].x - duv[u] * xn.x) * rdv[jl];
+                bv[u].y = (bv[u].y - duv[u] * xn.y) * rdv[jl];
+                xn = bv[u];
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < kCh; ++u)
+              if (c0 + u < jn) data[(c0 + u) * RS + col] = bv[u];
           }
         }
         if (a.zero00 && m == 0 && col == 0)
@@ -379,7 +443,7 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
     cl.sync();
   }
 
-  fft_rows_dit_inv<T>(data, jn, RS, tw, a.P, kRun);
+  fft_rows_dit_inv<T, 4>(data, jn, RS, tw, a.P, kRun);
 
   fence_async_shared();
   __syncthreads();
@@ -437,37 +501,40 @@ struct XinvArgs {
   const double* __restrict__ phi00;   // FP64 mean mode added to the output (mixed path)
   int accumulate;                // 1: rhs += result (refinement)
   FftPasses P;
-  int lpb;
   int pz;                        // spectrum row pitch
+  int rs;                        // shared-memory row stride
   double scale_div;              // nxp*nzp
 };
 
 template <typename T>
-__global__ void __launch_bounds__(128) k_xfft_inv(XinvArgs<T> a) {
+__global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
   using C = typename cplx<T>::t;
   extern __shared__ __align__(16) unsigned char xi_smem[];
-  __shared__ int s_j[2 * kMaxLines], s_k[2 * kMaxLines], s_off[2 * kMaxLines];
+  __shared__ int s_j[2 * kLinesX], s_k[2 * kLinesX], s_off[2 * kLinesX];
   const Dims& d = a.d;
-  const int N = d.Nx, L = a.lpb, nk = d.nkx;
-  C* tw = reinterpret_cast<C*>(xi_smem);
-  C* b0 = tw + N;
-  C* b1 = b0 + L * N;
-  for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = a.tw[t];
+  const int N = d.Nx, nk = d.nkx, RS = a.rs;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  XfftSmem<T> sm = xfft_carve<T>(xi_smem, N, RS);
+  for (int t = tid; t < N; t += nt) {
+    sm.tw[t] = a.tw[t];
+    sm.pos[t] = dif_k_to_position(t, a.P);
+  }
   const int64_t nreal = (int64_t)d.Ny * d.Nz;
-  const int64_t r0 = (int64_t)blockIdx.x * L * 2;
-  if (threadIdx.x < 2 * L) {
-    const int64_t r = r0 + threadIdx.x;
+  const int64_t r0 = (int64_t)blockIdx.x * kLinesX * 2;
+  if (tid < 2 * kLinesX) {
+    const int64_t r = r0 + tid;
     int j = -1, k = -1, off = 0;
     if (r < nreal) line_info(d, a.pz, r, &j, &k, &off);
-    s_j[threadIdx.x] = j;
-    s_k[threadIdx.x] = k;
-    s_off[threadIdx.x] = off;
+    s_j[tid] = j;
+    s_k[tid] = k;
+    s_off[tid] = off;
   }
   __syncthreads();
-  // Z = A + iB on the full circle from the two half spectra
-  for (int t = threadIdx.x; t < L * nk; t += blockDim.x) {
-    const int pl = t % L;
-    const int mm = t / L;
+  // Z = A + iB on the full circle from the two half spectra, placed at the
+  // digit-reversed positions the inverse transform expects
+  for (int t = tid; t < kLinesX * nk; t += nt) {
+    const int pl = t % kLinesX;
+    const int mm = t / kLinesX;
     const int64_t ra = r0 + 2 * pl;
     const C* in = a.spec + (int64_t)mm * d.Ny * a.pz;
     C A = C{(T)0, (T)0}, B = C{(T)0, (T)0};
@@ -477,26 +544,25 @@ __global__ void __launch_bounds__(128) k_xfft_inv(XinvArgs<T> a) {
     C Z;
     Z.x = A.x - B.y;
     Z.y = A.y + B.x;
-    b0[pl * N + mm] = Z;
+    sm.buf[pl * RS + sm.pos[mm]] = Z;
     if (mm > 0 && 2 * mm < N) {
       C Zc;
       Zc.x = A.x + B.y;
       Zc.y = -A.y + B.x;
-      b0[pl * N + (N - mm)] = Zc;
+      sm.buf[pl * RS + sm.pos[N - mm]] = Zc;
     }
   }
   __syncthreads();
-  C* res = fft_lines<T, true>(b0, b1, L, tw, a.P);
+  fft_rows_dit_inv<T, 2>(sm.buf, kLinesX, RS, sm.tw, a.P, 128 / (int)sizeof(C));
   const double sd = a.scale_div;
-  for (int t = threadIdx.x; t < 2 * L * N; t += blockDim.x) {
-    const int rl = t / N;
-    const int ii = t - rl * N;
+  const int ii = tid % N, rls = nt / N;
+  const int i = 2 + ii;
+  for (int rl = tid / N; rl < 2 * kLinesX; rl += rls) {
     const int j = s_j[rl], k = s_k[rl];
     if (j < 0) continue;
-    const C z = res[(rl >> 1) * N + ii];
+    const C z = sm.buf[(rl >> 1) * RS + ii];
     double v = (double)((rl & 1) ? z.y : z.x) / sd;
     if (a.phi00) v += a.phi00[j - 2];
-    const int i = 2 + ii;
     const int64_t o = idxR(d, i, j, k);
     if (a.accumulate) v += a.rhs[o];
     // apply_periodic_xz_centers (src/poisson.f90:106-125): x plane nxg-1 and
@@ -521,10 +587,28 @@ __global__ void __launch_bounds__(128) k_xfft_inv(XinvArgs<T> a) {
 // ---------------------------------------------------------------------------
 // host drivers
 // ---------------------------------------------------------------------------
+// x-FFT launch shape: threads a multiple of Nx (at least 128), shared-memory
+// rows padded (FP64: rs = 1 mod 8, FP32: rs odd) so that the line-parallel
+// accesses are conflict-free
+static int xfft_threads(const Dims& d) {
+  int nt = d.Nx;
+  while (nt < 128) nt += d.Nx;
+  return nt;
+}
+
 template <typename T>
-static int xfft_smem(const Dims& d, bool linesum) {
-  return (int)(sizeof(typename cplx<T>::t) * (d.Nx + 2 * kLinesX * d.Nx) +
-               (linesum ? sizeof(double) * 2 * kLinesX * d.Nx : 0));
+static int xfft_rs(const Dims& d) {
+  int rs = d.Nx;
+  if (sizeof(T) == 8) { while (rs % 8 != 1) ++rs; }
+  else { while (rs % 2 != 1) ++rs; }
+  return rs;
+}
+
+template <typename T>
+static int xfft_smem(const Dims& d) {
+  return (int)(sizeof(typename cplx<T>::t) * ((size_t)d.Nx + (size_t)kLinesX * xfft_rs<T>(d)) +
+               sizeof(int) * (d.Nx + (d.Nx & 1)) +
+               (sizeof(T) == 4 ? sizeof(double) * 2 * kLinesX * d.Nx : 0));
 }
 
 // cluster decomposition of a kx slab: smallest power-of-two cluster whose
@@ -538,7 +622,13 @@ static bool choose_cluster(const Dims& d, int pz, int& cs, int& jc, int& rs, int
   rs = pz;
   if (sizeof(T) == 8) { while (rs % 8 != 1) ++rs; }
   else { while (rs % 4 != 2) ++rs; }
+  // a multiple of Nz (one column per thread, fixed FFT butterflies) when
+  // Nz <= kYzThreads
   nt = kYzThreads;
+  if (d.Nz <= kYzThreads) {
+    nt = d.Nz * (kYzThreads / d.Nz);
+    if (nt > 128 && d.Nz >= 128) nt = d.Nz;
+  }
   for (cs = 1; cs <= 16; cs *= 2) {
     jc = (d.Ny + cs - 1) / cs;
     if ((cs - 1) * jc >= d.Ny) continue;      // every CTA must own a row
@@ -581,7 +671,7 @@ static int launch_yz(Handle* h, typename cplx<T>::t* spec, const typename cplx<T
 template <typename T>
 static int set_limits(Handle* h, int smem_yz, int cs) {
   const Dims& d = h->d;
-  const int smx = xfft_smem<T>(d, sizeof(T) == 4);
+  const int smx = xfft_smem<T>(d);
   C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_xfft_fwd<true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
   C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_xfft_fwd<false, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
   C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_xfft_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
@@ -616,14 +706,16 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
   const FftPasses Px = get_passes(d.Nx);
   const int64_t npairs = ((int64_t)d.Ny * d.Nz + 1) / 2;
   const unsigned nbx = (unsigned)((npairs + kLinesX - 1) / kLinesX);
-  const int smx = xfft_smem<T>(d, f32);
+  const int smx = xfft_smem<T>(d);
+  const int ntx = xfft_threads(d);
+  const int rsx = xfft_rs<T>(d);
   if (parts & 1) {
     XfwdArgs<T> a{};
     a.d = d; a.m = h->m; a.U = U; a.V = V; a.W = W; a.rhs = rhs_in;
-    a.spec = spec; a.tw = twx; a.P = Px; a.lpb = kLinesX; a.pz = pz;
+    a.spec = spec; a.tw = twx; a.P = Px; a.pz = pz; a.rs = rsx;
     a.linesum = f32 ? S.linesum : nullptr;
-    if (from_div) k_xfft_fwd<true, T><<<nbx, 128, smx, s>>>(a);
-    else k_xfft_fwd<false, T><<<nbx, 128, smx, s>>>(a);
+    if (from_div) k_xfft_fwd<true, T><<<nbx, ntx, smx, s>>>(a);
+    else k_xfft_fwd<false, T><<<nbx, ntx, smx, s>>>(a);
     C3D_LAUNCH_CHECK(h);
     if (f32) {
       k_mode00<<<1, 256, sizeof(double) * d.Ny, s>>>(d, S.linesum, S.mult, S.rdp, S.du, S.phi00);
@@ -638,8 +730,8 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     XinvArgs<T> a{};
     a.d = d; a.spec = spec; a.tw = twx; a.rhs = out; a.phi1 = phi1;
     a.phi00 = f32 ? S.phi00 : nullptr; a.accumulate = accumulate;
-    a.P = Px; a.lpb = kLinesX; a.pz = pz; a.scale_div = (double)d.Nx * (double)d.Nz;
-    k_xfft_inv<T><<<nbx, 128, smx, s>>>(a);
+    a.P = Px; a.pz = pz; a.rs = rsx; a.scale_div = (double)d.Nx * (double)d.Nz;
+    k_xfft_inv<T><<<nbx, ntx, smx, s>>>(a);
     C3D_LAUNCH_CHECK(h);
   }
   if (parts == 7) h->stats.poisson_solves++;
@@ -819,8 +911,8 @@ int poisson_setup(Handle* h) {
     h->last_error = "nx_global must be even";
     return C3D_ERR_PARAM;
   }
-  if (2 * kLinesX * d.Nx > 16 * 1024 || d.Nx > 4096) {
-    h->last_error = "nx_global too large for the x FFT kernels";
+  if (d.Nx > kMaxNx) {
+    h->last_error = "nx_global too large for the x FFT kernels (nx_global - 2 <= 512)";
     return C3D_ERR_UNSUPPORTED;
   }
   int rc;
