@@ -28,6 +28,7 @@
 // slab is Ny contiguous rows of pz >= Nz complex values.
 #include <cooperative_groups.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -122,6 +123,9 @@ static int build_tri_table(Handle* h) {
     if ((rc = dev_alloc(h, &S.dl32, Ny))) return rc;
     if ((rc = dev_alloc(h, &S.du32, Ny))) return rc;
   }
+  S.h_rdp = rdp;
+  S.h_mult = mult;
+  S.h_du = du;
   cudaStream_t s = h->stream;
   C3D_CUDA_TRY(h, cudaMemcpyAsync(S.rdp, rdp.data(), nt * 8, cudaMemcpyHostToDevice, s));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(S.mult, mult.data(), nt * 8, cudaMemcpyHostToDevice, s));
@@ -131,6 +135,55 @@ static int build_tri_table(Handle* h) {
   C3D_CUDA_TRY(h, cudaMemcpyAsync(S.du, du.data(), Ny * 8, cudaMemcpyHostToDevice, s));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(S.dl32, dl32.data(), Ny * 4, cudaMemcpyHostToDevice, s));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(S.du32, du32.data(), Ny * 4, cudaMemcpyHostToDevice, s));
+  return cudaStreamSynchronize(s) == cudaSuccess ? 0 : C3D_ERR_CUDA;
+}
+
+// Homogeneous solutions of the partitioned elimination for a cluster of cs
+// CTAs with jc rows each.  CTA c owns rows j0 = c*jc .. j1; with the local
+// sweeps started from y(j0-1) = 0 and x(j1+1) = 0, the true solution is
+//   x(j) = xl(j) + Y_in * xh(j) + X_in * gh(j),  Y_in = y(j0-1), X_in = x(j1+1),
+//   h(j) = -MULT(j-1) h(j-1), h(j0-1) = 1;  xh = back substitution of h;
+//   gh(j) = -DU(j)/D'(j) gh(j+1), gh(j1+1) = 1;  Y_in(c+1) = yl_c(j1) + h_c(j1) Y_in(c).
+template <typename T>
+static int build_partition_tables(Handle* h, int cs, int jc, T** xh_d, T** gh_d, T** hend_d) {
+  const Dims& d = h->d;
+  SpectralState& S = h->sp;
+  const int Ny = d.Ny, nkx = d.nkx, nkzs = d.nkzs;
+  const int64_t nt = (int64_t)Ny * nkzs * nkx;
+  std::vector<T> xh(nt), gh(nt), hend((size_t)nkx * cs * nkzs);
+  std::vector<double> hv(Ny), xv(Ny), gv(Ny);
+  for (int m = 0; m < nkx; ++m) {
+    for (int kzs = 0; kzs < nkzs; ++kzs) {
+      auto at = [&](int j) { return ((int64_t)m * Ny + j) * nkzs + kzs; };
+      for (int c = 0; c < cs; ++c) {
+        const int j0 = c * jc, j1 = std::min(j0 + jc, Ny) - 1;
+        double hh = 1.0;
+        for (int j = j0; j <= j1; ++j) {
+          hh = (j > 0) ? -S.h_mult[at(j - 1)] * hh : 0.0;
+          hv[j] = hh;
+        }
+        hend[((size_t)m * cs + c) * nkzs + kzs] = (T)hh;
+        double xn = 0.0, gn = 1.0;
+        for (int j = j1; j >= j0; --j) {
+          const double rd = S.h_rdp[at(j)];
+          xn = (hv[j] - S.h_du[j] * xn) * rd;
+          gn = -S.h_du[j] * gn * rd;
+          xh[at(j)] = (T)xn;
+          gh[at(j)] = (T)gn;
+        }
+      }
+    }
+  }
+  int rc;
+  if (*xh_d == nullptr) {
+    if ((rc = dev_alloc(h, xh_d, nt))) return rc;
+    if ((rc = dev_alloc(h, gh_d, nt))) return rc;
+    if ((rc = dev_alloc(h, hend_d, (int64_t)hend.size()))) return rc;
+  }
+  cudaStream_t s = h->stream;
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(*xh_d, xh.data(), nt * sizeof(T), cudaMemcpyHostToDevice, s));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(*gh_d, gh.data(), nt * sizeof(T), cudaMemcpyHostToDevice, s));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(*hend_d, hend.data(), hend.size() * sizeof(T), cudaMemcpyHostToDevice, s));
   return cudaStreamSynchronize(s) == cudaSuccess ? 0 : C3D_ERR_CUDA;
 }
 
@@ -280,6 +333,9 @@ struct YzArgs {
   const T* __restrict__ rdp;     // 1/D'(j) per (m, j, kz')
   const T* __restrict__ dl;      // Dyy(j+1, j)
   const T* __restrict__ du;      // Dyy(j, j+1)
+  const T* __restrict__ xh;      // partitioned-elimination tables
+  const T* __restrict__ gh;
+  const T* __restrict__ hend;
   unsigned long long* err;       // sticky error bits
   FftPasses P;
   int cs;        // CTAs per cluster
@@ -300,6 +356,7 @@ template <typename T>
 __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
   using C = typename cplx<T>::t;
   constexpr int JM = yz_jmax<T>();
+  constexpr int kYzB = 4;   // FFT rows per batch
   constexpr int kRun = 128 / (int)sizeof(C);   // q-runs that fill a shared-memory wavefront
   extern __shared__ __align__(128) unsigned char yz_smem[];
   __shared__ __align__(8) uint64_t bar;
@@ -314,7 +371,10 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
   const int jn = min(Jc, Ny - j0);             // rows owned by this CTA (>= 1)
   C* data = reinterpret_cast<C*>(yz_smem);
   C* tw = data + (size_t)Jc * RS;
-  T* sdl = reinterpret_cast<T*>(tw + Nz);
+  C* ylast = tw + Nz;                          // local forward value of the last row
+  C* xfirst = ylast + Nz;                      // local back-substituted first row
+  C* yin = xfirst + Nz;                        // carry Y_in of this CTA
+  T* sdl = reinterpret_cast<T*>(yin + Nz);
   T* sdu = sdl + Ny;
   const int tid = threadIdx.x, nt = blockDim.x;
   C* g = a.spec + ((int64_t)m * Ny + j0) * a.pz;
@@ -337,113 +397,171 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
   if (!loaded) atomicOr(a.err, 1ull);
   __syncthreads();
 
-  fft_rows_dif<T, 4>(data, jn, RS, tw, a.P, kRun);
+  fft_rows_dif<T, kYzB>(data, jn, RS, tw, a.P, kRun);
 
-  // pivots of this thread's column for rows j0-1 .. j0+jn-1 (one column per
+  // pivots of this thread's column for rows j0 .. j0+jn-1 (one column per
   // thread when Nz <= blockDim; otherwise reloaded per column below)
   const T* rdp_m = a.rdp + (int64_t)m * Ny * nkzs;
   const bool one_col = Nz <= nt;
   T rdv[JM];
-  T rdm1 = (T)0;
   auto load_pivots = [&](int col) {
     const int kz = dif_position_to_k(col, a.P);
     const int kzs = kz <= Nz - kz ? kz : Nz - kz;
 #pragma unroll
     for (int jl = 0; jl < JM; ++jl)
       rdv[jl] = jl < jn ? __ldg(rdp_m + (int64_t)(j0 + jl) * nkzs + kzs) : (T)0;
-    rdm1 = j0 > 0 ? __ldg(rdp_m + (int64_t)(j0 - 1) * nkzs + kzs) : (T)0;
   };
   if (one_col && tid < Nz) load_pivots(tid);
 
+  // Partitioned elimination: every CTA sweeps its own rows at once from
+  // y(j0-1) = 0 and x(j1+1) = 0, publishes its last forward value and its
+  // first back-substituted value, then corrects its rows with the carries
+  //   x(j) = xl(j) + Y_in xh(j) + X_in gh(j).
   // The sweeps take rows in chunks of kCh: loads of a chunk are issued
   // together, the recurrence runs in registers, then the chunk is stored.
   constexpr int kCh = 4;
-  // forward elimination B(j) -= DL(j-1)/D'(j-1) * B(j-1)
-  for (int c = 0; c < cs; ++c) {
-    if (crank == c) {
-      const C* up = c > 0 ? cl.map_shared_rank(data, c - 1) : nullptr;
-      for (int col = tid; col < Nz; col += nt) {
-        if (!one_col) load_pivots(col);
-        C prev = c > 0 ? up[(size_t)(Jc - 1) * RS + col] : C{(T)0, (T)0};
+  for (int col = tid; col < Nz; col += nt) {
+    if (!one_col) load_pivots(col);
+    // local forward elimination B(j) -= DL(j-1)/D'(j-1) * B(j-1)
+    C prev = C{(T)0, (T)0};
 #pragma unroll
-        for (int c0 = 0; c0 < JM; c0 += kCh) {
-          if (c0 < jn) {
-            C bv[kCh];
-            T dlv[kCh];
+    for (int c0 = 0; c0 < JM; c0 += kCh) {
+      if (c0 < jn) {
+        C bv[kCh];
+        T dlv[kCh];
 #pragma unroll
-            for (int u = 0; u < kCh; ++u) {
-              const int jl = c0 + u;
-              bv[u] = C{(T)0, (T)0};
-              dlv[u] = (T)0;
-              if (jl < jn) {
-                bv[u] = data[jl * RS + col];
-                if (j0 + jl > 0) dlv[u] = sdl[j0 + jl - 1];
-              }
+        for (int u = 0; u < kCh; ++u) {
+          const int jl = c0 + u;
+          bv[u] = C{(T)0, (T)0};
+          dlv[u] = (T)0;
+          if (jl < jn) {
+            bv[u] = data[jl * RS + col];
+            if (jl > 0) dlv[u] = sdl[j0 + jl - 1];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kCh; ++u) {
+          const int jl = c0 + u;
+          if (jl < jn) {
+            if (jl > 0) {
+              const T mu = dlv[u] * rdv[jl > 0 ? jl - 1 : 0];
+              bv[u].x = bv[u].x - mu * prev.x;
+              bv[u].y = bv[u].y - mu * prev.y;
             }
+            prev = bv[u];
+          }
+        }
 #pragma unroll
-            for (int u = 0; u < kCh; ++u) {
-              const int jl = c0 + u;
-              if (jl < jn) {
-                // row 0 of the slab has no predecessor (dlv = 0, prev = 0)
-                const T mu = dlv[u] * (jl == 0 ? rdm1 : rdv[jl > 0 ? jl - 1 : 0]);
-                bv[u].x = bv[u].x - mu * prev.x;
-                bv[u].y = bv[u].y - mu * prev.y;
-                prev = bv[u];
-              }
-            }
+        for (int u = 0; u < kCh; ++u)
+          if (c0 + u < jn) data[(c0 + u) * RS + col] = bv[u];
+      }
+    }
+    ylast[col] = prev;
+    // local back substitution x(j) = (B(j) - DU(j) x(j+1)) / D'(j)
+    C xn = C{(T)0, (T)0};
 #pragma unroll
-            for (int u = 0; u < kCh; ++u)
-              if (c0 + u < jn) data[(c0 + u) * RS + col] = bv[u];
+    for (int c0 = JM - kCh; c0 >= 0; c0 -= kCh) {
+      if (c0 < jn) {
+        C bv[kCh];
+        T duv[kCh];
+#pragma unroll
+        for (int u = 0; u < kCh; ++u) {
+          const int jl = c0 + u;
+          bv[u] = C{(T)0, (T)0};
+          duv[u] = (T)0;
+          if (jl < jn) {
+            bv[u] = data[jl * RS + col];
+            duv[u] = sdu[j0 + jl];
+          }
+        }
+#pragma unroll
+        for (int u = kCh - 1; u >= 0; --u) {
+          const int jl = c0 + u;
+          if (jl < jn) {
+            bv[u].x = (bv[u].x - duv[u] * xn.x) * rdv[jl];
+            bv[u].y = (bv[u].y - duv[u] * xn.y) * rdv[jl];
+            xn = bv[u];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kCh; ++u)
+          if (c0 + u < jn) data[(c0 + u) * RS + col] = bv[u];
+      }
+    }
+    xfirst[col] = xn;
+  }
+  cl.sync();
+  // carries: Y_in(c+1) = ylast_c + hend_c Y_in(c) forward over the cluster,
+  // published per CTA; then X_in(c-1) = xfirst_c + Y_in(c) xh_c(j0) + X_in(c) gh_c(j0)
+  // backward from the last CTA (X_in = 0 there)
+  const T* xh_m = a.xh + (int64_t)m * Ny * nkzs;
+  const T* gh_m = a.gh + (int64_t)m * Ny * nkzs;
+  const T* hend_m = a.hend + (int64_t)m * cs * nkzs;
+  for (int col = tid; col < Nz; col += nt) {
+    const int kz = dif_position_to_k(col, a.P);
+    const int kzs = kz <= Nz - kz ? kz : Nz - kz;
+    C Y = C{(T)0, (T)0};
+    for (int c = 0; c < crank; ++c) {
+      const C yl = cl.map_shared_rank(ylast, c)[col];
+      const T he = __ldg(hend_m + (int64_t)c * nkzs + kzs);
+      Y.x = yl.x + he * Y.x;
+      Y.y = yl.y + he * Y.y;
+    }
+    yin[col] = Y;
+  }
+  cl.sync();
+  for (int col = tid; col < Nz; col += nt) {
+    const int kz = dif_position_to_k(col, a.P);
+    const int kzs = kz <= Nz - kz ? kz : Nz - kz;
+    const C Y = yin[col];
+    C X = C{(T)0, (T)0};
+    for (int c = cs - 1; c > crank; --c) {
+      const C xf = cl.map_shared_rank(xfirst, c)[col];
+      const C yc = cl.map_shared_rank(yin, c)[col];
+      const int64_t o = (int64_t)(c * Jc) * nkzs + kzs;
+      const T xhf = __ldg(xh_m + o), ghf = __ldg(gh_m + o);
+      C Xn;
+      Xn.x = xf.x + yc.x * xhf + X.x * ghf;
+      Xn.y = xf.y + yc.y * xhf + X.y * ghf;
+      X = Xn;
+    }
+    // correction of this CTA's rows
+#pragma unroll
+    for (int c0 = 0; c0 < JM; c0 += kCh) {
+      if (c0 < jn) {
+        C bv[kCh];
+        T xv[kCh], gv[kCh];
+#pragma unroll
+        for (int u = 0; u < kCh; ++u) {
+          const int jl = c0 + u;
+          bv[u] = C{(T)0, (T)0};
+          xv[u] = (T)0;
+          gv[u] = (T)0;
+          if (jl < jn) {
+            const int64_t o = (int64_t)(j0 + jl) * nkzs + kzs;
+            bv[u] = data[jl * RS + col];
+            xv[u] = __ldg(xh_m + o);
+            gv[u] = __ldg(gh_m + o);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kCh; ++u) {
+          if (c0 + u < jn) {
+            bv[u].x += Y.x * xv[u] + X.x * gv[u];
+            bv[u].y += Y.y * xv[u] + X.y * gv[u];
+            data[(c0 + u) * RS + col] = bv[u];
           }
         }
       }
     }
-    cl.sync();
+    if (a.zero00 && m == 0 && col == 0)
+      for (int jl = 0; jl < jn; ++jl) data[jl * RS] = C{(T)0, (T)0};
   }
-  // back substitution x(j) = (B(j) - DU(j) x(j+1)) / D'(j), DU(Ny-1) = 0
-  for (int c = cs - 1; c >= 0; --c) {
-    if (crank == c) {
-      const C* dn = c < cs - 1 ? cl.map_shared_rank(data, c + 1) : nullptr;
-      for (int col = tid; col < Nz; col += nt) {
-        if (!one_col) load_pivots(col);
-        C xn = c < cs - 1 ? dn[col] : C{(T)0, (T)0};
-#pragma unroll
-        for (int c0 = JM - kCh; c0 >= 0; c0 -= kCh) {
-          if (c0 < jn) {
-            C bv[kCh];
-            T duv[kCh];
-#pragma unroll
-            for (int u = 0; u < kCh; ++u) {
-              const int jl = c0 + u;
-              bv[u] = C{(T)0, (T)0};
-              duv[u] = (T)0;
-              if (jl < jn) {
-                bv[u] = data[jl * RS + col];
-                duv[u] = sdu[j0 + jl];
-              }
-            }
-#pragma unroll
-            for (int u = kCh - 1; u >= 0; --u) {
-              const int jl = c0 + u;
-              if (jl < jn) {
-                bv[u].x = (bv[u].x - duv[u] * xn.x) * rdv[jl];
-                bv[u].y = (bv[u].y - duv[u] * xn.y) * rdv[jl];
-                xn = bv[u];
-              }
-            }
-#pragma unroll
-            for (int u = 0; u < kCh; ++u)
-              if (c0 + u < jn) data[(c0 + u) * RS + col] = bv[u];
-          }
-        }
-        if (a.zero00 && m == 0 && col == 0)
-          for (int jl = 0; jl < jn; ++jl) data[jl * RS] = C{(T)0, (T)0};
-      }
-    }
-    cl.sync();
-  }
+  __syncthreads();
 
-  fft_rows_dit_inv<T, 4>(data, jn, RS, tw, a.P, kRun);
+  fft_rows_dit_inv<T, kYzB>(data, jn, RS, tw, a.P, kRun);
+  // no CTA leaves while another may still read its ylast / xfirst
+  cl.sync();
 
   fence_async_shared();
   __syncthreads();
@@ -633,7 +751,7 @@ static bool choose_cluster(const Dims& d, int pz, int& cs, int& jc, int& rs, int
     jc = (d.Ny + cs - 1) / cs;
     if ((cs - 1) * jc >= d.Ny) continue;      // every CTA must own a row
     if (jc > yz_jmax<T>()) continue;
-    const size_t bytes = esz * ((size_t)jc * rs + d.Nz) + 2 * sizeof(T) * d.Ny;
+    const size_t bytes = esz * ((size_t)jc * rs + 4 * (size_t)d.Nz) + 2 * sizeof(T) * d.Ny;
     if (bytes <= 112 * 1024 || (cs == 16 && bytes <= 224 * 1024)) {
       smem = (int)bytes;
       return true;
@@ -644,11 +762,12 @@ static bool choose_cluster(const Dims& d, int pz, int& cs, int& jc, int& rs, int
 
 template <typename T>
 static int launch_yz(Handle* h, typename cplx<T>::t* spec, const typename cplx<T>::t* tw, const T* rdp,
-                     const T* dl, const T* du, int cs, int jc, int rs, int pz, int nt, int smem,
-                     int zero00) {
+                     const T* dl, const T* du, const T* xh, const T* gh, const T* hend, int cs, int jc,
+                     int rs, int pz, int nt, int smem, int zero00) {
   const Dims& d = h->d;
   YzArgs<T> a{};
   a.d = d; a.spec = spec; a.tw = tw; a.rdp = rdp; a.dl = dl; a.du = du;
+  a.xh = xh; a.gh = gh; a.hend = hend;
   a.err = &h->sc->err;
   a.P = get_passes(d.Nz); a.cs = cs; a.jc = jc; a.rs = rs; a.pz = pz; a.zero00 = zero00;
   cudaLaunchConfig_t cfg{};
@@ -692,15 +811,17 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
   using C = typename cplx<T>::t;
   C* spec;
   const C *twx, *twz;
-  const T *rdp, *dl, *du;
+  const T *rdp, *dl, *du, *xh, *gh, *hend;
   int cs, jc, rs, pz, nt, smem;
   if (f32) {
     spec = (C*)S.spec32; twx = (const C*)S.twx32; twz = (const C*)S.twz32;
     rdp = (const T*)S.rdp32; dl = (const T*)S.dl32; du = (const T*)S.du32;
+    xh = (const T*)S.xh32; gh = (const T*)S.gh32; hend = (const T*)S.hend32;
     cs = S.cs32; jc = S.jc32; rs = S.rs32; pz = S.pz32; nt = S.nt32; smem = S.smem32;
   } else {
     spec = (C*)S.spec; twx = (const C*)S.twx; twz = (const C*)S.twz;
     rdp = (const T*)S.rdp; dl = (const T*)S.dl; du = (const T*)S.du;
+    xh = (const T*)S.xh; gh = (const T*)S.gh; hend = (const T*)S.hend;
     cs = S.cs64; jc = S.jc64; rs = S.rs64; pz = S.pz64; nt = S.nt64; smem = S.smem64;
   }
   const FftPasses Px = get_passes(d.Nx);
@@ -723,7 +844,7 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     }
   }
   if (parts & 2) {
-    int rc = launch_yz<T>(h, spec, twz, rdp, dl, du, cs, jc, rs, pz, nt, smem, f32 ? 1 : 0);
+    int rc = launch_yz<T>(h, spec, twz, rdp, dl, du, xh, gh, hend, cs, jc, rs, pz, nt, smem, f32 ? 1 : 0);
     if (rc) return rc;
   }
   if (parts & 4) {
@@ -928,7 +1049,12 @@ int poisson_setup(Handle* h) {
     if ((rc = dev_alloc(h, &S.spec, ns))) return rc;
     if ((rc = set_limits<double>(h, S.smem64, S.cs64))) return rc;
   }
-  return build_tri_table(h);
+  if ((rc = build_tri_table(h))) return rc;
+  if ((rc = build_partition_tables<double>(h, S.cs64, S.jc64, &S.xh, &S.gh, &S.hend))) return rc;
+  if (S.spec32 != nullptr &&
+      (rc = build_partition_tables<float>(h, S.cs32, S.jc32, &S.xh32, &S.gh32, &S.hend32)))
+    return rc;
+  return 0;
 }
 
 int mixed_setup(Handle* h) {
@@ -948,6 +1074,7 @@ int mixed_setup(Handle* h) {
   if ((rc = dev_alloc(h, &S.linesum, (int64_t)d.Ny * d.Nz))) return rc;
   if ((rc = dev_alloc(h, &S.phi00, d.Ny))) return rc;
   if ((rc = set_limits<float>(h, S.smem32, S.cs32))) return rc;
+  if ((rc = build_partition_tables<float>(h, S.cs32, S.jc32, &S.xh32, &S.gh32, &S.hend32))) return rc;
   C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return 0;
 }
