@@ -141,6 +141,88 @@ def cores_used():
         return os.cpu_count() or 1
 
 
+def measure_mixed(steps=10):
+    """Mixed-precision Poisson against the FP64 path: steps/s of each and the
+    max-norm relative difference of u, v, w after ``steps`` steps from the same
+    seeded state."""
+    import numpy as np
+    out = {}
+    fields = {}
+    for mode in ("fp64", "mixed"):
+        ch = make_channel(mode)
+        ch.compute_time_step_RK3(steps)
+        fields[mode] = {n: ch.download(n) for n in ("U", "V", "W")}
+        ch.compute_time_step_RK3(50)
+        out[mode] = {"steps_per_s": 1e3 / ch.last_step_time_ms(), "max_div": ch.check_divergence()}
+        if mode == "mixed":
+            out[mode]["refinement_sweeps"] = ch.stats()["refinement_sweeps"]
+        ch.close()
+    out["max_rel_diff_after_%d_steps" % steps] = {
+        n: float(np.abs(fields["mixed"][n] - fields["fp64"][n]).max() / np.abs(fields["fp64"][n]).max())
+        for n in ("U", "V", "W")}
+    return out
+
+
+def make_ib_channel(maxit):
+    """cfg2: the 192x129x192 channel with an immersed plane at y = 0.2 above
+    the lower wall (y = -0.8 in wall-centred coordinates), 192x192 markers,
+    standing wave 0.02 sin(2 pi x/Lx) cos(2 pi t/5); uniform wall buffer
+    (grid_type 2) so the delta stencils of the plane lie in uniform y cells."""
+    import channel3d_parallel_b200 as c3d
+    ch = c3d.Channel(nx_global=NX, ny_global=NY, nz_global=NZ, Lxp=LX, Lzp=LZ, nu=NU, CFL=-DT,
+                     x_mass_cte=1, grid_type=2, alpha_stretch=2.0, min_buffer_width=0.3,
+                     dPdx=3.0 * NU, body_type="wall_standing_wave", nxb=NX - 2, nzb=NZ - 2,
+                     body_param_1=0.02, body_param_2=2 * math.pi / 5, body_param_3=1.0,
+                     body_param_4=0.2, cg_tol=1e-10, cg_max_iter=maxit)
+    ch.compute_heaviside()
+    c3d.seeded_initial_state(ch, 3.0 * NU, NU)
+    return ch
+
+
+def measure_ib(maxit=50, steps=2):
+    """Schur BiCGSTAB of the IB projection on cfg2 for each preconditioner:
+    iterations and device ms per solve (3 solves per step), ms per iteration
+    (2 Schur applications) and the residual reached."""
+    import channel3d_parallel_b200 as c3d
+    L = c3d.lib
+
+    def run(ch, n):
+        s0 = ch.stats()
+        ch.compute_time_step_RK3(n)
+        s1 = ch.stats()
+        ns = s1["bicgstab_solves"] - s0["bicgstab_solves"]
+        it = s1["bicgstab_iters"] - s0["bicgstab_iters"]
+        ms = s1["bicgstab_ms"] - s0["bicgstab_ms"]
+        return {"iters_per_solve": it / ns, "ms_per_solve": ms / ns, "ms_per_iter": ms / max(it, 1),
+                "iters_per_step": it / n, "last_residual": s1["last_residual"],
+                "fallbacks": s1["precond_fallbacks"] - s0["precond_fallbacks"]}
+
+    res = {"config": "cfg2 plane y=0.2, 192x192 markers, standing wave A=0.02 omega=2pi/5",
+           "markers": (NX - 2) * (NZ - 2), "cg_tol": 1e-10, "cg_max_iter": maxit, "modes": {}}
+    for name, mode in (("none", L.PRECOND_NONE), ("jacobi", L.PRECOND_JACOBI), ("spai", L.PRECOND_SPAI)):
+        ch = make_ib_channel(maxit)
+        ch.set_mode(precond=mode)
+        res["modes"][name] = run(ch, steps)
+        ch.close()
+    ch = make_ib_channel(maxit)
+    ch.set_mode(precond=L.PRECOND_JACOBI)
+    t0 = time.perf_counter()
+    for _ in range(3):                 # probe pairs at three geometries (stages of Jacobi steps)
+        ch.precond_probe()
+        ch.compute_time_step_RK3(1)
+    t_probe = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    loss = ch.precond_train(epochs=400, lr=2e-3)
+    t_train = time.perf_counter() - t0
+    ch.set_mode(precond=L.PRECOND_LEARNED)
+    r = run(ch, steps)
+    r.update({"train_loss": loss, "train_s": t_train, "probe_and_step_s": t_probe,
+              "pairs": ch.precond_info()["pairs"]})
+    res["modes"]["learned"] = r
+    ch.close()
+    return res
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -273,6 +355,10 @@ def run_ours(args):
         e2e_sec = float(t.item())
     e2e_val = ws / e2e_sec
 
+    extras = {}
+    if ws == 1 and not args.no_extras:
+        extras["mixed_vs_fp64"] = measure_mixed()
+        extras["ib_schur"] = measure_ib(maxit=args.ib_maxit)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         sec = cpu_baseline_sample(1)
@@ -305,6 +391,7 @@ def run_ours(args):
         "clocks": clk,
         "max_div": div,
     }
+    line.update(extras)
     print(json.dumps(line), flush=True)
 
 
@@ -316,6 +403,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--poisson", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-precision and IB Schur-solve measurements")
+    ap.add_argument("--ib-maxit", type=int, default=50,
+                    help="BiCGSTAB iteration cap of the IB measurement (reference default 50)")
     ap.add_argument("--device-only", action="store_true",
                     help="only the device-timed step loop (used for profiler captures)")
     args = ap.parse_args()

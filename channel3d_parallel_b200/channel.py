@@ -291,6 +291,54 @@ class Channel:
         self._check(self._lib.c3d_kernel_launches(self.handle, C.byref(v)))
         return v.value
 
+    # ---- learned preconditioner of the Schur solve ----
+    def precond_collect(self, enable=True, max_store=48, max_sets=16):
+        """Collect (residual, correction) moments from converged Schur solves."""
+        self._check(self._lib.c3d_precond_collect(self.handle, int(bool(enable)), int(max_store),
+                                                  int(max_sets)))
+
+    def precond_probe(self):
+        """Add one training set of probed (correction, response) moments."""
+        self._check(self._lib.c3d_precond_probe(self.handle))
+
+    def precond_train(self, epochs=400, lr=2e-3):
+        """Train the network on the collected sets; returns the relative loss."""
+        v = C.c_double(0.0)
+        self._check(self._lib.c3d_precond_train(self.handle, int(epochs), float(lr), C.byref(v)))
+        return v.value
+
+    def precond_info(self):
+        pairs, sets, epochs, loss = C.c_int64(0), C.c_int(0), C.c_int(0), C.c_double(0)
+        self._check(self._lib.c3d_precond_info(self.handle, C.byref(pairs), C.byref(sets),
+                                               C.byref(epochs), C.byref(loss)))
+        return {"pairs": pairs.value, "sets": sets.value, "epochs": epochs.value,
+                "loss": loss.value}
+
+    def precond_params(self):
+        """(parameters[PRECOND_NPARAM], sig[8]) as float32 arrays."""
+        buf = np.zeros(L.PRECOND_NPARAM + 8, dtype=np.float32)
+        self._check(self._lib.c3d_precond_get_params(self.handle, L.fptr(buf), len(buf)))
+        return buf[:L.PRECOND_NPARAM].copy(), buf[L.PRECOND_NPARAM:].copy()
+
+    def precond_set_params(self, params, sig=None):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        sg = None if sig is None else np.ascontiguousarray(sig, dtype=np.float32)
+        self._check(self._lib.c3d_precond_set_params(self.handle, L.fptr(p), len(p),
+                                                     L.fptr(sg) if sg is not None else None))
+
+    def precond_eval(self, feats, moments, sig):
+        """Network output, loss and parameter gradient on caller data."""
+        f = np.ascontiguousarray(feats, dtype=np.float32)
+        mo = np.ascontiguousarray(moments, dtype=np.float32)
+        sg = np.ascontiguousarray(sig, dtype=np.float32)
+        m = f.shape[0]
+        out = np.zeros((m, 16), dtype=np.float32)
+        grad = np.zeros(L.PRECOND_NPARAM, dtype=np.float32)
+        loss = C.c_double(0.0)
+        self._check(self._lib.c3d_precond_eval(self.handle, L.fptr(f), L.fptr(mo), m, L.fptr(sg),
+                                               L.fptr(out), L.fptr(grad), C.byref(loss)))
+        return out, grad, loss.value
+
 
 def laminar_perturbed_fields(grid, dims, dPdx, nu, Ly=2.0, amplitude=0.1, seed=0):
     """Host fields of the seeded initial state: laminar profile

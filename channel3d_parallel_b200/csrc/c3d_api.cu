@@ -244,6 +244,7 @@ static void free_handle(Handle* h) {
   if (h->device >= 0) cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   ib_free(h);
+  mlp_free(h);
   mixed_free(h);
   if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
   for (void* p : h->allocations) cudaFree(p);
@@ -457,7 +458,7 @@ static int sync_scalars_from_device(Handle* h) {
 // ---------------------------------------------------------------------------
 static int enqueue_step(Handle* h, double dt, double to) {
   static const double rk_t[3] = {8.0 / 15.0, 2.0 / 3.0, 1.0};
-  int rc;
+  int rc, warn = 0;
   for (int s = 1; s <= 3; ++s) {
     if ((rc = launch_rhs_stage(h, s, dt))) return rc;
     if ((rc = launch_fill_ghosts3(h, h->Us, h->Vs, h->Ws))) return rc;
@@ -469,17 +470,21 @@ static int enqueue_step(Handle* h, double dt, double to) {
     }
     if ((rc = launch_projection_step(h, s, dt))) return rc;   // :117-118, :123
     if (h->ib) {
-      if ((rc = ib_projection(h, dt, s))) return rc;          // :119-122
+      // a Schur solve that reached cg_max_iter is a warning: the reference
+      // stops iterating and completes the step (src/projection.f90:60)
+      rc = ib_projection(h, dt, s);                           // :119-122
+      if (rc < 0) return rc;
+      if (rc > 0) warn = rc;
     }
   }
   if (h->p.x_mass_cte == 1) {                                  // :187-193
     if ((rc = launch_massflow_correction(h, dt))) return rc;
   }
-  return 0;
+  return warn;
 }
 
 static int run_steps(Handle* h, int nsteps) {
-  int rc;
+  int rc, warn = 0;
   C3D_CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
   for (int n = 0; n < nsteps; ++n) {
     double dt;
@@ -512,7 +517,9 @@ static int run_steps(Handle* h, int nsteps) {
       h->P_pending = true;
       h->P_pending_dt = dt;
     } else {
-      if ((rc = enqueue_step(h, dt, to))) return rc;
+      rc = enqueue_step(h, dt, to);
+      if (rc < 0) return rc;
+      if (rc > 0) warn = rc;
     }
     h->t = to + 1.0 * dt;
     h->stats.steps++;
@@ -523,8 +530,12 @@ static int run_steps(Handle* h, int nsteps) {
   C3D_CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
   h->last_step_ms = nsteps > 0 ? ms / nsteps : 0.0;
   C3D_CUDA_TRY(h, cudaGetLastError());
-  return sync_scalars_from_device(h);
+  if ((rc = sync_scalars_from_device(h))) return rc;
+  if (warn) h->last_error = "a Schur solve stopped at cg_max_iter before reaching cg_tol";
+  return warn;
 }
+
+Handle* lookup_handle(int id) { return lookup(id); }
 
 }  // namespace c3d
 
@@ -750,7 +761,7 @@ int c3d_set_mode(int id, int poisson_mode, int precond_mode) {
   GET_HANDLE(id);
   if (poisson_mode != C3D_POISSON_FP64 && poisson_mode != C3D_POISSON_MIXED &&
       poisson_mode != C3D_POISSON_MIXED_UNREFINED) RET(h, C3D_ERR_PARAM);
-  if (precond_mode < C3D_PRECOND_NONE || precond_mode > C3D_PRECOND_LEARNED) RET(h, C3D_ERR_PARAM);
+  if (precond_mode < C3D_PRECOND_NONE || precond_mode > C3D_PRECOND_SPAI) RET(h, C3D_ERR_PARAM);
   if (poisson_mode != C3D_POISSON_FP64) {
     int rc = mixed_setup(h);
     if (rc) RET(h, rc);

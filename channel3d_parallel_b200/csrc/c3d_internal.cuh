@@ -144,6 +144,7 @@ int parse_namelist(const std::string& text, Params& p, std::string& err);
 void set_global_error(const std::string& msg);
 
 struct IbState;   // immersed-boundary state (k_ib.cu)
+struct MlpState;  // learned preconditioner network (k_mlp.cu)
 struct MixedState;  // mixed-precision work buffers (k_poisson.cu)
 
 struct Handle {
@@ -187,6 +188,7 @@ struct Handle {
   double last_step_ms = 0;
   IbState* ib = nullptr;
   MixedState* mixed = nullptr;
+  MlpState* mlp = nullptr;
   // one RK3 step captured as a CUDA graph (valid for graph_dt)
   cudaGraphExec_t step_exec = nullptr;
   double graph_dt = 0;
@@ -256,6 +258,7 @@ int compute_dt_cfl(Handle* h, double* dt);
 // immersed boundary (k_ib.cu)
 int ib_create(Handle* h);
 void ib_free(Handle* h);
+void mlp_free(Handle* h);
 int ib_setup_geometry(Handle* h, double t);
 int ib_setup_operators(Handle* h);
 int ib_heaviside(Handle* h);

@@ -1,0 +1,72 @@
+// Immersed-boundary state shared by the IB operators (k_ib.cu) and the
+// learned preconditioner (k_mlp.cu).
+#pragma once
+#include <string>
+#include <vector>
+
+#include "c3d_internal.cuh"
+
+namespace c3d {
+
+struct IbState {
+  std::string kind;
+  bool moving = false;
+  int nb = 0, nbodies = 0;
+  // host geometry
+  std::vector<double> xb, yb, zb, ub, nrm, sb;
+  std::vector<int> yref, body;
+  std::vector<int> body_count;
+  // device geometry
+  double *xb_d = nullptr, *yb_d = nullptr, *zb_d = nullptr, *ub_d = nullptr, *nrm_d = nullptr, *sb_d = nullptr;
+  int *yref_d = nullptr, *body_d = nullptr;
+  double* binv_d = nullptr;          // 1/markers per body
+  // 1-D grids (Fortran-indexed) for the weight kernel
+  double *x_d = nullptr, *y_d = nullptr, *z_d = nullptr, *xm_d = nullptr, *ym_d = nullptr, *zm_d = nullptr;
+  // operator tables: [type(4)][axis(3)][a(5)][nb]
+  int* idx_d = nullptr;
+  double* w1_d = nullptr;
+  double* off_d = nullptr;
+  int* flag_d = nullptr;
+  // fields
+  double *Ureg = nullptr, *Vreg = nullptr, *Wreg = nullptr;
+  double *Hu = nullptr, *Hv = nullptr, *Hw = nullptr;     // interior Heaviside
+  double *Hce = nullptr;                                  // Hc exterior (rhs_p extents)
+  double *Ut = nullptr, *Vt = nullptr, *Wt = nullptr;     // scratch fields
+  // marker vectors
+  double *fb = nullptr, *E1nHc = nullptr, *E1nH = nullptr;
+  double *rhs = nullptr, *scr0 = nullptr, *scr1 = nullptr, *scr2 = nullptr;
+  double *r = nullptr, *rhat = nullptr, *p = nullptr, *nu = nullptr, *ph = nullptr, *s = nullptr;
+  double *sh = nullptr, *t = nullptr;
+  double* red = nullptr;             // partial sums
+  double* sc = nullptr;              // BiCGSTAB scalars
+  // marker lattice: index = ix + lat_nx * iz (every body type lays its markers
+  // out row by row); lat_nx = nb when there is no second direction
+  int lat_nx = 0;
+  // preconditioner: per-marker 4x4 blocks [nb][4][4] acting on
+  // (r[b], r[nb+b], r[2nb+b], r[3nb+b]); the Jacobi blocks are diagonal
+  double* jac_blk = nullptr;
+  double* lrn_blk = nullptr;
+  double* spai_blk = nullptr;        // probed block sparse approximate inverse
+  double* prb = nullptr;             // [4][4nb] probe responses of one colour class
+  bool have_jac = false, have_lrn = false;
+  std::vector<double> yb_at_jac;     // marker y when the Jacobi diagonal was probed
+  int jac_clipped[4] = {0, 0, 0, 0}; // safeguarded diagonal entries per component
+  double dt_at_jac = 0;
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr;   // Schur-solve timing
+  ~IbState() {
+    if (ev_a) cudaEventDestroy(ev_a);
+    if (ev_b) cudaEventDestroy(ev_b);
+  }
+};
+
+
+// learned-preconditioner entry points used by the Schur solver (k_mlp.cu)
+int mlp_build_blocks(Handle* h, double dt);               // lrn_blk from the network
+bool mlp_collecting(const Handle* h);                     // training-pair collection on
+int mlp_store_iterate(Handle* h, const double* x, const double* r, int k);
+int mlp_collect_solve(Handle* h, int iters_stored);       // moments from the stored iterates
+// probe pass of the Schur operator (k_ib.cu): Jacobi and SPAI blocks, and,
+// when mom is not null, per-marker SPAI moments [nb][36]
+int ib_probe(Handle* h, double dt, float* mom);
+
+}  // namespace c3d

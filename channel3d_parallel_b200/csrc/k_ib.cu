@@ -15,49 +15,17 @@
 //  - the reference's marker partition, support planes and MPI gathers are
 //    replaced by direct indexing of the resident fields: a stencil point on
 //    the periodic duplicate centre plane nzg-1 is folded onto plane 2.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "c3d_internal.cuh"
+#include "ib_state.cuh"
 
 namespace c3d {
 
 static const double kPiIb = 4.0 * std::atan(1.0);
-
-struct IbState {
-  std::string kind;
-  bool moving = false;
-  int nb = 0, nbodies = 0;
-  // host geometry
-  std::vector<double> xb, yb, zb, ub, nrm, sb;
-  std::vector<int> yref, body;
-  std::vector<int> body_count;
-  // device geometry
-  double *xb_d = nullptr, *yb_d = nullptr, *zb_d = nullptr, *ub_d = nullptr, *nrm_d = nullptr, *sb_d = nullptr;
-  int *yref_d = nullptr, *body_d = nullptr;
-  double* binv_d = nullptr;          // 1/markers per body
-  // 1-D grids (Fortran-indexed) for the weight kernel
-  double *x_d = nullptr, *y_d = nullptr, *z_d = nullptr, *xm_d = nullptr, *ym_d = nullptr, *zm_d = nullptr;
-  // operator tables: [type(4)][axis(3)][a(5)][nb]
-  int* idx_d = nullptr;
-  double* w1_d = nullptr;
-  double* off_d = nullptr;
-  int* flag_d = nullptr;
-  // fields
-  double *Ureg = nullptr, *Vreg = nullptr, *Wreg = nullptr;
-  double *Hu = nullptr, *Hv = nullptr, *Hw = nullptr;     // interior Heaviside
-  double *Hce = nullptr;                                  // Hc exterior (rhs_p extents)
-  double *Ut = nullptr, *Vt = nullptr, *Wt = nullptr;     // scratch fields
-  // marker vectors
-  double *fb = nullptr, *E1nHc = nullptr, *E1nH = nullptr;
-  double *rhs = nullptr, *scr0 = nullptr, *scr1 = nullptr, *scr2 = nullptr;
-  double *r = nullptr, *rhat = nullptr, *p = nullptr, *nu = nullptr, *ph = nullptr, *s = nullptr;
-  double *sh = nullptr, *t = nullptr, *minv = nullptr;
-  double* red = nullptr;             // partial sums
-  double* sc = nullptr;              // BiCGSTAB scalars
-  bool have_minv = false;
-};
 
 // ---------------------------------------------------------------------------
 // host geometry: setup_IB_geometry (src/immersed_boundary_geometry.f90:70-398)
@@ -71,11 +39,13 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
     s->xb.assign(nb, 0); s->yb.assign(nb, 0); s->zb.assign(nb, 0);
     s->ub.assign(3 * nb, 0); s->nrm.assign(3 * nb, 0); s->sb.assign(nb, 0);
     s->yref.assign(nb, 1); s->body.assign(nb, 0);
+    s->lat_nx = nb;
   };
   if (s->kind == "center_wall") {                                     // :80-115
     if (p.grid_type != 0) { err = "Error: body type is incompatible with grid type"; return C3D_ERR_PARAM; }
     const int nb = nxb * nzb;
     resize(nb);
+    s->lat_nx = nxb;
     const double dxb = Lxp / nxb, dzb = Lzp / nzb;
     for (int j = 1; j <= nzb; ++j)
       for (int i = 1; i <= nxb; ++i) {
@@ -96,6 +66,7 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
     const int nw = two ? 2 : 1;
     const int nb = nw * nxb * nzb;
     resize(nb);
+    s->lat_nx = nw * nxb;
     const double dxb = Lxp / nxb, dzb = Lzp / nzb;
     const double A = p.body_param_1, om = p.body_param_2, b3 = p.body_param_3;
     const double y0 = two ? 0.0 : p.body_param_4;
@@ -157,6 +128,7 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
   } else if (s->kind == "traveling_wave_x") {                          // :271-390
     const int nb = 2 * nxb * nzb;
     resize(nb);
+    s->lat_nx = 2 * nxb;
     const double dxb = Lxp / nxb, dzb = Lzp / nzb;
     const double b1 = p.body_param_1, b2 = p.body_param_2, b3 = p.body_param_3, tr = p.body_ramp_up_time;
     double amp, damp;
@@ -215,6 +187,7 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
     const int nxbt = nxb1 + nxb2;
     const int nb = nxbt * nzb;
     resize(nb);
+    s->lat_nx = nxbt;
     const double xc = 0.5 * Lxp, yc = 0.5 * p.Ly_channel;
     const double dsb1 = 2 * 3.14159 * r1 / nxb1, dsb2 = 2 * 3.14159 * r2 / nxb2;
     for (int j = 1; j <= nzb; ++j) {
@@ -676,6 +649,104 @@ __global__ void k_bcg_init(double* sc) {
   sc[0] = 1.0; sc[1] = 1.0; sc[2] = 1.0; sc[5] = 1.0;
 }
 
+// out_b = B_b in_b for every marker b, with in_b = (in[b], in[nb+b],
+// in[2nb+b], in[3nb+b]) and B_b the 4x4 block blk[16*b ..] (row-major)
+__global__ void k_apply_blocks(int nb, const double* __restrict__ blk, const double* __restrict__ in,
+                               double* __restrict__ out) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    double v[4], B[16];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) v[c] = in[(int64_t)c * nb + b];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) B[q] = blk[16 * (int64_t)b + q];
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      out[(int64_t)c * nb + b] = B[4 * c] * v[0] + B[4 * c + 1] * v[1] + B[4 * c + 2] * v[2] + B[4 * c + 3] * v[3];
+  }
+}
+
+// probe vector of one colour class: unit entries in block `blk` on the
+// markers with (ix mod px, iz mod pz) = (cx, cz), ix = l mod lat_nx, iz = l / lat_nx
+__global__ void k_probe_mask(int nb, int lat_nx, int blk, int px, int pz, int cx, int cz,
+                             double* __restrict__ e) {
+  const int64_t n = 4 * (int64_t)nb;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i / nb), l = (int)(i - (int64_t)c * nb);
+    const int ix = l % lat_nx, iz = l / lat_nx;
+    e[i] = (c == blk && ix % px == cx && iz % pz == cz) ? 1.0 : 0.0;
+  }
+}
+
+// Per marker of the probed colour class, from the responses R_c = S e_c of
+// the four component probes: the column block C_b of S restricted to the
+// lattice neighbourhood N(b) (|dix| <= 2, |diz| <= 2, periodic, all four
+// components), G_b = C_b^T C_b and the diagonal block S_bb.  Outputs the
+// Jacobi block diag(1/S_bb,cc), the block sparse approximate inverse
+// M_b = G_b^-1 S_bb^T (minimiser of ||e_b - C_b M_b||_F, the marker's block
+// column of min ||I - S M||_F), and optionally the moments Crr = G_b,
+// Cer = S_bb, Cee = 1 (36 floats) for training.
+__global__ void k_probe_spai(int nb, int lat, int nrow, int px, int pz, int cx, int cz,
+                             const double* __restrict__ R, double* __restrict__ jac,
+                             double* __restrict__ spai, float* __restrict__ mom) {
+  const int64_t n = 4 * (int64_t)nb;
+  for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nb; l += gridDim.x * blockDim.x) {
+    const int ix = l % lat, iz = l / lat;
+    if (ix % px != cx || iz % pz != cz) continue;
+    double G[16] = {0}, S[16];
+    for (int dz = -2; dz <= 2; ++dz)
+      for (int dx = -2; dx <= 2; ++dx) {
+        const int jx = (ix + dx + lat) % lat, jz = (iz + dz + nrow) % nrow;
+        const int lp = jx + lat * jz;
+        if (lp >= nb) continue;
+        for (int cr = 0; cr < 4; ++cr) {
+          const int64_t row = (int64_t)cr * nb + lp;
+          double v[4];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) v[c] = R[(int64_t)c * n + row];
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) G[4 * a + b] += v[a] * v[b];
+        }
+      }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) S[4 * a + c] = R[(int64_t)c * n + (int64_t)a * nb + l];
+    for (int c = 0; c < 4; ++c) {
+      const double dg = S[5 * c];
+      jac[16 * (int64_t)l + 5 * c] = (fabs(dg) > 1e-300) ? 1.0 / dg : 1.0;
+    }
+    // M = G^-1 S^T by Gauss-Jordan with partial pivoting on [G | S^T]
+    double Aug[4][8];
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) { Aug[a][b] = G[4 * a + b]; Aug[a][4 + b] = S[4 * b + a]; }
+    bool sing = false;
+    for (int c = 0; c < 4; ++c) {
+      int piv = c;
+      for (int r = c + 1; r < 4; ++r) if (fabs(Aug[r][c]) > fabs(Aug[piv][c])) piv = r;
+      if (!(fabs(Aug[piv][c]) > 1e-300)) { sing = true; break; }
+      if (piv != c)
+        for (int q = 0; q < 8; ++q) { const double t = Aug[c][q]; Aug[c][q] = Aug[piv][q]; Aug[piv][q] = t; }
+      const double inv = 1.0 / Aug[c][c];
+      for (int q = 0; q < 8; ++q) Aug[c][q] *= inv;
+      for (int r = 0; r < 4; ++r)
+        if (r != c) {
+          const double f = Aug[r][c];
+          for (int q = 0; q < 8; ++q) Aug[r][q] -= f * Aug[c][q];
+        }
+    }
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b)
+        spai[16 * (int64_t)l + 4 * a + b] = sing ? (a == b ? jac[16 * (int64_t)l + 5 * a] : 0.0) : Aug[a][4 + b];
+    if (mom) {
+      float* m = mom + 36 * (int64_t)l;
+      for (int q = 0; q < 16; ++q) { m[q] = (float)G[q]; m[16 + q] = (float)S[q]; }
+      for (int q = 0; q < 4; ++q) m[32 + q] = 1.f;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // IB projection final update: U = Ui - Ureg - G(dt*Pint - phi2)
 // ---------------------------------------------------------------------------
@@ -820,9 +891,12 @@ int ib_create(Handle* h) {
   if ((rc = dev_alloc(h, &s->Vt, sizeV(d)))) return rc;
   if ((rc = dev_alloc(h, &s->Wt, sizeW(d)))) return rc;
   double** vecs[] = {&s->fb, &s->E1nHc, &s->E1nH, &s->rhs, &s->scr0, &s->scr1, &s->scr2, &s->r,
-                     &s->rhat, &s->p, &s->nu, &s->ph, &s->s, &s->sh, &s->t, &s->minv};
+                     &s->rhat, &s->p, &s->nu, &s->ph, &s->s, &s->sh, &s->t};
   for (auto v : vecs)
     if ((rc = dev_alloc(h, v, 4 * (int64_t)nb))) return rc;
+  if ((rc = dev_alloc(h, &s->jac_blk, 16 * (int64_t)nb))) return rc;
+  if ((rc = dev_alloc(h, &s->lrn_blk, 16 * (int64_t)nb))) return rc;
+  if ((rc = dev_alloc(h, &s->spai_blk, 16 * (int64_t)nb))) return rc;
   if ((rc = dev_alloc(h, &s->red, 2 * kIbRedBlocks + 16))) return rc;
   if ((rc = dev_alloc(h, &s->sc, 16))) return rc;
   // H = 1 (interior) until compute_heaviside runs (app/main.f90:80-85)
@@ -870,7 +944,7 @@ int ib_setup_operators(Handle* h) {
   C3D_CUDA_TRY(h, cudaMemcpyAsync(&flag, s->flag_d, 4, cudaMemcpyDeviceToHost, h->stream));
   C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   if (flag) { h->last_error = "Error: zi_supp out of range (marker stencil outside the grid)"; return C3D_ERR_PARAM; }
-  s->have_minv = false;
+  s->have_lrn = false;
   return 0;
 }
 
@@ -1000,24 +1074,25 @@ static int dot(Handle* h, const double* a, const double* b, const double* c, con
 // diagonal (Jacobi) preconditioner: diag(S) estimated by probing with
 // well-separated unit vectors per unknown block
 static int build_jacobi(Handle* h, double dt);
+static bool jacobi_stale(Handle* h, double dt);
 
-// bicgstab(x, b), src/projection.f90:146-186 (right-preconditioned with a
-// diagonal when the Jacobi mode is selected)
-int ib_bicgstab(Handle* h, const double* b, double dt) {
+// bicgstab(x, b), src/projection.f90:146-186, right-preconditioned with
+// per-marker 4x4 blocks when a preconditioner is selected.
+// Preconditioner modes: NONE (the reference's unpreconditioned solver),
+// JACOBI (diagonal blocks from lattice probing), SPAI (probed 4x4 block
+// sparse approximate inverse), LEARNED (4x4 blocks per marker from the
+// network, which also supplies a warm start x0 += M r0).  In
+// LEARNED mode the solve falls back to Jacobi, restarting from the current
+// iterate, when the residual stalls (the best residual of the last
+// kStallWindow iterations is not 1 % below the best before them) or breaks
+// down (non-finite scalars; restart from the entry guess).
+static const int kStallWindow = 20;
+
+static int bcg_restart(Handle* h, const double* b, double* x, double dt, unsigned gb) {
   IbState* s = h->ib;
   const int64_t n = 4 * (int64_t)s->nb;
-  const unsigned gb = 148 * 4;
   int rc;
-  const double* minv = nullptr;
-  if (h->precond_mode != C3D_PRECOND_NONE) {
-    if (!s->have_minv) {
-      if ((rc = build_jacobi(h, dt))) return rc;
-    }
-    minv = s->minv;
-  }
-  double* x = s->fb;
-  // r = b - S x
-  if ((rc = ib_schur(h, x, s->r, dt))) return rc;
+  if ((rc = ib_schur(h, x, s->r, dt))) return rc;                    // r = b - S x
   k_axpby<<<gb, 256, 0, h->stream>>>(n, 1.0, b, -1.0, s->r, s->r);
   C3D_LAUNCH_CHECK(h);
   C3D_CUDA_TRY(h, cudaMemcpyAsync(s->rhat, s->r, 8 * n, cudaMemcpyDeviceToDevice, h->stream));
@@ -1025,17 +1100,65 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
   C3D_CUDA_TRY(h, cudaMemsetAsync(s->p, 0, 8 * n, h->stream));
   k_bcg_init<<<1, 1, 0, h->stream>>>(s->sc);
   C3D_LAUNCH_CHECK(h);
+  return 0;
+}
+
+int ib_bicgstab(Handle* h, const double* b, double dt) {
+  IbState* s = h->ib;
+  const int nb = s->nb;
+  const int64_t n = 4 * (int64_t)nb;
+  const unsigned gb = 148 * 4;
+  const unsigned gm = (unsigned)((nb + 255) / 256);
+  int rc;
+  int mode = h->precond_mode;
+  if (mode == C3D_PRECOND_LEARNED && !s->have_lrn) {
+    if ((rc = mlp_build_blocks(h, dt))) return rc;
+  }
+  if (mode != C3D_PRECOND_NONE && jacobi_stale(h, dt)) {
+    if ((rc = build_jacobi(h, dt))) return rc;
+  }
+  const double* blk = mode == C3D_PRECOND_LEARNED ? s->lrn_blk
+                      : mode == C3D_PRECOND_JACOBI ? s->jac_blk
+                      : mode == C3D_PRECOND_SPAI   ? s->spai_blk : nullptr;
+  double* x = s->fb;
+  if (!s->ev_a) {
+    C3D_CUDA_TRY(h, cudaEventCreate(&s->ev_a));
+    C3D_CUDA_TRY(h, cudaEventCreate(&s->ev_b));
+  }
+  C3D_CUDA_TRY(h, cudaEventRecord(s->ev_a, h->stream));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->scr1, x, 8 * n, cudaMemcpyDeviceToDevice, h->stream));
+  if ((rc = bcg_restart(h, b, x, dt, gb))) return rc;
+  if (mode == C3D_PRECOND_LEARNED) {
+    // warm start x0 += M r0
+    k_apply_blocks<<<gm, 256, 0, h->stream>>>(nb, blk, s->r, s->scr2);
+    C3D_LAUNCH_CHECK(h);
+    k_axpby<<<gb, 256, 0, h->stream>>>(n, 1.0, x, 1.0, s->scr2, x);
+    C3D_LAUNCH_CHECK(h);
+    if ((rc = bcg_restart(h, b, x, dt, gb))) return rc;
+  }
+  const bool collect = mlp_collecting(h);
   const double eps = h->p.cg_tol * h->p.cg_tol;
   double err = 1.0;
-  int it = 0;
+  int it = 0, stored = 0;
+  std::vector<double> hist;
   while (it < h->p.cg_max_iter && err >= eps) {
+    if (collect && (rc = mlp_store_iterate(h, x, s->r, stored))) return rc;
+    if (collect) ++stored;
     if ((rc = dot(h, s->rhat, s->r, nullptr, nullptr, 0))) return rc;           // rho_n, bta
-    k_bcg_p<<<gb, 256, 0, h->stream>>>(n, s->r, s->p, s->nu, s->ph, minv, s->sc);
+    k_bcg_p<<<gb, 256, 0, h->stream>>>(n, s->r, s->p, s->nu, s->ph, nullptr, s->sc);
     C3D_LAUNCH_CHECK(h);
+    if (blk) {
+      k_apply_blocks<<<gm, 256, 0, h->stream>>>(nb, blk, s->p, s->ph);
+      C3D_LAUNCH_CHECK(h);
+    }
     if ((rc = ib_schur(h, s->ph, s->nu, dt))) return rc;
     if ((rc = dot(h, s->rhat, s->nu, nullptr, nullptr, 1))) return rc;          // alpha
-    k_bcg_s<<<gb, 256, 0, h->stream>>>(n, s->r, s->nu, s->s, s->sh, x, s->ph, minv, s->sc);
+    k_bcg_s<<<gb, 256, 0, h->stream>>>(n, s->r, s->nu, s->s, s->sh, x, s->ph, nullptr, s->sc);
     C3D_LAUNCH_CHECK(h);
+    if (blk) {
+      k_apply_blocks<<<gm, 256, 0, h->stream>>>(nb, blk, s->s, s->sh);
+      C3D_LAUNCH_CHECK(h);
+    }
     if ((rc = ib_schur(h, s->sh, s->t, dt))) return rc;
     if ((rc = dot(h, s->t, s->s, s->t, s->t, 2))) return rc;                    // om
     k_bcg_x<<<kIbRedBlocks, 256, 0, h->stream>>>(n, x, s->r, s->s, s->sh, s->t, s->sc, s->red);
@@ -1045,7 +1168,38 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
     C3D_CUDA_TRY(h, cudaMemcpyAsync(&err, s->sc + 5, 8, cudaMemcpyDeviceToHost, h->stream));
     C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     ++it;
+    hist.push_back(err);
+    if (mode == C3D_PRECOND_LEARNED) {
+      const bool broke = !(err == err) || std::isinf(err);
+      // stall: the best residual of the last kStallWindow iterations is not
+      // 1 % below the best one before them
+      bool stalled = false;
+      if ((int)hist.size() > kStallWindow) {
+        const size_t cut = hist.size() - kStallWindow;
+        const double before = *std::min_element(hist.begin(), hist.begin() + cut);
+        const double recent = *std::min_element(hist.begin() + cut, hist.end());
+        stalled = recent > 0.98 * before;   // squared norms: |r| down < 1 %
+      }
+      if (broke || stalled) {
+        h->stats.precond_fallbacks++;
+        mode = C3D_PRECOND_JACOBI;
+        blk = s->jac_blk;
+        if (broke)   // the iterate may be polluted: restart from the entry guess
+          C3D_CUDA_TRY(h, cudaMemcpyAsync(x, s->scr1, 8 * n, cudaMemcpyDeviceToDevice, h->stream));
+        if ((rc = bcg_restart(h, b, x, dt, gb))) return rc;
+        hist.clear();
+        err = 1.0;
+      }
+    }
   }
+  if (collect && err < eps && (rc = mlp_collect_solve(h, stored))) return rc;
+  C3D_CUDA_TRY(h, cudaEventRecord(s->ev_b, h->stream));
+  C3D_CUDA_TRY(h, cudaEventSynchronize(s->ev_b));
+  float ms = 0.f;
+  C3D_CUDA_TRY(h, cudaEventElapsedTime(&ms, s->ev_a, s->ev_b));
+  h->stats.last_bicgstab_ms = ms;
+  h->stats.bicgstab_ms += ms;
+  h->stats.precond_mode = mode;
   h->stats.bicgstab_solves++;
   h->stats.bicgstab_iters += it;
   h->stats.last_bicgstab_iters = it;
@@ -1055,38 +1209,71 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
   return 0;
 }
 
-static int build_jacobi(Handle* h, double dt) {
-  // probe: unit entries on every P-th marker of one block, P = 8; the diagonal
-  // of the probed markers is read from S e; unprobed markers take the value of
-  // the probed marker below them in index order (a translation-invariant
-  // estimate on the lattice bodies)
+// Probe pass: lattice colour classes (ix = cx mod px, iz = cz mod pz, px =
+// pz = 5, beyond the 5-point delta support), one unit probe per component and
+// class, 4*px*pz Schur applications in all.  Fills the Jacobi and SPAI
+// blocks; with mom != null also the SPAI training moments.
+int ib_probe(Handle* h, double dt, float* mom) {
   IbState* s = h->ib;
   const int nb = s->nb;
   const int64_t n = 4 * (int64_t)nb;
-  const int P = 8;
-  std::vector<double> diag(n, 0.0), e(n), Se(n);
-  for (int blk = 0; blk < 4; ++blk) {
-    for (int phase = 0; phase < 1; ++phase) {
-      std::fill(e.begin(), e.end(), 0.0);
-      for (int l = phase; l < nb; l += P) e[(int64_t)blk * nb + l] = 1.0;
-      C3D_CUDA_TRY(h, cudaMemcpyAsync(s->scr0, e.data(), 8 * n, cudaMemcpyHostToDevice, h->stream));
-      int rc = ib_schur(h, s->scr0, s->scr1, dt);
-      if (rc) return rc;
-      C3D_CUDA_TRY(h, cudaMemcpyAsync(Se.data(), s->scr1, 8 * n, cudaMemcpyDeviceToHost, h->stream));
-      C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-      for (int l = 0; l < nb; ++l) {
-        const int src = (l / P) * P + phase;
-        const int64_t i = (int64_t)blk * nb + (src < nb ? src : l);
-        diag[(int64_t)blk * nb + l] = Se[i];
+  const int lat = s->lat_nx > 0 ? s->lat_nx : nb;
+  const int nrow = (nb + lat - 1) / lat;
+  const int px = std::min(5, lat), pz = std::min(5, nrow);
+  const unsigned gb = 148 * 4;
+  int rc;
+  if (s->prb == nullptr && (rc = dev_alloc(h, &s->prb, 4 * n))) return rc;
+  C3D_CUDA_TRY(h, cudaMemsetAsync(s->jac_blk, 0, 16 * 8 * (size_t)nb, h->stream));
+  for (int cz = 0; cz < pz; ++cz)
+    for (int cx = 0; cx < px; ++cx) {
+      for (int blk = 0; blk < 4; ++blk) {
+        k_probe_mask<<<gb, 256, 0, h->stream>>>(nb, lat, blk, px, pz, cx, cz, s->scr0);
+        C3D_LAUNCH_CHECK(h);
+        if ((rc = ib_schur(h, s->scr0, s->prb + (size_t)blk * n, dt))) return rc;
+      }
+      k_probe_spai<<<(nb + 127) / 128, 128, 0, h->stream>>>(nb, lat, nrow, px, pz, cx, cz, s->prb, s->jac_blk,
+                                                            s->spai_blk, mom);
+      C3D_LAUNCH_CHECK(h);
+    }
+  // safeguard: the diagonal of S can be small or change sign on some markers
+  // (a moving plane crossing the stretched y cells); entries below 0.2 of the
+  // component's median magnitude, or of the other sign, take the median
+  std::vector<double> jb((size_t)16 * nb);
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(jb.data(), s->jac_blk, 8 * jb.size(), cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  for (int c = 0; c < 4; ++c) {
+    std::vector<double> dg(nb);
+    for (int l = 0; l < nb; ++l) dg[l] = 1.0 / jb[16 * (size_t)l + 5 * c];
+    std::vector<double> tmp(dg);
+    std::nth_element(tmp.begin(), tmp.begin() + nb / 2, tmp.end());
+    const double med = tmp[nb / 2];
+    int clipped = 0;
+    for (int l = 0; l < nb; ++l) {
+      const double d = dg[l];
+      if (!(std::fabs(d) >= 0.2 * std::fabs(med)) || (d > 0) != (med > 0)) {
+        jb[16 * (size_t)l + 5 * c] = 1.0 / med;
+        ++clipped;
       }
     }
+    s->jac_clipped[c] = clipped;
   }
-  std::vector<double> minv(n);
-  for (int64_t i = 0; i < n; ++i) minv[i] = (std::fabs(diag[i]) > 1e-300) ? 1.0 / diag[i] : 1.0;
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->minv, minv.data(), 8 * n, cudaMemcpyHostToDevice, h->stream));
-  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  s->have_minv = true;
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->jac_blk, jb.data(), 8 * jb.size(), cudaMemcpyHostToDevice, h->stream));
+  s->have_jac = true;
+  s->yb_at_jac = s->yb;
+  s->dt_at_jac = dt;
   return 0;
+}
+
+static int build_jacobi(Handle* h, double dt) { return ib_probe(h, dt, nullptr); }
+
+// the Jacobi blocks are re-probed when dt changed or a marker moved by more
+// than a tenth of the smallest wall-normal spacing since the last probe
+static bool jacobi_stale(Handle* h, double dt) {
+  IbState* s = h->ib;
+  if (!s->have_jac || s->dt_at_jac != dt || s->yb_at_jac.size() != s->yb.size()) return true;
+  double mx = 0.0;
+  for (size_t k = 0; k < s->yb.size(); ++k) mx = std::max(mx, std::fabs(s->yb[k] - s->yb_at_jac[k]));
+  return mx > 0.1 * h->dymin;
 }
 
 // compute_heaviside, src/heaviside.f90:20-54
@@ -1112,7 +1299,7 @@ int ib_heaviside(Handle* h) {
   if ((rc = launch_fill_ghosts3(h, s->Hu, s->Hv, s->Hw))) return rc;              // :49
   if ((rc = gather_c(h, s->Hce, 1.0, s->E1nHc))) return rc;                       // :51
   if ((rc = gather3(h, G_E1N, s->Ut, s->Vt, s->Wt, s->E1nH))) return rc;          // :52
-  s->have_minv = false;
+  s->have_lrn = false;
   return 0;
 }
 

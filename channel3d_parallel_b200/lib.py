@@ -25,7 +25,7 @@ FIELD = dict(U=1, V=2, W=3, P=4, RHS_P=5, P_INTERIM=6, RHS_U=7, RHS_V=8, RHS_W=9
              HU_INTERIOR=16, HV_INTERIOR=17, HW_INTERIOR=18, HC_EXTERIOR=19)
 MARKER = dict(FB=40, UB=41, XB=42, YB=43, ZB=44, NORMALS=45, SB=46, E1NH_EXT=47, E1NHC_EXT=48)
 POISSON_FP64, POISSON_MIXED, POISSON_MIXED_UNREFINED = 0, 1, 2
-PRECOND_NONE, PRECOND_JACOBI, PRECOND_LEARNED = 0, 1, 2
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_LEARNED, PRECOND_SPAI = 0, 1, 2, 3
 
 
 class Dims(C.Structure):
@@ -40,10 +40,12 @@ class Stats(C.Structure):
                 ("precond_fallbacks", C.c_int64), ("last_residual", C.c_double),
                 ("dPdx", C.c_double), ("dPdy", C.c_double), ("dPdz", C.c_double),
                 ("t", C.c_double), ("dt", C.c_double), ("qflow_x_0", C.c_double),
-                ("status", C.c_int32)]
+                ("status", C.c_int32), ("precond_mode", C.c_int32),
+                ("last_bicgstab_ms", C.c_double), ("bicgstab_ms", C.c_double)]
 
 
 _D = C.POINTER(C.c_double)
+_F = C.POINTER(C.c_float)
 _I64x3 = C.POINTER(C.c_int64)
 _INT = C.c_int
 
@@ -91,7 +93,15 @@ PROTOTYPES = {
     "c3d_profile_kernels": [_INT, _INT, _D, _INT],
     "c3d_mean_mass_flow_u_noalloc": [C.c_void_p, _INT, _INT, _INT, C.c_void_p, C.c_void_p,
                                      C.c_void_p],
+    "c3d_precond_collect": [_INT, _INT, _INT, _INT],
+    "c3d_precond_probe": [_INT],
+    "c3d_precond_train": [_INT, _INT, C.c_double, _D],
+    "c3d_precond_info": [_INT, C.POINTER(C.c_int64), C.POINTER(C.c_int), C.POINTER(C.c_int), _D],
+    "c3d_precond_get_params": [_INT, _F, _INT],
+    "c3d_precond_set_params": [_INT, _F, _INT, _F],
+    "c3d_precond_eval": [_INT, _F, _F, _INT, _F, _F, _F, _D],
 }
+PRECOND_NPARAM = 22800
 KERNEL_CLASSES = ("rhs_stage", "ghosts", "div_xfft", "spectral_yz", "xfft_inv", "grad_sub",
                   "massflow")
 
@@ -132,6 +142,11 @@ def check(rc, handle=0):
 def dptr(a):
     """Pointer to the data of a contiguous float64 numpy array."""
     return a.ctypes.data_as(_D)
+
+
+def fptr(a):
+    """Pointer to the data of a contiguous float32 numpy array."""
+    return a.ctypes.data_as(_F)
 
 
 def box(lb, ub):

@@ -81,6 +81,7 @@ extern "C" {
 #define C3D_PRECOND_NONE        0   /* reference BiCGSTAB (unpreconditioned)    */
 #define C3D_PRECOND_JACOBI      1   /* diagonal (Jacobi) preconditioner         */
 #define C3D_PRECOND_LEARNED     2   /* learned preconditioner + warm start      */
+#define C3D_PRECOND_SPAI        3   /* probed 4x4 block sparse approximate inverse */
 
 typedef struct c3d_dims {
   int32_t nx, ny, nz;          /* nx_global, ny_global, nz_global            */
@@ -102,6 +103,9 @@ typedef struct c3d_stats {
   double  t, dt;               /* simulation time and last dt                 */
   double  qflow_x_0;           /* target bulk flow                            */
   int32_t status;              /* last status code                            */
+  int32_t precond_mode;        /* preconditioner of the last Schur solve      */
+  double  last_bicgstab_ms;    /* device time of the last Schur solve (ms)    */
+  double  bicgstab_ms;         /* accumulated device time of Schur solves     */
 } c3d_stats;
 
 /* ---- lifecycle ------------------------------------------------------------
@@ -208,6 +212,37 @@ int c3d_kernel_launches(int handle, int64_t* count);
  * rhs_stage, ghosts, div_xfft, spectral_yz, xfft_inv, grad_sub, massflow
  * (FP64 kernels).  Writes min(nmax, 7) entries.                              */
 int c3d_profile_kernels(int handle, int nrep, double* ms, int nmax);
+
+/* ---- learned preconditioner / warm start of the IB Schur solve ------------
+ * No reference counterpart (the reference's bicgstab, src/projection.f90:146-186,
+ * is unpreconditioned).  A per-marker 4x4 block z_b = A_b r_b with A_b predicted
+ * from 32 geometry features by an MLP 32-128-128-16 (BF16 weights, FP32
+ * accumulation, tcgen05 tensor cores); selected with c3d_set_mode(...,
+ * C3D_PRECOND_LEARNED).  The solve falls back to Jacobi when it stalls.
+ *
+ * c3d_precond_collect: while enabled, converged Schur solves keep up to
+ *   max_store iterates and add one training set (moments of the residual /
+ *   correction pairs of that geometry); up to max_sets sets are kept.
+ * c3d_precond_train: full-batch Adam over the collected sets; final_loss is
+ *   the relative least-squares loss (1 = no better than zero correction).
+ * c3d_precond_probe: probe the Schur operator on the current geometry with
+ *   lattice colour classes (100 applications) and add one training set of
+ *   (unit correction, response) moments: the block sparse-approximate-inverse
+ *   target min ||I - S M||_F.  All sets of one network use one kind of pairs.
+ * c3d_precond_info: pairs used, sets, epochs trained, last loss.
+ * c3d_precond_get_params / set_params: the packed FP32 parameters
+ *   (C3D_PRECOND_NPARAM values; get_params appends sig_r[4], sig_e[4]).
+ * c3d_precond_eval: forward, loss and parameter gradient on caller data
+ *   (m rows of 32 features and 36 moments; sig = sig_r[4], sig_e[4]). */
+#define C3D_PRECOND_NPARAM 22800
+int c3d_precond_collect(int handle, int enable, int max_store, int max_sets);
+int c3d_precond_probe(int handle);
+int c3d_precond_train(int handle, int epochs, double lr, double* final_loss);
+int c3d_precond_info(int handle, int64_t* pairs, int* sets, int* epochs, double* last_loss);
+int c3d_precond_get_params(int handle, float* params, int n);
+int c3d_precond_set_params(int handle, const float* params, int n, const float* sig);
+int c3d_precond_eval(int handle, const float* feats, const float* moments, int m, const float* sig,
+                     float* out, float* grad, double* loss);
 
 /* ---- allocation-free entry ------------------------------------------------
  * No counterpart in the reference.  Bulk flux of U, the value of
