@@ -25,7 +25,7 @@ def small_channel():
                        CFL=-1e-3, grid_type=0, alpha_stretch=0.0)
 
 
-@pytest.mark.parametrize("m", [128, 300])
+@pytest.mark.parametrize("m", [128, 300, 16384])
 def test_network_forward_and_gradient_match_oracle(m):
     p, X, mom, sig = mo.random_case(m, seed=m)
     with small_channel() as ch:
