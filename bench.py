@@ -179,7 +179,7 @@ def make_ib_channel(maxit):
     return ch
 
 
-def measure_ib(maxit=50, steps=2):
+def measure_ib(maxit=50, steps=2, modes=("none", "jacobi", "spai", "learned")):
     """Schur BiCGSTAB of the IB projection on cfg2 for each preconditioner:
     iterations and device ms per solve (3 solves per step), ms per iteration
     (2 Schur applications) and the residual reached."""
@@ -200,10 +200,14 @@ def measure_ib(maxit=50, steps=2):
     res = {"config": "cfg2 plane y=0.2, 192x192 markers, standing wave A=0.02 omega=2pi/5",
            "markers": (NX - 2) * (NZ - 2), "cg_tol": 1e-10, "cg_max_iter": maxit, "modes": {}}
     for name, mode in (("none", L.PRECOND_NONE), ("jacobi", L.PRECOND_JACOBI), ("spai", L.PRECOND_SPAI)):
+        if name not in modes:
+            continue
         ch = make_ib_channel(maxit)
         ch.set_mode(precond=mode)
         res["modes"][name] = run(ch, steps)
         ch.close()
+    if "learned" not in modes:
+        return res
     ch = make_ib_channel(maxit)
     ch.set_mode(precond=L.PRECOND_JACOBI)
     t0 = time.perf_counter()
@@ -407,11 +411,18 @@ def main():
                     help="skip the mixed-precision and IB Schur-solve measurements")
     ap.add_argument("--ib-maxit", type=int, default=50,
                     help="BiCGSTAB iteration cap of the IB measurement (reference default 50)")
+    ap.add_argument("--only-ib", action="store_true",
+                    help="only the IB Schur-solve measurement (--steps steps per preconditioner)")
+    ap.add_argument("--ib-modes", default="none,jacobi,spai,learned")
     ap.add_argument("--device-only", action="store_true",
                     help="only the device-timed step loop (used for profiler captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.only_ib:
+        print(json.dumps(measure_ib(maxit=args.ib_maxit, steps=args.steps,
+                                    modes=tuple(args.ib_modes.split(",")))), flush=True)
+        return
     if args.impl == "reference":
         if args.steps > 20:
             args.steps = 10     # each CPU step is a full RK3 step (seconds)

@@ -242,6 +242,8 @@ int launch_rhs_only(Handle* h, int component);
 int poisson_setup(Handle* h);
 int launch_divergence(Handle* h, const double* U, const double* V, const double* W, double* rhs);
 int launch_poisson_solve(Handle* h, double* rhs, int rk_step, double dt);
+int launch_poisson_of_div(Handle* h, const double* U, const double* V, const double* W, double* out,
+                          int rk_step, double dt);
 int launch_projection_step(Handle* h, int rk_step, double dt);
 int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, const double* Wi,
                              const double* phi, double dt, double* Uo, double* Vo, double* Wo);

@@ -39,6 +39,7 @@ struct IbState {
   double *sh = nullptr, *t = nullptr;
   double* red = nullptr;             // partial sums
   double* sc = nullptr;              // BiCGSTAB scalars
+  unsigned* ticket = nullptr;        // last-block counter of the body sums
   // marker lattice: index = ix + lat_nx * iz (every body type lays its markers
   // out row by row); lat_nx = nb when there is no second direction
   int lat_nx = 0;

@@ -217,6 +217,88 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
       }
     }
     s->nbodies = 2;
+  } else if (s->kind == "two_cylinders_z") {
+    // extension: two separate spanwise cylinders of radius body_param_1,
+    // counter-rotating with surface speeds +-body_param_2, centred at
+    // (body_param_3, Ly/2) and (2 body_param_3, Ly/2 + body_param_4); nxb
+    // markers around each, nzb spanwise; conventions of double_cylinders_z
+    // (src/immersed_boundary_geometry.f90:117-174): normals point out of the
+    // fluid (into each cylinder), sb = arc length x dz, one body per cylinder
+    if (p.grid_type != 0) { err = "Error: body type is incompatible with grid type"; return C3D_ERR_PARAM; }
+    const double r = p.body_param_1, us = p.body_param_2;
+    const double dzb = Lzp / nzb, dsb = 2.0 * kPiIb * r / nxb;
+    const int nb = 2 * nxb * nzb;
+    resize(nb);
+    s->lat_nx = 2 * nxb;
+    const double xc[2] = {p.body_param_3, 2.0 * p.body_param_3};
+    const double yc[2] = {0.5 * p.Ly_channel, 0.5 * p.Ly_channel + p.body_param_4};
+    const double sgn[2] = {1.0, -1.0};
+    for (int j = 1; j <= nzb; ++j)
+      for (int c = 0; c < 2; ++c)
+        for (int i = 1; i <= nxb; ++i) {
+          const int k = i + c * nxb + 2 * nxb * (j - 1) - 1;
+          const double th = (double)(i - 1) * 2.0 * kPiIb / nxb;
+          s->xb[k] = xc[c] + r * std::cos(th);
+          s->yb[k] = yc[c] + r * std::sin(th);
+          s->zb[k] = ((double)j - 0.5) * dzb;
+          s->ub[k] = -sgn[c] * us * std::sin(th);
+          s->ub[nb + k] = sgn[c] * us * std::cos(th);
+          s->sb[k] = dsb * dzb;
+          s->nrm[k] = -std::cos(th);
+          s->nrm[nb + k] = -std::sin(th);
+          s->body[k] = c;
+        }
+    s->nbodies = 2;
+  } else if (s->kind == "wall_plates") {
+    // extension: nxb x nzb thin plates standing on the lower wall, height
+    // h = body_param_1, width half the spanwise pitch, 32 x 16 markers each
+    // (up x across); plate (pi, pj) bends in x with the tip displacement
+    // a sin(omega t + phi), a = body_param_2, omega = body_param_3, phase phi
+    // from the splitmix64 stream seeded with body_param_4:
+    //   x = x_p + a (y/h)^2 sin(omega t + phi),  u_b = d/dt of it,
+    //   n = (1, -dx/dy, 0)/|.|,  32 marker rows from y0 = 3 dymin (the
+    //   lowest height whose delta stencil stays above the wall) to the tip h.
+    // Marker (k, m) of plate (pi, pj) sits at lattice (ix, iz) =
+    // ((pi-1)*32 + k-1, (pj-1)*16 + m-1); all plates form one body.
+    constexpr int my = 32, mz = 16;
+    const double hh = p.body_param_1, amp = p.body_param_2, om = p.body_param_3;
+    const double pitchx = Lxp / nxb, pitchz = Lzp / nzb, wz = 0.5 * pitchz;
+    const int nb = nxb * nzb * my * mz;
+    resize(nb);
+    s->lat_nx = nxb * my;
+    uint64_t st = (uint64_t)(int64_t)std::llround(p.body_param_4);
+    std::vector<double> phase(nxb * nzb);
+    for (auto& ph : phase) {
+      st += 0x9E3779B97F4A7C15ull;
+      uint64_t z = st;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      z ^= z >> 31;
+      ph = 2.0 * kPiIb * (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    }
+    for (int pj = 1; pj <= nzb; ++pj)
+      for (int m = 1; m <= mz; ++m)
+        for (int pi = 1; pi <= nxb; ++pi)
+          for (int kk = 1; kk <= my; ++kk) {
+            const int ix = (pi - 1) * my + kk - 1, iz = (pj - 1) * mz + m - 1;
+            const int k = ix + s->lat_nx * iz;
+            const double ph = phase[(pi - 1) + nxb * (pj - 1)];
+            const double y0 = 3.0 * h->dymin;
+            const double y = y0 + (kk - 1) * (hh - y0) / (my - 1), eta = y / hh;
+            const double sn = std::sin(om * t + ph), cs = std::cos(om * t + ph);
+            s->xb[k] = (pi - 0.5) * pitchx + amp * eta * eta * sn;
+            s->yb[k] = y;
+            s->zb[k] = (pj - 0.5) * pitchz + ((double)m - 0.5 - 0.5 * mz) * (wz / mz);
+            s->ub[k] = amp * eta * eta * om * cs;
+            const double slope = 2.0 * amp * y / (hh * hh) * sn;
+            const double nn = std::sqrt(1.0 + slope * slope);
+            s->nrm[k] = 1.0 / nn;
+            s->nrm[nb + k] = -slope / nn;
+            s->sb[k] = ((hh - 3.0 * h->dymin) / (my - 1)) * (wz / mz);
+            s->yref[k] = 1;
+            s->body[k] = 0;
+          }
+    s->nbodies = 1;
   } else {
     err = "Error: No corresponding body type found for: " + s->kind;
     return C3D_ERR_PARAM;
@@ -410,56 +492,71 @@ __device__ __forceinline__ int64_t lin(int n1, int n2, int i, int j, int k, int 
   return (int64_t)(i - 1) + (int64_t)n1 * ((j - 1) + (int64_t)n2 * (k - 1));
 }
 
-__global__ void __launch_bounds__(256) k_ib_gather(GatherArgs a) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+// one thread per (marker, component): the 15 one-dimensional weights and
+// indices of its stencil load coalesced (consecutive markers, consecutive
+// addresses), then the 5x5x5 tensor product is walked in registers
+__global__ void __launch_bounds__(128) k_ib_gather(GatherArgs a) {
   const int nb = a.T.nb;
-  if (warp >= nb * a.ncomp) return;
-  const int c = warp / nb;
-  const int l = warp - c * nb;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nb * a.ncomp) return;
+  const int c = gid / nb;
+  const int l = gid - c * nb;
   const int t = a.type[c];
   const OpTables& T = a.T;
-  const double nx_ = T.nrm[l], ny_ = T.nrm[nb + l], nz_ = T.nrm[2 * nb + l];
-  double acc = 0.0;
-  for (int pnt = lane; pnt < 125; pnt += 32) {
-    const int qk = pnt / 25, qj = (pnt / 5) % 5, qi = pnt % 5;
-    const int ix = T.idx[tslot(nb, t, 0, qi, l)];
-    const int iy = T.idx[tslot(nb, t, 1, qj, l)];
-    const int iz = T.idx[tslot(nb, t, 2, qk, l)];
-    const double w = T.scale * T.w1[tslot(nb, t, 0, qi, l)] * T.w1[tslot(nb, t, 1, qj, l)] *
-                     T.w1[tslot(nb, t, 2, qk, l)];
-    double v;
-    if (a.mode == G_GRAD) {
-      const Dims& d = a.d;
-      const double* P = a.phi;
-      double gv = 0.0;
-      const double p0 = P[idxR(d, ix, iy, iz)];
-      if (t == 0) gv = (P[idxR(d, ix + 1, iy, iz)] - p0) * a.m.rdxg[ix];
-      else if (t == 1) gv = (iy >= 2 && iy <= d.ny - 1) ? (P[idxR(d, ix, iy + 1, iz)] - p0) * a.m.rdyg[iy] : 0.0;
-      else gv = (P[idxR(d, ix, iy, iz + 1)] - p0) * a.m.rdzg[iz];
-      const GField& g = a.f[c];
-      v = gv * a.phimul - a.reg[c][lin(g.n1, g.n2, ix, iy, iz, 0)];
-    } else {
-      const GField& g = a.f[c];
-      v = g.F[lin(g.n1, g.n2, ix, iy, iz, g.rhsp)] * g.mul;
-    }
-    double term = w * v;
-    if (a.mode == G_E1N) {
-      const double dxn = nx_ * T.off[tslot(nb, t, 0, qi, l)] + ny_ * T.off[tslot(nb, t, 1, qj, l)] +
-                         nz_ * T.off[tslot(nb, t, 2, qk, l)];
-      term = term * dxn;
-    }
-    acc += term;
-  }
+  int ix[5], iy[5], iz[5];
+  double wx[5], wy[5], wz[5], ox[5], oy[5], oz[5];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if (lane == 0) {
-    double r = a.sign * acc;
-    const int i = c * nb + l;
-    if (a.sub) r -= a.sub[i] * a.subv[i];
-    if (a.addv) r += a.addv[i];
-    a.out[i] = r;
+  for (int q = 0; q < 5; ++q) {
+    ix[q] = T.idx[tslot(nb, t, 0, q, l)];
+    iy[q] = T.idx[tslot(nb, t, 1, q, l)];
+    iz[q] = T.idx[tslot(nb, t, 2, q, l)];
+    wx[q] = T.w1[tslot(nb, t, 0, q, l)];
+    wy[q] = T.w1[tslot(nb, t, 1, q, l)];
+    wz[q] = T.w1[tslot(nb, t, 2, q, l)];
   }
+  const bool e1n = a.mode == G_E1N;
+  if (e1n) {
+    const double nx_ = T.nrm[l], ny_ = T.nrm[nb + l], nz_ = T.nrm[2 * nb + l];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      ox[q] = nx_ * T.off[tslot(nb, t, 0, q, l)];
+      oy[q] = ny_ * T.off[tslot(nb, t, 1, q, l)];
+      oz[q] = nz_ * T.off[tslot(nb, t, 2, q, l)];
+    }
+  }
+  const Dims& d = a.d;
+  const GField& g = a.f[c];
+  double acc = 0.0;
+  for (int qk = 0; qk < 5; ++qk) {
+    for (int qj = 0; qj < 5; ++qj) {
+      const double wjk = T.scale * wy[qj] * wz[qk];
+#pragma unroll
+      for (int qi = 0; qi < 5; ++qi) {
+        double v;
+        if (a.mode == G_GRAD) {
+          const double* P = a.phi;
+          const double p0 = P[idxR(d, ix[qi], iy[qj], iz[qk])];
+          double gv;
+          if (t == 0) gv = (P[idxR(d, ix[qi] + 1, iy[qj], iz[qk])] - p0) * a.m.rdxg[ix[qi]];
+          else if (t == 1)
+            gv = (iy[qj] >= 2 && iy[qj] <= d.ny - 1)
+                     ? (P[idxR(d, ix[qi], iy[qj] + 1, iz[qk])] - p0) * a.m.rdyg[iy[qj]] : 0.0;
+          else gv = (P[idxR(d, ix[qi], iy[qj], iz[qk] + 1)] - p0) * a.m.rdzg[iz[qk]];
+          v = gv * a.phimul - a.reg[c][lin(g.n1, g.n2, ix[qi], iy[qj], iz[qk], 0)];
+        } else {
+          v = g.F[lin(g.n1, g.n2, ix[qi], iy[qj], iz[qk], g.rhsp)] * g.mul;
+        }
+        double term = wjk * wx[qi] * v;
+        if (e1n) term *= ox[qi] + oy[qj] + oz[qk];
+        acc += term;
+      }
+    }
+  }
+  double r = a.sign * acc;
+  const int i = c * nb + l;
+  if (a.sub) r -= a.sub[i] * a.subv[i];
+  if (a.addv) r += a.addv[i];
+  a.out[i] = r;
 }
 
 enum SpreadMode { S_RAW = 0, S_JUMP = 1, S_NORMAL = 2 };
@@ -475,33 +572,42 @@ struct SpreadArgs {
   double dtnu, dt;
 };
 
-__global__ void __launch_bounds__(256) k_ib_spread(SpreadArgs a) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+// one thread per (marker, component), as the gather; within one atomic
+// instruction the threads of a warp (consecutive markers) add to distinct
+// grid points
+__global__ void __launch_bounds__(128) k_ib_spread(SpreadArgs a) {
   const int nb = a.T.nb;
-  if (warp >= nb * a.ncomp) return;
-  const int cc = warp / nb;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nb * a.ncomp) return;
+  const int cc = gid / nb;
   const int c = a.comp0 + cc;
-  const int l = warp - cc * nb;
+  const int l = gid - cc * nb;
   const OpTables& T = a.T;
   double fl;
   if (a.mode == S_RAW) fl = a.f[l];
   else if (a.mode == S_NORMAL) fl = T.nrm[c * nb + l];
   else fl = a.dtnu * a.f[c * nb + l] - a.dt * a.f[3 * nb + l] * T.nrm[c * nb + l];
-  const double amp = T.factor * T.sb[l] * fl;
+  const double amp = T.scale * T.factor * T.sb[l] * fl;
+  int ix[5], iy[5], iz[5];
+  double wx[5], wy[5], wz[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    ix[q] = T.idx[tslot(nb, c, 0, q, l)];
+    iy[q] = T.idx[tslot(nb, c, 1, q, l)];
+    iz[q] = T.idx[tslot(nb, c, 2, q, l)];
+    wx[q] = T.w1[tslot(nb, c, 0, q, l)];
+    wy[q] = T.w1[tslot(nb, c, 1, q, l)];
+    wz[q] = T.w1[tslot(nb, c, 2, q, l)];
+  }
   double* F = a.F[cc];
   const int n1 = a.n1[cc], n2 = a.n2[cc];
-  for (int pnt = lane; pnt < 125; pnt += 32) {
-    const int qk = pnt / 25, qj = (pnt / 5) % 5, qi = pnt % 5;
-    const int ix = T.idx[tslot(nb, c, 0, qi, l)];
-    const int iy = T.idx[tslot(nb, c, 1, qj, l)];
-    const int iz = T.idx[tslot(nb, c, 2, qk, l)];
-    const double w = T.scale * T.w1[tslot(nb, c, 0, qi, l)] * T.w1[tslot(nb, c, 1, qj, l)] *
-                     T.w1[tslot(nb, c, 2, qk, l)];
-    const double val = w * T.factor * T.sb[l] * fl;
-    (void)amp;
-    atomicAdd(F + lin(n1, n2, ix, iy, iz, 0), val);
-  }
+  for (int qk = 0; qk < 5; ++qk)
+    for (int qj = 0; qj < 5; ++qj) {
+      const double wjk = wy[qj] * wz[qk];
+#pragma unroll
+      for (int qi = 0; qi < 5; ++qi)
+        atomicAdd(F + lin(n1, n2, ix[qi], iy[qj], iz[qk], 0), wx[qi] * wjk * amp);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -525,6 +631,54 @@ __global__ void k_body_sums(const double* __restrict__ v, const int* __restrict_
   }
   if (threadIdx.x == 0) out[b] = sm[0];
   (void)nbodies;
+}
+
+// Same sums for up to kMaxBodies bodies over the whole grid: per-thread
+// per-body accumulators, block partials, and the last block to finish
+// (ticket) adds the partials in block order.
+constexpr int kMaxBodies = 8;
+constexpr int kBodyBlocks = 64;
+__global__ void __launch_bounds__(256) k_body_sums_grid(const double* __restrict__ v, const int* __restrict__ body,
+                                                       int nb, int nbodies, double* __restrict__ part,
+                                                       unsigned* __restrict__ ticket, double* __restrict__ out) {
+  double acc[kMaxBodies];
+#pragma unroll
+  for (int q = 0; q < kMaxBodies; ++q) acc[q] = 0.0;
+  for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nb; l += gridDim.x * blockDim.x) {
+    const int b = body[l];
+    const double x = v[l];
+#pragma unroll
+    for (int q = 0; q < kMaxBodies; ++q)
+      if (q == b) acc[q] += x;
+  }
+  __shared__ double sm[8][kMaxBodies];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < kMaxBodies; ++q) {
+    double x = acc[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) sm[w][q] = x;
+  }
+  __syncthreads();
+  __shared__ bool last;
+  if (threadIdx.x < kMaxBodies) {
+    double x = 0.0;
+    for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) x += sm[ww][threadIdx.x];
+    part[blockIdx.x * kMaxBodies + threadIdx.x] = x;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < nbodies) {
+    double x = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) x += __ldcg(part + b * kMaxBodies + threadIdx.x);
+    out[threadIdx.x] = x;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
 }
 
 // v(p rows) = v - mean_body; then v -= E1nHc * pj (optional)
@@ -815,7 +969,7 @@ static OpTables tables(Handle* h) {
   return T;
 }
 
-static unsigned warp_blocks(int64_t warps) { return (unsigned)((warps * 32 + 255) / 256); }
+static unsigned thread_blocks(int64_t n) { return (unsigned)((n + 127) / 128); }
 
 static int upload_geometry(Handle* h) {
   IbState* s = h->ib;
@@ -854,7 +1008,7 @@ int ib_create(Handle* h) {
   h->ib = s;
   s->kind = h->p.body_type;
   s->moving = (s->kind == "standing_wave" || s->kind == "traveling_wave_x" ||
-               s->kind == "wall_standing_wave");
+               s->kind == "wall_standing_wave" || s->kind == "wall_plates");
   std::string err;
   int rc = geometry_host(h, s, h->t, err);
   if (rc) { h->last_error = err; return rc; }
@@ -898,6 +1052,7 @@ int ib_create(Handle* h) {
   if ((rc = dev_alloc(h, &s->lrn_blk, 16 * (int64_t)nb))) return rc;
   if ((rc = dev_alloc(h, &s->spai_blk, 16 * (int64_t)nb))) return rc;
   if ((rc = dev_alloc(h, &s->red, 2 * kIbRedBlocks + 16))) return rc;
+  if ((rc = dev_alloc(h, &s->ticket, 1))) return rc;
   if ((rc = dev_alloc(h, &s->sc, 16))) return rc;
   // H = 1 (interior) until compute_heaviside runs (app/main.f90:80-85)
   std::vector<double> ones(std::max(sizeU(d), std::max(sizeV(d), sizeW(d))), 1.0);
@@ -961,7 +1116,7 @@ static int gather3(Handle* h, int mode, const double* U, const double* V, const 
   a.f[0] = gf_u(h->d, U); a.f[1] = gf_v(h->d, V); a.f[2] = gf_w(h->d, W);
   a.type[0] = 0; a.type[1] = 1; a.type[2] = 2;
   a.ncomp = 3; a.mode = mode; a.out = out; a.sign = sign; a.sub = sub; a.subv = subv; a.addv = addv;
-  k_ib_gather<<<warp_blocks(3 * (int64_t)h->ib->nb), 256, 0, h->stream>>>(a);
+  k_ib_gather<<<thread_blocks(3 * (int64_t)h->ib->nb), 128, 0, h->stream>>>(a);
   C3D_LAUNCH_CHECK(h);
   return 0;
 }
@@ -972,7 +1127,7 @@ static int gather_c(Handle* h, const double* P, double mul, double* out, double 
   a.f[0] = GField{P, h->d.nxg - 2, h->d.nyg - 2, 1, mul};
   a.type[0] = 3;
   a.ncomp = 1; a.mode = G_E1N; a.out = out; a.sign = sign;
-  k_ib_gather<<<warp_blocks(h->ib->nb), 256, 0, h->stream>>>(a);
+  k_ib_gather<<<thread_blocks(h->ib->nb), 128, 0, h->stream>>>(a);
   C3D_LAUNCH_CHECK(h);
   return 0;
 }
@@ -991,7 +1146,7 @@ static int spread(Handle* h, int mode, int comp0, int ncomp, const double* f, do
     a.n1[c] = n1s[comp0 + c];
     a.n2[c] = n2s[comp0 + c];
   }
-  k_ib_spread<<<warp_blocks((int64_t)ncomp * s->nb), 256, 0, h->stream>>>(a);
+  k_ib_spread<<<thread_blocks((int64_t)ncomp * s->nb), 128, 0, h->stream>>>(a);
   C3D_LAUNCH_CHECK(h);
   return 0;
 }
@@ -1010,7 +1165,12 @@ static int reg_all(Handle* h, int mode, const double* f, double dt) {
 
 static int remove_mean(Handle* h, double* v, const double* pj_for_e1nhc) {
   IbState* s = h->ib;
-  k_body_sums<<<s->nbodies, 256, 0, h->stream>>>(v, s->body_d, s->nb, s->nbodies, s->red);
+  if (s->nbodies <= kMaxBodies) {
+    k_body_sums_grid<<<kBodyBlocks, 256, 0, h->stream>>>(v, s->body_d, s->nb, s->nbodies, s->red + 16,
+                                                         s->ticket, s->red);
+  } else {
+    k_body_sums<<<s->nbodies, 256, 0, h->stream>>>(v, s->body_d, s->nb, s->nbodies, s->red);
+  }
   C3D_LAUNCH_CHECK(h);
   k_remove_mean<<<(s->nb + 255) / 256, 256, 0, h->stream>>>(v, s->body_d, s->red, s->binv_d, s->nb,
                                                             pj_for_e1nhc ? s->E1nHc : nullptr,
@@ -1042,8 +1202,7 @@ int ib_schur(Handle* h, const double* f, double* Sf, double dt) {
   const int nb = s->nb;
   int rc;
   if ((rc = reg_all(h, S_JUMP, f, dt))) return rc;                      // :106-114
-  if ((rc = launch_divergence(h, s->Ureg, s->Vreg, s->Wreg, h->rhs_p))) return rc;   // :117
-  if ((rc = launch_poisson_solve(h, h->rhs_p, 0, dt))) return rc;        // :120
+  if ((rc = launch_poisson_of_div(h, s->Ureg, s->Vreg, s->Wreg, h->rhs_p, 0, dt))) return rc;   // :117-120
   // Sf(p) = -E1n_c(phi/dt); mean removal; -E1nHc_ext*p_jump        :123-126
   if ((rc = gather_c(h, h->rhs_p, 1.0 / dt, Sf + 3 * nb, -1.0))) return rc;
   if ((rc = remove_mean(h, Sf + 3 * nb, f + 3 * nb))) return rc;
@@ -1055,7 +1214,7 @@ int ib_schur(Handle* h, const double* f, double* Sf, double dt) {
   a.mode = G_GRAD; a.phi = h->rhs_p; a.phimul = 1.0;
   a.reg[0] = s->Ureg; a.reg[1] = s->Vreg; a.reg[2] = s->Wreg;
   a.out = Sf; a.sign = 1.0; a.sub = s->E1nH; a.subv = f;
-  k_ib_gather<<<warp_blocks(3 * (int64_t)nb), 256, 0, h->stream>>>(a);
+  k_ib_gather<<<thread_blocks(3 * (int64_t)nb), 128, 0, h->stream>>>(a);
   C3D_LAUNCH_CHECK(h);
   return 0;
 }
@@ -1319,8 +1478,7 @@ int ib_projection(Handle* h, double dt, int rk_step) {
   const int warn = rc;
   // R f, divergence, Poisson (P side effect at rk_step 1), final update   :63-94
   if ((rc = reg_all(h, S_JUMP, s->fb, dt))) return rc;
-  if ((rc = launch_divergence(h, s->Ureg, s->Vreg, s->Wreg, h->rhs_p))) return rc;
-  if ((rc = launch_poisson_solve(h, h->rhs_p, rk_step, dt))) return rc;
+  if ((rc = launch_poisson_of_div(h, s->Ureg, s->Vreg, s->Wreg, h->rhs_p, rk_step, dt))) return rc;
   const Dims& d = h->d;
   dim3 b(32, 4, 2), g((d.Nx + 31) / 32, (d.Ny + 3) / 4, (d.Nz + 1) / 2);
   k_ib_final<<<g, b, 0, h->stream>>>(d, h->m, h->Us, h->Vs, h->Ws, s->Ureg, s->Vreg, s->Wreg,

@@ -900,6 +900,18 @@ int launch_poisson_solve(Handle* h, double* rhs, int rk_step, double dt) {
   return 0;
 }
 
+// solve for the divergence of (U, V, W) into out (rhs_p layout), the
+// divergence computed inside the forward x FFT (divergence followed by
+// solve_poisson_equation, src/differential_operators.f90:54-74 and
+// src/poisson.f90:33-101); P side effect at rk_step 1
+int launch_poisson_of_div(Handle* h, const double* U, const double* V, const double* W, double* out,
+                          int rk_step, double dt) {
+  int rc = run_spectral_t<double>(h, true, U, V, W, nullptr, out, rk_step == 1 ? h->phi1 : nullptr, 0, 7);
+  if (rc) return rc;
+  if (rk_step == 1) { h->P_pending = true; h->P_pending_dt = dt; }
+  return 0;
+}
+
 // ---------------------------------------------------------------------------
 // projection: U = Ui - G phi at interior points (src/projection.f90:40-44),
 // optional P_interim = phi/dt; ghosts are filled by the caller

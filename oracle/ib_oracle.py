@@ -32,7 +32,8 @@ class Body:
     def __init__(self, g, p, t=0.0, markers=None):
         self.g, self.p = g, p
         self.kind = p["body_type"]
-        self.moving = self.kind in ("standing_wave", "traveling_wave_x", "wall_standing_wave")
+        self.moving = self.kind in ("standing_wave", "traveling_wave_x", "wall_standing_wave",
+                                    "wall_plates")
         self.markers = markers
         self.update(t)
 
@@ -61,6 +62,10 @@ class Body:
             self._traveling_wave(t)
         elif kind == "double_cylinders_z":                          # :117-174
             self._double_cylinders()
+        elif kind == "two_cylinders_z":
+            self._two_cylinders()
+        elif kind == "wall_plates":
+            self._wall_plates(t)
         elif kind == "markers":
             m = self.markers
             self.xb, self.yb, self.zb = m["xb"].copy(), m["yb"].copy(), m["zb"].copy()
@@ -246,6 +251,98 @@ class Body:
         self.xb, self.yb, self.zb, self.ub, self.normals, self.sb = xb, yb, zb, ub, nrm, sb
         self.y_ref = np.ones(nb, dtype=np.int64)
         self.blocks = [np.array(inner), np.array(outer)]
+
+    def _two_cylinders(self):
+        """Two separate spanwise cylinders (no reference analog; conventions
+        of double_cylinders_z, src/immersed_boundary_geometry.f90:117-174):
+        radius body_param_1, surface speeds +-body_param_2, centres
+        (body_param_3, Ly/2) and (2 body_param_3, Ly/2 + body_param_4); normals
+        into each cylinder; one body per cylinder."""
+        g, p = self.g, self.p
+        nxb, nzb = p["nxb"], p["nzb"]
+        r, us = p["body_param_1"], p["body_param_2"]
+        dzb = g.Lzp / nzb
+        dsb = 2.0 * PI * r / nxb
+        nb = 2 * nxb * nzb
+        xc = (p["body_param_3"], 2.0 * p["body_param_3"])
+        yc = (0.5 * p["ly_channel"], 0.5 * p["ly_channel"] + p["body_param_4"])
+        sgn = (1.0, -1.0)
+        xb, yb, zb = np.zeros(nb), np.zeros(nb), np.zeros(nb)
+        ub, nrm, sb = np.zeros(3 * nb), np.zeros(3 * nb), np.zeros(nb)
+        blocks = ([], [])
+        for j in range(1, nzb + 1):
+            for c in range(2):
+                for i in range(1, nxb + 1):
+                    k = i + c * nxb + 2 * nxb * (j - 1) - 1
+                    th = (i - 1) * 2.0 * PI / nxb
+                    xb[k] = xc[c] + r * math.cos(th)
+                    yb[k] = yc[c] + r * math.sin(th)
+                    zb[k] = (j - 0.5) * dzb
+                    ub[k] = -sgn[c] * us * math.sin(th)
+                    ub[nb + k] = sgn[c] * us * math.cos(th)
+                    sb[k] = dsb * dzb
+                    nrm[k] = -math.cos(th)
+                    nrm[nb + k] = -math.sin(th)
+                    blocks[c].append(k)
+        self.xb, self.yb, self.zb, self.ub, self.normals, self.sb = xb, yb, zb, ub, nrm, sb
+        self.y_ref = np.ones(nb, dtype=np.int64)
+        self.blocks = [np.array(blocks[0]), np.array(blocks[1])]
+
+    def _wall_plates(self, t):
+        """Wall-mounted bending plates (no reference analog): nxb x nzb plates
+        of height h = body_param_1 and width half the spanwise pitch, 32 x 16
+        markers each, rows from 3 dymin above the wall to the tip;
+        x = x_p + a (y/h)^2 sin(omega t + phi), a = body_param_2,
+        omega = body_param_3, phi from splitmix64 seeded with body_param_4."""
+        g, p = self.g, self.p
+        nxb, nzb = p["nxb"], p["nzb"]
+        my, mz = 32, 16
+        hh, amp, om = p["body_param_1"], p["body_param_2"], p["body_param_3"]
+        pitchx, pitchz = g.Lxp / nxb, g.Lzp / nzb
+        wz = 0.5 * pitchz
+        lat = nxb * my
+        nb = nxb * nzb * my * mz
+        phase = splitmix64_phases(int(round(p["body_param_4"])), nxb * nzb)
+        xb, yb, zb = np.zeros(nb), np.zeros(nb), np.zeros(nb)
+        ub, nrm, sb = np.zeros(3 * nb), np.zeros(3 * nb), np.zeros(nb)
+        for pj in range(1, nzb + 1):
+            for m in range(1, mz + 1):
+                for pi_ in range(1, nxb + 1):
+                    for kk in range(1, my + 1):
+                        ix, iz = (pi_ - 1) * my + kk - 1, (pj - 1) * mz + m - 1
+                        k = ix + lat * iz
+                        ph = phase[(pi_ - 1) + nxb * (pj - 1)]
+                        y0 = 3.0 * g.dymin
+                        y = y0 + (kk - 1) * (hh - y0) / (my - 1)
+                        eta = y / hh
+                        sn, cs = math.sin(om * t + ph), math.cos(om * t + ph)
+                        xb[k] = (pi_ - 0.5) * pitchx + amp * eta * eta * sn
+                        yb[k] = y
+                        zb[k] = (pj - 0.5) * pitchz + (m - 0.5 - 0.5 * mz) * (wz / mz)
+                        ub[k] = amp * eta * eta * om * cs
+                        slope = 2.0 * amp * y / (hh * hh) * sn
+                        nn = math.sqrt(1.0 + slope * slope)
+                        nrm[k] = 1.0 / nn
+                        nrm[nb + k] = -slope / nn
+                        sb[k] = ((hh - 3.0 * g.dymin) / (my - 1)) * (wz / mz)
+        self.xb, self.yb, self.zb, self.ub, self.normals, self.sb = xb, yb, zb, ub, nrm, sb
+        self.y_ref = np.ones(nb, dtype=np.int64)
+        self.blocks = [np.arange(nb)]
+
+
+def splitmix64_phases(seed, n):
+    """n phases 2 pi u, u in [0, 1) from the splitmix64 stream of ``seed``."""
+    mask = (1 << 64) - 1
+    st = seed & mask
+    out = np.zeros(n)
+    for q in range(n):
+        st = (st + 0x9E3779B97F4A7C15) & mask
+        z = st
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
+        z ^= z >> 31
+        out[q] = 2.0 * PI * (z >> 11) * (1.0 / 9007199254740992.0)
+    return out
 
 
 def remove_mean_per_body(body, f):
