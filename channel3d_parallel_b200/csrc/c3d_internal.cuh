@@ -244,6 +244,8 @@ int launch_divergence(Handle* h, const double* U, const double* V, const double*
 int launch_poisson_solve(Handle* h, double* rhs, int rk_step, double dt);
 int launch_poisson_of_div(Handle* h, const double* U, const double* V, const double* W, double* out,
                           int rk_step, double dt);
+int launch_poisson_of_div_band(Handle* h, const double* U, const double* V, const double* W, double* out,
+                               int jlo, int jhi);
 int launch_projection_step(Handle* h, int rk_step, double dt);
 int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, const double* Wi,
                              const double* phi, double dt, double* Uo, double* Vo, double* Wo);

@@ -40,6 +40,7 @@ struct IbState {
   double* red = nullptr;             // partial sums
   double* sc = nullptr;              // BiCGSTAB scalars
   unsigned* ticket = nullptr;        // last-block counter of the body sums
+  int iy_lo = 1, iy_hi = 1 << 30;    // y rows touched by any stencil
   // marker lattice: index = ix + lat_nx * iz (every body type lays its markers
   // out row by row); lat_nx = nb when there is no second direction
   int lat_nx = 0;

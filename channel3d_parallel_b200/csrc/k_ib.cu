@@ -1080,6 +1080,20 @@ int ib_setup_geometry(Handle* h, double t) {
   return upload_geometry(h);
 }
 
+// smallest and largest y index of any stencil (all four locations)
+__global__ void k_iy_range(const int* __restrict__ idx, int nb, int* __restrict__ range) {
+  int lo = 1 << 30, hi = -(1 << 30);
+  for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nb; l += gridDim.x * blockDim.x)
+    for (int t = 0; t < 4; ++t)
+      for (int q = 0; q < 5; ++q) {
+        const int iy = idx[tslot(nb, t, 1, q, l)];
+        lo = min(lo, iy);
+        hi = max(hi, iy);
+      }
+  atomicMin(range, lo);
+  atomicMax(range + 1, hi);
+}
+
 int ib_setup_operators(Handle* h) {
   IbState* s = h->ib;
   if (!s) return C3D_ERR_UNSUPPORTED;
@@ -1099,6 +1113,16 @@ int ib_setup_operators(Handle* h) {
   C3D_CUDA_TRY(h, cudaMemcpyAsync(&flag, s->flag_d, 4, cudaMemcpyDeviceToHost, h->stream));
   C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   if (flag) { h->last_error = "Error: zi_supp out of range (marker stencil outside the grid)"; return C3D_ERR_PARAM; }
+  // y rows the stencils touch: the Schur complement's spread field and the
+  // rows of its potential read by the gathers lie in [iy_lo - 1, iy_hi + 1]
+  int range[2] = {1 << 30, -(1 << 30)};
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->flag_d + 1, range, 8, cudaMemcpyHostToDevice, h->stream));
+  k_iy_range<<<std::min(148, (s->nb + 255) / 256), 256, 0, h->stream>>>(s->idx_d, s->nb, s->flag_d + 1);
+  C3D_LAUNCH_CHECK(h);
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(range, s->flag_d + 1, 8, cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  s->iy_lo = range[0];
+  s->iy_hi = range[1];
   s->have_lrn = false;
   return 0;
 }
@@ -1152,6 +1176,26 @@ static int spread(Handle* h, int mode, int comp0, int ncomp, const double* f, do
 }
 
 // zero U_reg, V_reg, W_reg and spread; then boundary conditions
+// R f for the Schur complement: only the rows [jlo, jhi] of the spread
+// fields are cleared (the banded solve reads nothing else; rows outside keep
+// zeros or values of earlier geometries that no banded reader touches)
+static int reg_all_band(Handle* h, int mode, const double* f, double dt, int jlo, int jhi) {
+  IbState* s = h->ib;
+  const Dims& d = h->d;
+  double* F[3] = {s->Ureg, s->Vreg, s->Wreg};
+  const int n1[3] = {d.nx, d.nxg, d.nxg}, n2[3] = {d.nyg, d.ny, d.nyg}, n3[3] = {d.nzg, d.nzg, d.nz};
+  for (int c = 0; c < 3; ++c) {
+    const int a = std::max(jlo, 1), b = std::min(jhi, n2[c]);
+    if (b < a) continue;
+    const size_t plane = 8 * (size_t)n1[c] * n2[c];
+    C3D_CUDA_TRY(h, cudaMemset2DAsync(F[c] + (size_t)(a - 1) * n1[c], plane, 0, 8 * (size_t)n1[c] * (b - a + 1),
+                                      n3[c], h->stream));
+  }
+  int rc = spread(h, mode, 0, 3, f, dt, s->Ureg, s->Vreg, s->Wreg);
+  if (rc) return rc;
+  return launch_fill_ghosts3(h, s->Ureg, s->Vreg, s->Wreg);
+}
+
 static int reg_all(Handle* h, int mode, const double* f, double dt) {
   IbState* s = h->ib;
   const Dims& d = h->d;
@@ -1201,8 +1245,10 @@ int ib_schur(Handle* h, const double* f, double* Sf, double dt) {
   IbState* s = h->ib;
   const int nb = s->nb;
   int rc;
-  if ((rc = reg_all(h, S_JUMP, f, dt))) return rc;                      // :106-114
-  if ((rc = launch_poisson_of_div(h, s->Ureg, s->Vreg, s->Wreg, h->rhs_p, 0, dt))) return rc;   // :117-120
+  // :106-120 on the band of y rows the markers' stencils reach
+  const int jlo = s->iy_lo - 1, jhi = s->iy_hi + 1;
+  if ((rc = reg_all_band(h, S_JUMP, f, dt, jlo - 1, jhi + 1))) return rc;
+  if ((rc = launch_poisson_of_div_band(h, s->Ureg, s->Vreg, s->Wreg, h->rhs_p, jlo, jhi))) return rc;
   // Sf(p) = -E1n_c(phi/dt); mean removal; -E1nHc_ext*p_jump        :123-126
   if ((rc = gather_c(h, h->rhs_p, 1.0 / dt, Sf + 3 * nb, -1.0))) return rc;
   if ((rc = remove_mean(h, Sf + 3 * nb, f + 3 * nb))) return rc;

@@ -211,6 +211,7 @@ struct XfwdArgs {
   FftPasses P;
   int pz;                                     // spectrum row pitch
   int rs;                                     // shared-memory row stride
+  int64_t rbase, nlines;                      // lines rbase .. rbase+nlines-1 (a band of j rows)
 };
 
 // real x-line r = (k-2) + Nz*(j-2); its spectrum goes to slab offset
@@ -255,8 +256,8 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
     sm.tw[t] = a.tw[t];
     sm.pos[t] = dif_k_to_position(t, a.P);
   }
-  const int64_t nreal = (int64_t)d.Ny * d.Nz;
-  const int64_t r0 = (int64_t)blockIdx.x * kLinesX * 2;
+  const int64_t nreal = a.rbase + a.nlines;
+  const int64_t r0 = a.rbase + (int64_t)blockIdx.x * kLinesX * 2;
   if (tid < 2 * kLinesX) {
     const int64_t r = r0 + tid;
     int j = -1, k = -1, off = 0;
@@ -343,6 +344,9 @@ struct YzArgs {
   int rs;        // shared-memory row stride (complex values)
   int pz;        // HBM row pitch (complex values)
   int zero00;    // 1: leave the kx = kz = 0 column to the FP64 mean-mode solve
+  int rlo, rhi;  // rows (j-2) with a nonzero right-hand side and rows of the
+                 // solution needed: the band [rlo, rhi]; other rows start at
+                 // zero and are not transformed back or stored
 };
 
 // CTA c of the cluster owns rows j0 = c*jc .. j0+jn-1 of the slab.  Shared
@@ -385,10 +389,18 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
     fence_mbar_init();
   }
   __syncthreads();
+  // this CTA's rows of the band: [blo, bhi)
+  const int blo = min(max(a.rlo - j0, 0), jn), bhi = max(min(a.rhi + 1 - j0, jn), blo);
   if (tid < 32) {
-    if (tid == 0) mbar_arrive_expect_tx(&bar, rowbytes * (unsigned)jn);
+    if (tid == 0) mbar_arrive_expect_tx(&bar, rowbytes * (unsigned)(bhi - blo));
     __syncwarp();
-    for (int r = tid; r < jn; r += 32) bulk_load(data + (size_t)r * RS, g + (int64_t)r * a.pz, rowbytes, &bar);
+    for (int r = blo + tid; r < bhi; r += 32)
+      bulk_load(data + (size_t)r * RS, g + (int64_t)r * a.pz, rowbytes, &bar);
+  }
+  for (int t = tid; t < (jn - (bhi - blo)) * Nz; t += nt) {   // rows outside the band start at zero
+    const int rr = t / Nz, col = t - rr * Nz;
+    const int r = rr < blo ? rr : rr + (bhi - blo);
+    data[(size_t)r * RS + col] = C{(T)0, (T)0};
   }
   for (int t = tid; t < Nz; t += nt) tw[t] = a.tw[t];
   for (int t = tid; t < Ny; t += nt) { sdl[t] = a.dl[t]; sdu[t] = a.du[t]; }
@@ -397,7 +409,7 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
   if (!loaded) atomicOr(a.err, 1ull);
   __syncthreads();
 
-  fft_rows_dif<T, kYzB>(data, jn, RS, tw, a.P, kRun);
+  fft_rows_dif<T, kYzB>(data + (size_t)blo * RS, bhi - blo, RS, tw, a.P, kRun);
 
   // pivots of this thread's column for rows j0 .. j0+jn-1 (one column per
   // thread when Nz <= blockDim; otherwise reloaded per column below)
@@ -559,7 +571,7 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
   }
   __syncthreads();
 
-  fft_rows_dit_inv<T, kYzB>(data, jn, RS, tw, a.P, kRun);
+  fft_rows_dit_inv<T, kYzB>(data + (size_t)blo * RS, bhi - blo, RS, tw, a.P, kRun);
   // no CTA leaves while another may still read its ylast / xfirst
   cl.sync();
 
@@ -567,7 +579,7 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
   __syncthreads();
   if (tid < 32) {
     if (loaded) {
-      for (int r = tid; r < jn; r += 32) bulk_store(g + (int64_t)r * a.pz, data + (size_t)r * RS, rowbytes);
+      for (int r = blo + tid; r < bhi; r += 32) bulk_store(g + (int64_t)r * a.pz, data + (size_t)r * RS, rowbytes);
       bulk_commit();
       bulk_wait_read_all();
     } else {
@@ -621,6 +633,7 @@ struct XinvArgs {
   FftPasses P;
   int pz;                        // spectrum row pitch
   int rs;                        // shared-memory row stride
+  int64_t rbase, nlines;         // lines rbase .. rbase+nlines-1 (a band of j rows)
   double scale_div;              // nxp*nzp
 };
 
@@ -637,8 +650,8 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
     sm.tw[t] = a.tw[t];
     sm.pos[t] = dif_k_to_position(t, a.P);
   }
-  const int64_t nreal = (int64_t)d.Ny * d.Nz;
-  const int64_t r0 = (int64_t)blockIdx.x * kLinesX * 2;
+  const int64_t nreal = a.rbase + a.nlines;
+  const int64_t r0 = a.rbase + (int64_t)blockIdx.x * kLinesX * 2;
   if (tid < 2 * kLinesX) {
     const int64_t r = r0 + tid;
     int j = -1, k = -1, off = 0;
@@ -763,13 +776,14 @@ static bool choose_cluster(const Dims& d, int pz, int& cs, int& jc, int& rs, int
 template <typename T>
 static int launch_yz(Handle* h, typename cplx<T>::t* spec, const typename cplx<T>::t* tw, const T* rdp,
                      const T* dl, const T* du, const T* xh, const T* gh, const T* hend, int cs, int jc,
-                     int rs, int pz, int nt, int smem, int zero00) {
+                     int rs, int pz, int nt, int smem, int zero00, int rlo, int rhi) {
   const Dims& d = h->d;
   YzArgs<T> a{};
   a.d = d; a.spec = spec; a.tw = tw; a.rdp = rdp; a.dl = dl; a.du = du;
   a.xh = xh; a.gh = gh; a.hend = hend;
   a.err = &h->sc->err;
   a.P = get_passes(d.Nz); a.cs = cs; a.jc = jc; a.rs = rs; a.pz = pz; a.zero00 = zero00;
+  a.rlo = rlo; a.rhi = rhi;
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)(cs * d.nkx), 1, 1);
   cfg.blockDim = dim3((unsigned)nt, 1, 1);
@@ -803,7 +817,8 @@ static int set_limits(Handle* h, int smem_yz, int cs) {
 // parts: bit0 x FFT, bit1 yz, bit2 inverse x FFT
 template <typename T>
 static int run_spectral_t(Handle* h, bool from_div, const double* U, const double* V, const double* W,
-                          const double* rhs_in, double* out, double* phi1, int accumulate, int parts) {
+                          const double* rhs_in, double* out, double* phi1, int accumulate, int parts,
+                          int blo = 0, int bhi = -1) {
   const Dims& d = h->d;
   SpectralState& S = h->sp;
   cudaStream_t s = h->stream;
@@ -825,7 +840,9 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     cs = S.cs64; jc = S.jc64; rs = S.rs64; pz = S.pz64; nt = S.nt64; smem = S.smem64;
   }
   const FftPasses Px = get_passes(d.Nx);
-  const int64_t npairs = ((int64_t)d.Ny * d.Nz + 1) / 2;
+  if (bhi < 0) bhi = d.Ny - 1;                 // band of j rows (0-based j-2); full by default
+  const int64_t rbase = (int64_t)blo * d.Nz, nlines = (int64_t)(bhi - blo + 1) * d.Nz;
+  const int64_t npairs = (nlines + 1) / 2;
   const unsigned nbx = (unsigned)((npairs + kLinesX - 1) / kLinesX);
   const int smx = xfft_smem<T>(d);
   const int ntx = xfft_threads(d);
@@ -833,7 +850,7 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
   if (parts & 1) {
     XfwdArgs<T> a{};
     a.d = d; a.m = h->m; a.U = U; a.V = V; a.W = W; a.rhs = rhs_in;
-    a.spec = spec; a.tw = twx; a.P = Px; a.pz = pz; a.rs = rsx;
+    a.spec = spec; a.tw = twx; a.P = Px; a.pz = pz; a.rs = rsx; a.rbase = rbase; a.nlines = nlines;
     a.linesum = f32 ? S.linesum : nullptr;
     if (from_div) k_xfft_fwd<true, T><<<nbx, ntx, smx, s>>>(a);
     else k_xfft_fwd<false, T><<<nbx, ntx, smx, s>>>(a);
@@ -844,14 +861,16 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     }
   }
   if (parts & 2) {
-    int rc = launch_yz<T>(h, spec, twz, rdp, dl, du, xh, gh, hend, cs, jc, rs, pz, nt, smem, f32 ? 1 : 0);
+    int rc = launch_yz<T>(h, spec, twz, rdp, dl, du, xh, gh, hend, cs, jc, rs, pz, nt, smem, f32 ? 1 : 0,
+                          blo, bhi);
     if (rc) return rc;
   }
   if (parts & 4) {
     XinvArgs<T> a{};
     a.d = d; a.spec = spec; a.tw = twx; a.rhs = out; a.phi1 = phi1;
     a.phi00 = f32 ? S.phi00 : nullptr; a.accumulate = accumulate;
-    a.P = Px; a.pz = pz; a.rs = rsx; a.scale_div = (double)d.Nx * (double)d.Nz;
+    a.P = Px; a.pz = pz; a.rs = rsx; a.rbase = rbase; a.nlines = nlines;
+    a.scale_div = (double)d.Nx * (double)d.Nz;
     k_xfft_inv<T><<<nbx, ntx, smx, s>>>(a);
     C3D_LAUNCH_CHECK(h);
   }
@@ -910,6 +929,17 @@ int launch_poisson_of_div(Handle* h, const double* U, const double* V, const dou
   if (rc) return rc;
   if (rk_step == 1) { h->P_pending = true; h->P_pending_dt = dt; }
   return 0;
+}
+
+// the same restricted to a band of j rows (Fortran j = jlo..jhi): the
+// divergence of (U, V, W) is zero outside the band and the caller reads the
+// solution only inside it (the Schur complement's spread field and its
+// gathers); rows of `out` outside the band are left as they were
+int launch_poisson_of_div_band(Handle* h, const double* U, const double* V, const double* W, double* out,
+                               int jlo, int jhi) {
+  const int blo = std::max(jlo - 2, 0), bhi = std::min(jhi - 2, h->d.Ny - 1);
+  if (bhi < blo) return 0;
+  return run_spectral_t<double>(h, true, U, V, W, nullptr, out, nullptr, 0, 7, blo, bhi);
 }
 
 // ---------------------------------------------------------------------------
