@@ -270,6 +270,7 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
   // nt is a multiple of N: thread -> x index ii, real lines rl0, rl0 + nt/N, ...
   const int ii = tid % N, rls = nt / N;
   const int i = 2 + ii;
+#pragma unroll 4
   for (int rl = tid / N; rl < 2 * kLinesX; rl += rls) {
     const int j = s_j[rl], k = s_k[rl];
     double val = 0.0;
@@ -688,6 +689,7 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
   const double sd = a.scale_div;
   const int ii = tid % N, rls = nt / N;
   const int i = 2 + ii;
+#pragma unroll 4
   for (int rl = tid / N; rl < 2 * kLinesX; rl += rls) {
     const int j = s_j[rl], k = s_k[rl];
     if (j < 0) continue;

@@ -213,18 +213,38 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
   const bool hasv = active && (j <= d.Ny);
   const double dPdx = a.sc->dPdx, dPdy = a.sc->dPdy, dPdz = a.sc->dPdz;
 
+  // halo-tile positions of this thread (at most two: PN <= 2 * TX * TY): the
+  // offset of plane 1 and the x/y validity are fixed, plane k adds k-1 planes
+  constexpr int kPos = (PN + TX * TY - 1) / (TX * TY);
+  int64_t offU[kPos], offV[kPos], offW[kPos];
+  bool okU[kPos], okV[kPos], okW[kPos];
+#pragma unroll
+  for (int q = 0; q < kPos; ++q) {
+    const int t = tid + q * TX * TY;
+    const int li = t % PX, lj = t / PX;
+    const int gi = i0 - 1 + li, gj = j0 - 1 + lj;
+    const bool in = t < PN;
+    okU[q] = in && gi <= d.nx && gj <= d.nyg;
+    okV[q] = in && gi <= d.nxg && gj <= d.ny;
+    okW[q] = in && gi <= d.nxg && gj <= d.nyg;
+    offU[q] = okU[q] ? idxU(d, gi, gj, 1) : 0;
+    offV[q] = okV[q] ? idxV(d, gi, gj, 1) : 0;
+    offW[q] = okW[q] ? idxW(d, gi, gj, 1) : 0;
+  }
+  const int64_t plU = (int64_t)d.nx * d.nyg, plV = (int64_t)d.nxg * d.ny, plW = (int64_t)d.nxg * d.nyg;
   // asynchronous copy of plane k (tile + halo) of U, V, W into a slot
   auto issue_plane = [&](int k) {
     const int slot = k & (NSLOT - 1);
-    for (int t = tid; t < PN; t += TX * TY) {
-      const int li = t % PX, lj = t / PX;
-      const int gi = i0 - 1 + li, gj = j0 - 1 + lj;
-      const bool vu = gi <= d.nx && gj <= d.nyg && k <= d.nzg;
-      const bool vv = gi <= d.nxg && gj <= d.ny && k <= d.nzg;
-      const bool vw = gi <= d.nxg && gj <= d.nyg && k <= d.nz;
-      cp_async8(&sU[slot][t], vu ? a.U + idxU(d, gi, gj, k) : a.U, vu);
-      cp_async8(&sV[slot][t], vv ? a.V + idxV(d, gi, gj, k) : a.V, vv);
-      cp_async8(&sW[slot][t], vw ? a.W + idxW(d, gi, gj, k) : a.W, vw);
+    const int64_t kk = k - 1;
+#pragma unroll
+    for (int q = 0; q < kPos; ++q) {
+      const int t = tid + q * TX * TY;
+      if (t < PN) {
+        const bool vu = okU[q] && k <= d.nzg, vv = okV[q] && k <= d.nzg, vw = okW[q] && k <= d.nz;
+        cp_async8(&sU[slot][t], vu ? a.U + offU[q] + kk * plU : a.U, vu);
+        cp_async8(&sV[slot][t], vv ? a.V + offV[q] + kk * plV : a.V, vv);
+        cp_async8(&sW[slot][t], vw ? a.W + offW[q] + kk * plW : a.W, vw);
+      }
     }
     cp_async_commit();
   };
@@ -235,15 +255,25 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
     else cp_async_commit();
   }
   const int c = (ty + 1) * PX + (tx + 1);     // own cell in the padded tile
+  // x- and y-indexed metric factors of this column, constant over the march
+  const int ic = active ? i : 2, jc = active ? j : 2;
+  const double rdxg_i = m.rdxg[ic], rdx_i = m.rdx[ic];
+  const double cxpF_i = m.cxpF[ic], cxmF_i = m.cxmF[ic], cxpC_i = m.cxpC[ic], cxmC_i = m.cxmC[ic];
+  const double rdy_j = m.rdy[jc], rdyg_j = m.rdyg[jc];
+  const double cypC_j = m.cypC[jc], cymC_j = m.cymC[jc], cypF_j = m.cypF[jc], cymF_j = m.cymF[jc];
+  const int64_t iu0 = idxU(d, ic, jc, 1), iv0 = idxV(d, ic, jc, 1), iw0 = idxW(d, ic, jc, 1);
   for (int k = k0; k <= k1; ++k) {
     if (k + 1 + AHEAD <= k1 + 1) issue_plane(k + 1 + AHEAD);
     else cp_async_commit();                   // keep the group count uniform
     cp_async_wait<AHEAD>();                   // planes up to k+1 have landed
     __syncthreads();
     const int sm = (k - 1) & (NSLOT - 1), s0 = k & (NSLOT - 1), sp = (k + 1) & (NSLOT - 1);
+    const double rdz_k = m.rdz[k], rdzg_k = m.rdzg[k];
+    const double czpC_k = m.czpC[k], czmC_k = m.czmC[k], czpF_k = m.czpF[k], czmF_k = m.czmF[k];
     if (active) {
-      const int64_t iu = idxU(d, i, j, k), iw = idxW(d, i, j, k);
-      const int64_t iv = idxV(d, i, j, k);
+      const int64_t kk = k - 1;
+      const int64_t iu = iu0 + kk * plU, iw = iw0 + kk * plW;
+      const int64_t iv = iv0 + kk * plV;
       double gu = 0.0, gv = 0.0, gw = 0.0;
       if (MODE == 2) {                        // issue the accumulator loads early
         gu = __ldg(a.Gu + iu);
@@ -263,12 +293,12 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
         const double v1m = AV(s0, 1, -1);
         const double w1m = AW(sm, 1, 0);
         const double ap = u0 + uxp, am = uxm + u0;
-        double r = (am * am - ap * ap) * (0.25 * m.rdxg[i]);
-        r += ((uym + u0) * (vym + v1m) - (u0 + uyp) * (v0 + vxp)) * (0.25 * m.rdy[j]);
-        r += ((uzm + u0) * (wzm + w1m) - (u0 + uzp) * (w0 + wxp)) * (0.25 * m.rdz[k]);
-        r += m.cxpF[i] * (uxp - u0) - m.cxmF[i] * (u0 - uxm)
-           + m.cypC[j] * (uyp - u0) - m.cymC[j] * (u0 - uym)
-           + m.czpC[k] * (uzp - u0) - m.czmC[k] * (u0 - uzm);
+        double r = (am * am - ap * ap) * (0.25 * rdxg_i);
+        r += ((uym + u0) * (vym + v1m) - (u0 + uyp) * (v0 + vxp)) * (0.25 * rdy_j);
+        r += ((uzm + u0) * (wzm + w1m) - (u0 + uzp) * (w0 + wxp)) * (0.25 * rdz_k);
+        r += cxpF_i * (uxp - u0) - cxmF_i * (u0 - uxm)
+           + cypC_j * (uyp - u0) - cymC_j * (u0 - uym)
+           + czpC_k * (uzp - u0) - czmC_k * (u0 - uzm);
         r += a.Hu ? dPdx * __ldg(a.Hu + iu) : dPdx;
         Fu = r;
       }
@@ -278,12 +308,12 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
         const double umzp = AU(sp, -1, 0);
         const double vzp = AV(sp, 0, 0), vymzp = AV(sp, 0, -1);
         const double am = wzm + w0, ap = w0 + wzp;
-        double r = (am * am - ap * ap) * (0.25 * m.rdzg[k]);
-        r += ((uxm + umzp) * (wxm + w0) - (u0 + uzp) * (w0 + wxp)) * (0.25 * m.rdx[i]);
-        r += ((vym + vymzp) * (wym + w0) - (v0 + vzp) * (w0 + wyp)) * (0.25 * m.rdy[j]);
-        r += m.cxpC[i] * (wxp - w0) - m.cxmC[i] * (w0 - wxm)
-           + m.cypC[j] * (wyp - w0) - m.cymC[j] * (w0 - wym)
-           + m.czpF[k] * (wzp - w0) - m.czmF[k] * (w0 - wzm);
+        double r = (am * am - ap * ap) * (0.25 * rdzg_k);
+        r += ((uxm + umzp) * (wxm + w0) - (u0 + uzp) * (w0 + wxp)) * (0.25 * rdx_i);
+        r += ((vym + vymzp) * (wym + w0) - (v0 + vzp) * (w0 + wyp)) * (0.25 * rdy_j);
+        r += cxpC_i * (wxp - w0) - cxmC_i * (w0 - wxm)
+           + cypC_j * (wyp - w0) - cymC_j * (w0 - wym)
+           + czpF_k * (wzp - w0) - czmF_k * (w0 - wzm);
         r += a.Hw ? dPdz * __ldg(a.Hw + iw) : dPdz;
         Fw = r;
       }
@@ -293,12 +323,12 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
         const double um1 = AU(s0, -1, 1);
         const double wyp = AW(s0, 0, 1), wypzm = AW(sm, 0, 1);
         const double am = vym + v0, ap = v0 + vyp;
-        double r = (am * am - ap * ap) * (0.25 * m.rdyg[j]);
-        r += ((uxm + um1) * (vxm + v0) - (u0 + uyp) * (v0 + vxp)) * (0.25 * m.rdx[i]);
-        r += ((vzm + v0) * (wzm + wypzm) - (v0 + vzp) * (w0 + wyp)) * (0.25 * m.rdz[k]);
-        r += m.cxpC[i] * (vxp - v0) - m.cxmC[i] * (v0 - vxm)
-           + m.cypF[j] * (vyp - v0) - m.cymF[j] * (v0 - vym)
-           + m.czpC[k] * (vzp - v0) - m.czmC[k] * (v0 - vzm);
+        double r = (am * am - ap * ap) * (0.25 * rdyg_j);
+        r += ((uxm + um1) * (vxm + v0) - (u0 + uyp) * (v0 + vxp)) * (0.25 * rdx_i);
+        r += ((vzm + v0) * (wzm + wypzm) - (v0 + vzp) * (w0 + wyp)) * (0.25 * rdz_k);
+        r += cxpC_i * (vxp - v0) - cxmC_i * (v0 - vxm)
+           + cypF_j * (vyp - v0) - cymF_j * (v0 - vym)
+           + czpC_k * (vzp - v0) - czmC_k * (v0 - vzm);
         r += a.Hv ? dPdy * __ldg(a.Hv + iv) : dPdy;
         Fv = r;
       }
