@@ -268,25 +268,42 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
   }
   __syncthreads();
   // nt is a multiple of N: thread -> x index ii, real lines rl0, rl0 + nt/N, ...
+  // taken four at a time: all loads of a batch are issued before any use
   const int ii = tid % N, rls = nt / N;
   const int i = 2 + ii;
-#pragma unroll 4
-  for (int rl = tid / N; rl < 2 * kLinesX; rl += rls) {
-    const int j = s_j[rl], k = s_k[rl];
-    double val = 0.0;
-    if (j > 0) {
-      if (FROM_DIV) {
-        const int64_t iu = idxU(d, i, j, k), iv = idxV(d, i, j, k), iw = idxW(d, i, j, k);
-        val = (a.U[iu] - a.U[iu - 1]) * a.m.rdx[i]
-            + (a.V[iv] - a.V[iv - d.nxg]) * a.m.rdy[j]
-            + (a.W[iw] - a.W[iw - (int64_t)d.nxg * d.nyg]) * a.m.rdz[k];
-      } else {
-        val = a.rhs[idxR(d, i, j, k)];
+  const double rdx_i = FROM_DIV ? a.m.rdx[i] : 0.0;
+  constexpr int kBatch = 4;
+  for (int rb = tid / N; rb < 2 * kLinesX; rb += kBatch * rls) {
+    double x0[kBatch], x1[kBatch], y0[kBatch], y1[kBatch], z0[kBatch], z1[kBatch];
+#pragma unroll
+    for (int q = 0; q < kBatch; ++q) {
+      const int rl = rb + q * rls;
+      const int j = rl < 2 * kLinesX ? s_j[rl] : -1, k = rl < 2 * kLinesX ? s_k[rl] : -1;
+      x0[q] = x1[q] = y0[q] = y1[q] = z0[q] = z1[q] = 0.0;
+      if (j > 0) {
+        if (FROM_DIV) {
+          const int64_t iu = idxU(d, i, j, k), iv = idxV(d, i, j, k), iw = idxW(d, i, j, k);
+          x1[q] = a.U[iu]; x0[q] = a.U[iu - 1];
+          y1[q] = a.V[iv]; y0[q] = a.V[iv - d.nxg];
+          z1[q] = a.W[iw]; z0[q] = a.W[iw - (int64_t)d.nxg * d.nyg];
+        } else {
+          x1[q] = a.rhs[idxR(d, i, j, k)];
+        }
       }
     }
-    C& z = sm.buf[(rl >> 1) * RS + ii];
-    if (rl & 1) z.y = (T)val; else z.x = (T)val;
-    if (a.linesum) sm.sval[rl * N + ii] = val;
+#pragma unroll
+    for (int q = 0; q < kBatch; ++q) {
+      const int rl = rb + q * rls;
+      if (rl >= 2 * kLinesX) continue;
+      const int j = s_j[rl], k = s_k[rl];
+      double val = 0.0;
+      if (j > 0)
+        val = FROM_DIV ? (x1[q] - x0[q]) * rdx_i + (y1[q] - y0[q]) * a.m.rdy[j] + (z1[q] - z0[q]) * a.m.rdz[k]
+                       : x1[q];
+      C& zz = sm.buf[(rl >> 1) * RS + ii];
+      if (rl & 1) zz.y = (T)val; else zz.x = (T)val;
+      if (a.linesum) sm.sval[rl * N + ii] = val;
+    }
   }
   __syncthreads();
   if (a.linesum && tid < 2 * kLinesX) {   // FP64 line sum in a fixed order
@@ -635,7 +652,7 @@ struct XinvArgs {
   int pz;                        // spectrum row pitch
   int rs;                        // shared-memory row stride
   int64_t rbase, nlines;         // lines rbase .. rbase+nlines-1 (a band of j rows)
-  double scale_div;              // nxp*nzp
+  double inv_scale;              // 1/(nxp*nzp)
 };
 
 template <typename T>
@@ -686,7 +703,7 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
   }
   __syncthreads();
   fft_rows_dit_inv<T, 2>(sm.buf, kLinesX, RS, sm.tw, a.P, 128 / (int)sizeof(C));
-  const double sd = a.scale_div;
+  const double rsd = a.inv_scale;
   const int ii = tid % N, rls = nt / N;
   const int i = 2 + ii;
 #pragma unroll 4
@@ -694,7 +711,7 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
     const int j = s_j[rl], k = s_k[rl];
     if (j < 0) continue;
     const C z = sm.buf[(rl >> 1) * RS + ii];
-    double v = (double)((rl & 1) ? z.y : z.x) / sd;
+    double v = (double)((rl & 1) ? z.y : z.x) * rsd;
     if (a.phi00) v += a.phi00[j - 2];
     const int64_t o = idxR(d, i, j, k);
     if (a.accumulate) v += a.rhs[o];
@@ -872,7 +889,7 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     a.d = d; a.spec = spec; a.tw = twx; a.rhs = out; a.phi1 = phi1;
     a.phi00 = f32 ? S.phi00 : nullptr; a.accumulate = accumulate;
     a.P = Px; a.pz = pz; a.rs = rsx; a.rbase = rbase; a.nlines = nlines;
-    a.scale_div = (double)d.Nx * (double)d.Nz;
+    a.inv_scale = 1.0 / ((double)d.Nx * (double)d.Nz);
     k_xfft_inv<T><<<nbx, ntx, smx, s>>>(a);
     C3D_LAUNCH_CHECK(h);
   }
