@@ -95,13 +95,6 @@ struct SpectralState {
   float *mult32 = nullptr, *rdp32 = nullptr;
   double *dl = nullptr, *du = nullptr;       // Dyy(j+1, j) and Dyy(j, j+1), j = 0..Ny-1 (0 past the end)
   float *dl32 = nullptr, *du32 = nullptr;
-  // Partitioned elimination across the CTAs of a cluster (rows j0..j1 per
-  // CTA), layout as the Thomas factors: xh = back substitution of the
-  // forward homogeneous solution h (h(j0-1) = 1), gh = backward homogeneous
-  // solution (x(j1+1) = 1); hend[(m*cs + c)*nkzs + kz'] = h(j1) of CTA c.
-  double *xh = nullptr, *gh = nullptr, *hend = nullptr;
-  float *xh32 = nullptr, *gh32 = nullptr, *hend32 = nullptr;
-  std::vector<double> h_rdp, h_mult, h_du;   // host copies of the factors
   // spectra, layout [m][j][k] = [(m*Ny + (j-2))*pz + (k-2)]: one kx slab is
   // Ny rows of pz complex values (pz*sizeof(complex) a multiple of 16 bytes)
   double2* spec = nullptr;

@@ -123,9 +123,6 @@ static int build_tri_table(Handle* h) {
     if ((rc = dev_alloc(h, &S.dl32, Ny))) return rc;
     if ((rc = dev_alloc(h, &S.du32, Ny))) return rc;
   }
-  S.h_rdp = rdp;
-  S.h_mult = mult;
-  S.h_du = du;
   cudaStream_t s = h->stream;
   C3D_CUDA_TRY(h, cudaMemcpyAsync(S.rdp, rdp.data(), nt * 8, cudaMemcpyHostToDevice, s));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(S.mult, mult.data(), nt * 8, cudaMemcpyHostToDevice, s));
@@ -135,55 +132,6 @@ static int build_tri_table(Handle* h) {
   C3D_CUDA_TRY(h, cudaMemcpyAsync(S.du, du.data(), Ny * 8, cudaMemcpyHostToDevice, s));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(S.dl32, dl32.data(), Ny * 4, cudaMemcpyHostToDevice, s));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(S.du32, du32.data(), Ny * 4, cudaMemcpyHostToDevice, s));
-  return cudaStreamSynchronize(s) == cudaSuccess ? 0 : C3D_ERR_CUDA;
-}
-
-// Homogeneous solutions of the partitioned elimination for a cluster of cs
-// CTAs with jc rows each.  CTA c owns rows j0 = c*jc .. j1; with the local
-// sweeps started from y(j0-1) = 0 and x(j1+1) = 0, the true solution is
-//   x(j) = xl(j) + Y_in * xh(j) + X_in * gh(j),  Y_in = y(j0-1), X_in = x(j1+1),
-//   h(j) = -MULT(j-1) h(j-1), h(j0-1) = 1;  xh = back substitution of h;
-//   gh(j) = -DU(j)/D'(j) gh(j+1), gh(j1+1) = 1;  Y_in(c+1) = yl_c(j1) + h_c(j1) Y_in(c).
-template <typename T>
-static int build_partition_tables(Handle* h, int cs, int jc, T** xh_d, T** gh_d, T** hend_d) {
-  const Dims& d = h->d;
-  SpectralState& S = h->sp;
-  const int Ny = d.Ny, nkx = d.nkx, nkzs = d.nkzs;
-  const int64_t nt = (int64_t)Ny * nkzs * nkx;
-  std::vector<T> xh(nt), gh(nt), hend((size_t)nkx * cs * nkzs);
-  std::vector<double> hv(Ny), xv(Ny), gv(Ny);
-  for (int m = 0; m < nkx; ++m) {
-    for (int kzs = 0; kzs < nkzs; ++kzs) {
-      auto at = [&](int j) { return ((int64_t)m * Ny + j) * nkzs + kzs; };
-      for (int c = 0; c < cs; ++c) {
-        const int j0 = c * jc, j1 = std::min(j0 + jc, Ny) - 1;
-        double hh = 1.0;
-        for (int j = j0; j <= j1; ++j) {
-          hh = (j > 0) ? -S.h_mult[at(j - 1)] * hh : 0.0;
-          hv[j] = hh;
-        }
-        hend[((size_t)m * cs + c) * nkzs + kzs] = (T)hh;
-        double xn = 0.0, gn = 1.0;
-        for (int j = j1; j >= j0; --j) {
-          const double rd = S.h_rdp[at(j)];
-          xn = (hv[j] - S.h_du[j] * xn) * rd;
-          gn = -S.h_du[j] * gn * rd;
-          xh[at(j)] = (T)xn;
-          gh[at(j)] = (T)gn;
-        }
-      }
-    }
-  }
-  int rc;
-  if (*xh_d == nullptr) {
-    if ((rc = dev_alloc(h, xh_d, nt))) return rc;
-    if ((rc = dev_alloc(h, gh_d, nt))) return rc;
-    if ((rc = dev_alloc(h, hend_d, (int64_t)hend.size()))) return rc;
-  }
-  cudaStream_t s = h->stream;
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(*xh_d, xh.data(), nt * sizeof(T), cudaMemcpyHostToDevice, s));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(*gh_d, gh.data(), nt * sizeof(T), cudaMemcpyHostToDevice, s));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(*hend_d, hend.data(), hend.size() * sizeof(T), cudaMemcpyHostToDevice, s));
   return cudaStreamSynchronize(s) == cudaSuccess ? 0 : C3D_ERR_CUDA;
 }
 
@@ -352,9 +300,6 @@ struct YzArgs {
   const T* __restrict__ rdp;     // 1/D'(j) per (m, j, kz')
   const T* __restrict__ dl;      // Dyy(j+1, j)
   const T* __restrict__ du;      // Dyy(j, j+1)
-  const T* __restrict__ xh;      // partitioned-elimination tables
-  const T* __restrict__ gh;
-  const T* __restrict__ hend;
   unsigned long long* err;       // sticky error bits
   FftPasses P;
   int cs;        // CTAs per cluster
@@ -429,31 +374,38 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
 
   fft_rows_dif<T, kYzB>(data + (size_t)blo * RS, bhi - blo, RS, tw, a.P, kRun);
 
-  // pivots of this thread's column for rows j0 .. j0+jn-1 (one column per
+  // pivots of this thread's column for rows j0-1 .. j0+jn-1 (one column per
   // thread when Nz <= blockDim; otherwise reloaded per column below)
   const T* rdp_m = a.rdp + (int64_t)m * Ny * nkzs;
   const bool one_col = Nz <= nt;
   T rdv[JM];
+  T rdm1 = (T)0;                               // pivot of row j0-1 (previous CTA)
   auto load_pivots = [&](int col) {
     const int kz = dif_position_to_k(col, a.P);
     const int kzs = kz <= Nz - kz ? kz : Nz - kz;
 #pragma unroll
     for (int jl = 0; jl < JM; ++jl)
       rdv[jl] = jl < jn ? __ldg(rdp_m + (int64_t)(j0 + jl) * nkzs + kzs) : (T)0;
+    rdm1 = j0 > 0 ? __ldg(rdp_m + (int64_t)(j0 - 1) * nkzs + kzs) : (T)0;
   };
   if (one_col && tid < Nz) load_pivots(tid);
 
-  // Partitioned elimination: every CTA sweeps its own rows at once from
-  // y(j0-1) = 0 and x(j1+1) = 0, publishes its last forward value and its
-  // first back-substituted value, then corrects its rows with the carries
-  //   x(j) = xl(j) + Y_in xh(j) + X_in gh(j).
+  // Partitioned elimination: every CTA sweeps its own rows at once, then
+  // corrects them with carries from its neighbours (no tables):
+  //   forward: y(j) = yl(j) + h(j) Y_in,  h(j0-1) = 1, h(j) = -MULT(j-1) h(j-1),
+  //            Y_in(c+1) = yl_c(j1) + h_c(j1) Y_in(c);
+  //   backward (on the corrected y): x(j) = xl(j) + g(j) X_in,  g(j1+1) = 1,
+  //            g(j) = -DU(j)/D'(j) g(j+1),  X_in(c-1) = xl_c(j0) + g_c(j0) X_in(c).
   // The sweeps take rows in chunks of kCh: loads of a chunk are issued
   // together, the recurrence runs in registers, then the chunk is stored.
   constexpr int kCh = 4;
+  // ylast / xfirst: published end values; hg[col] = (h(j1), g(j0))
+  C* hg = yin;
   for (int col = tid; col < Nz; col += nt) {
     if (!one_col) load_pivots(col);
-    // local forward elimination B(j) -= DL(j-1)/D'(j-1) * B(j-1)
+    // local forward elimination B(j) -= DL(j-1)/D'(j-1) * B(j-1) from y(j0-1) = 0
     C prev = C{(T)0, (T)0};
+    T hcur = (T)1;
 #pragma unroll
     for (int c0 = 0; c0 < JM; c0 += kCh) {
       if (c0 < jn) {
@@ -466,18 +418,19 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
           dlv[u] = (T)0;
           if (jl < jn) {
             bv[u] = data[jl * RS + col];
-            if (jl > 0) dlv[u] = sdl[j0 + jl - 1];
+            if (j0 + jl > 0) dlv[u] = sdl[j0 + jl - 1];
           }
         }
 #pragma unroll
         for (int u = 0; u < kCh; ++u) {
           const int jl = c0 + u;
           if (jl < jn) {
+            const T mu = dlv[u] * (jl == 0 ? rdm1 : rdv[jl > 0 ? jl - 1 : 0]);
             if (jl > 0) {
-              const T mu = dlv[u] * rdv[jl > 0 ? jl - 1 : 0];
               bv[u].x = bv[u].x - mu * prev.x;
               bv[u].y = bv[u].y - mu * prev.y;
             }
+            hcur = -mu * hcur;
             prev = bv[u];
           }
         }
@@ -487,8 +440,55 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
       }
     }
     ylast[col] = prev;
-    // local back substitution x(j) = (B(j) - DU(j) x(j+1)) / D'(j)
+    hg[col].x = hcur;
+  }
+  cl.sync();
+  for (int col = tid; col < Nz; col += nt) {
+    if (!one_col) load_pivots(col);
+    // Y_in = y(j0-1) from the predecessors' end values
+    C Y = C{(T)0, (T)0};
+    for (int c = 0; c < crank; ++c) {
+      const C yl = cl.map_shared_rank(ylast, c)[col];
+      const T he = cl.map_shared_rank(hg, c)[col].x;
+      const T yx = yl.x + he * Y.x, yy = yl.y + he * Y.y;
+      Y.x = yx;
+      Y.y = yy;
+    }
+    // forward correction y += h Y_in (h recomputed), then the local back
+    // substitution x(j) = (y(j) - DU(j) x(j+1)) / D'(j) from x(j1+1) = 0
+    T hcur = (T)1;
+#pragma unroll
+    for (int c0 = 0; c0 < JM; c0 += kCh) {
+      if (c0 < jn && crank > 0) {
+        C bv[kCh];
+        T dlv[kCh];
+#pragma unroll
+        for (int u = 0; u < kCh; ++u) {
+          const int jl = c0 + u;
+          bv[u] = C{(T)0, (T)0};
+          dlv[u] = (T)0;
+          if (jl < jn) {
+            bv[u] = data[jl * RS + col];
+            dlv[u] = sdl[j0 + jl - 1];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kCh; ++u) {
+          const int jl = c0 + u;
+          if (jl < jn) {
+            const T mu = dlv[u] * (jl == 0 ? rdm1 : rdv[jl > 0 ? jl - 1 : 0]);
+            hcur = -mu * hcur;
+            bv[u].x += hcur * Y.x;
+            bv[u].y += hcur * Y.y;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kCh; ++u)
+          if (c0 + u < jn) data[(c0 + u) * RS + col] = bv[u];
+      }
+    }
     C xn = C{(T)0, (T)0};
+    T gcur = (T)1;
 #pragma unroll
     for (int c0 = JM - kCh; c0 >= 0; c0 -= kCh) {
       if (c0 < jn) {
@@ -510,6 +510,7 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
           if (jl < jn) {
             bv[u].x = (bv[u].x - duv[u] * xn.x) * rdv[jl];
             bv[u].y = (bv[u].y - duv[u] * xn.y) * rdv[jl];
+            gcur = -duv[u] * rdv[jl] * gcur;
             xn = bv[u];
           }
         }
@@ -519,69 +520,49 @@ __global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
       }
     }
     xfirst[col] = xn;
-  }
-  cl.sync();
-  // carries: Y_in(c+1) = ylast_c + hend_c Y_in(c) forward over the cluster,
-  // published per CTA; then X_in(c-1) = xfirst_c + Y_in(c) xh_c(j0) + X_in(c) gh_c(j0)
-  // backward from the last CTA (X_in = 0 there)
-  const T* xh_m = a.xh + (int64_t)m * Ny * nkzs;
-  const T* gh_m = a.gh + (int64_t)m * Ny * nkzs;
-  const T* hend_m = a.hend + (int64_t)m * cs * nkzs;
-  for (int col = tid; col < Nz; col += nt) {
-    const int kz = dif_position_to_k(col, a.P);
-    const int kzs = kz <= Nz - kz ? kz : Nz - kz;
-    C Y = C{(T)0, (T)0};
-    for (int c = 0; c < crank; ++c) {
-      const C yl = cl.map_shared_rank(ylast, c)[col];
-      const T he = __ldg(hend_m + (int64_t)c * nkzs + kzs);
-      Y.x = yl.x + he * Y.x;
-      Y.y = yl.y + he * Y.y;
-    }
-    yin[col] = Y;
+    hg[col].y = gcur;
   }
   cl.sync();
   for (int col = tid; col < Nz; col += nt) {
-    const int kz = dif_position_to_k(col, a.P);
-    const int kzs = kz <= Nz - kz ? kz : Nz - kz;
-    const C Y = yin[col];
+    if (!one_col) load_pivots(col);
+    // X_in = x(j1+1) from the successors' first values
     C X = C{(T)0, (T)0};
     for (int c = cs - 1; c > crank; --c) {
       const C xf = cl.map_shared_rank(xfirst, c)[col];
-      const C yc = cl.map_shared_rank(yin, c)[col];
-      const int64_t o = (int64_t)(c * Jc) * nkzs + kzs;
-      const T xhf = __ldg(xh_m + o), ghf = __ldg(gh_m + o);
-      C Xn;
-      Xn.x = xf.x + yc.x * xhf + X.x * ghf;
-      Xn.y = xf.y + yc.y * xhf + X.y * ghf;
-      X = Xn;
+      const T ge = cl.map_shared_rank(hg, c)[col].y;
+      const T xx = xf.x + ge * X.x, xy = xf.y + ge * X.y;
+      X.x = xx;
+      X.y = xy;
     }
-    // correction of this CTA's rows
+    // backward correction x += g X_in (g recomputed from the last row up)
+    T gcur = (T)1;
 #pragma unroll
-    for (int c0 = 0; c0 < JM; c0 += kCh) {
-      if (c0 < jn) {
+    for (int c0 = JM - kCh; c0 >= 0; c0 -= kCh) {
+      if (c0 < jn && crank < cs - 1) {
         C bv[kCh];
-        T xv[kCh], gv[kCh];
+        T duv[kCh];
 #pragma unroll
         for (int u = 0; u < kCh; ++u) {
           const int jl = c0 + u;
           bv[u] = C{(T)0, (T)0};
-          xv[u] = (T)0;
-          gv[u] = (T)0;
+          duv[u] = (T)0;
           if (jl < jn) {
-            const int64_t o = (int64_t)(j0 + jl) * nkzs + kzs;
             bv[u] = data[jl * RS + col];
-            xv[u] = __ldg(xh_m + o);
-            gv[u] = __ldg(gh_m + o);
+            duv[u] = sdu[j0 + jl];
           }
         }
 #pragma unroll
-        for (int u = 0; u < kCh; ++u) {
-          if (c0 + u < jn) {
-            bv[u].x += Y.x * xv[u] + X.x * gv[u];
-            bv[u].y += Y.y * xv[u] + X.y * gv[u];
-            data[(c0 + u) * RS + col] = bv[u];
+        for (int u = kCh - 1; u >= 0; --u) {
+          const int jl = c0 + u;
+          if (jl < jn) {
+            gcur = -duv[u] * rdv[jl] * gcur;
+            bv[u].x += gcur * X.x;
+            bv[u].y += gcur * X.y;
           }
         }
+#pragma unroll
+        for (int u = 0; u < kCh; ++u)
+          if (c0 + u < jn) data[(c0 + u) * RS + col] = bv[u];
       }
     }
     if (a.zero00 && m == 0 && col == 0)
@@ -794,12 +775,11 @@ static bool choose_cluster(const Dims& d, int pz, int& cs, int& jc, int& rs, int
 
 template <typename T>
 static int launch_yz(Handle* h, typename cplx<T>::t* spec, const typename cplx<T>::t* tw, const T* rdp,
-                     const T* dl, const T* du, const T* xh, const T* gh, const T* hend, int cs, int jc,
-                     int rs, int pz, int nt, int smem, int zero00, int rlo, int rhi) {
+                     const T* dl, const T* du, int cs, int jc, int rs, int pz, int nt, int smem, int zero00,
+                     int rlo, int rhi) {
   const Dims& d = h->d;
   YzArgs<T> a{};
   a.d = d; a.spec = spec; a.tw = tw; a.rdp = rdp; a.dl = dl; a.du = du;
-  a.xh = xh; a.gh = gh; a.hend = hend;
   a.err = &h->sc->err;
   a.P = get_passes(d.Nz); a.cs = cs; a.jc = jc; a.rs = rs; a.pz = pz; a.zero00 = zero00;
   a.rlo = rlo; a.rhi = rhi;
@@ -845,17 +825,15 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
   using C = typename cplx<T>::t;
   C* spec;
   const C *twx, *twz;
-  const T *rdp, *dl, *du, *xh, *gh, *hend;
+  const T *rdp, *dl, *du;
   int cs, jc, rs, pz, nt, smem;
   if (f32) {
     spec = (C*)S.spec32; twx = (const C*)S.twx32; twz = (const C*)S.twz32;
     rdp = (const T*)S.rdp32; dl = (const T*)S.dl32; du = (const T*)S.du32;
-    xh = (const T*)S.xh32; gh = (const T*)S.gh32; hend = (const T*)S.hend32;
     cs = S.cs32; jc = S.jc32; rs = S.rs32; pz = S.pz32; nt = S.nt32; smem = S.smem32;
   } else {
     spec = (C*)S.spec; twx = (const C*)S.twx; twz = (const C*)S.twz;
     rdp = (const T*)S.rdp; dl = (const T*)S.dl; du = (const T*)S.du;
-    xh = (const T*)S.xh; gh = (const T*)S.gh; hend = (const T*)S.hend;
     cs = S.cs64; jc = S.jc64; rs = S.rs64; pz = S.pz64; nt = S.nt64; smem = S.smem64;
   }
   const FftPasses Px = get_passes(d.Nx);
@@ -880,8 +858,7 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     }
   }
   if (parts & 2) {
-    int rc = launch_yz<T>(h, spec, twz, rdp, dl, du, xh, gh, hend, cs, jc, rs, pz, nt, smem, f32 ? 1 : 0,
-                          blo, bhi);
+    int rc = launch_yz<T>(h, spec, twz, rdp, dl, du, cs, jc, rs, pz, nt, smem, f32 ? 1 : 0, blo, bhi);
     if (rc) return rc;
   }
   if (parts & 4) {
@@ -1110,12 +1087,7 @@ int poisson_setup(Handle* h) {
     if ((rc = dev_alloc(h, &S.spec, ns))) return rc;
     if ((rc = set_limits<double>(h, S.smem64, S.cs64))) return rc;
   }
-  if ((rc = build_tri_table(h))) return rc;
-  if ((rc = build_partition_tables<double>(h, S.cs64, S.jc64, &S.xh, &S.gh, &S.hend))) return rc;
-  if (S.spec32 != nullptr &&
-      (rc = build_partition_tables<float>(h, S.cs32, S.jc32, &S.xh32, &S.gh32, &S.hend32)))
-    return rc;
-  return 0;
+  return build_tri_table(h);
 }
 
 int mixed_setup(Handle* h) {
@@ -1135,7 +1107,6 @@ int mixed_setup(Handle* h) {
   if ((rc = dev_alloc(h, &S.linesum, (int64_t)d.Ny * d.Nz))) return rc;
   if ((rc = dev_alloc(h, &S.phi00, d.Ny))) return rc;
   if ((rc = set_limits<float>(h, S.smem32, S.cs32))) return rc;
-  if ((rc = build_partition_tables<float>(h, S.cs32, S.jc32, &S.xh32, &S.gh32, &S.hend32))) return rc;
   C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return 0;
 }
