@@ -957,20 +957,21 @@ __global__ void __launch_bounds__(256) k_grad_sub(Dims d, Metric m, const double
   const double px = __ldg(phi + idxR(d, i + 1, j, k));
   const double pz = __ldg(phi + idxR(d, i, j, k + 1));
   const int64_t iu = idxU(d, i, j, k), iw = idxW(d, i, j, k);
-  Uo[iu] = __ldg(Ui + iu) - (px - p0) * m.rdxg[i];
-  Wo[iw] = __ldg(Wi + iw) - (pz - p0) * m.rdzg[k];
-  double py = 0.0;
+  const double un = __ldg(Ui + iu) - (px - p0) * m.rdxg[i];
+  const double wn = __ldg(Wi + iw) - (pz - p0) * m.rdzg[k];
+  double py = 0.0, vn = 0.0;
   if (j <= d.Ny) {
     py = __ldg(phi + idxR(d, i, j + 1, k));
-    const int64_t iv = idxV(d, i, j, k);
-    Vo[iv] = __ldg(Vi + iv) - (py - p0) * m.rdyg[j];
+    vn = __ldg(Vi + idxV(d, i, j, k)) - (py - p0) * m.rdyg[j];
   }
+  Uo[iu] = un;
+  Wo[iw] = wn;
+  if (j <= d.Ny) Vo[idxV(d, i, j, k)] = vn;
   if (k == 2) {
     // the reference's gradient also covers plane nzg-1 (the duplicate of
     // plane 2) for the x and y components (src/differential_operators.f90:38-52)
     const int kd = d.Nz + 2;
-    const int64_t iud = idxU(d, i, j, kd);
-    Uo[iud] = __ldg(Ui + iud) - (px - p0) * m.rdxg[i];
+    Uo[idxU(d, i, j, kd)] = __ldg(Ui + idxU(d, i, j, kd)) - (px - p0) * m.rdxg[i];
     if (j <= d.Ny) {
       const int64_t ivd = idxV(d, i, j, kd);
       Vo[ivd] = __ldg(Vi + ivd) - (py - p0) * m.rdyg[j];
