@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
       a.linesum[r] = sum;
     }
   }
-  fft_rows_dif<T, 2>(sm.buf, kLinesX, RS, sm.tw, a.P, 128 / (int)sizeof(C));
+  fft_rows_dif<T, 1>(sm.buf, kLinesX, RS, sm.tw, a.P, 128 / (int)sizeof(C));
   // split Z = A + iB of the two real lines: A = (Z_m + conj Z_{N-m})/2,
   // B = (Z_m - conj Z_{N-m})/(2i), m = 0..N/2
   const int nk = d.nkx;
@@ -683,7 +683,7 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
     }
   }
   __syncthreads();
-  fft_rows_dit_inv<T, 2>(sm.buf, kLinesX, RS, sm.tw, a.P, 128 / (int)sizeof(C));
+  fft_rows_dit_inv<T, 1>(sm.buf, kLinesX, RS, sm.tw, a.P, 128 / (int)sizeof(C));
   const double rsd = a.inv_scale;
   const int ii = tid % N, rls = nt / N;
   const int i = 2 + ii;
