@@ -17,6 +17,8 @@ CASES = {
     "cfg0_34x65x34": (34, 65, 34, math.pi, math.pi / 2),
     "odd_ny_radix3": (50, 34, 26, 2.0, 1.0),
     "tall_ny_clusters": (18, 129, 18, 1.0, 0.5),
+    # Nz = 54 = 2 * 3^3
+    "nz54_radix3": (26, 20, 56, 1.7, 0.9),
 }
 
 

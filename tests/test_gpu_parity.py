@@ -22,6 +22,8 @@ CASES = {
     "uniform_small": (18, 17, 14, 1.0, 0.7, 0),
     # 127 interior rows: a kx slab spans a 4-CTA cluster (FP64)
     "tall_ny_clusters": (18, 129, 18, 1.0, 0.5, 1),
+    # Nz = 54 = 2 * 3^3: three radix-3 stages, 216-thread slab CTAs
+    "nz54_radix3": (26, 20, 56, 1.7, 0.9, 1),
 }
 
 

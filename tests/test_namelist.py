@@ -53,12 +53,13 @@ def test_library_reader_errors(text, msg):
     assert e.value.code == -1 and msg in str(e.value)
 
 
-def test_library_rejects_odd_nx():
+@pytest.mark.parametrize("nx,nz,which", [(35, 34, "nx"), (34, 29, "nz")])
+def test_library_rejects_odd_nx_nz(nx, nz, which):
     import channel3d_parallel_b200 as c3d
     from channel3d_parallel_b200.channel import namelist_text
     with pytest.raises(c3d.C3DError) as e:
-        c3d.Channel(text=namelist_text(nx_global=35, ny_global=17, nz_global=34, nu=1e-3, CFL=-1e-3))
-    assert e.value.code == -1 and "even" in str(e.value)
+        c3d.Channel(text=namelist_text(nx_global=nx, ny_global=17, nz_global=nz, nu=1e-3, CFL=-1e-3))
+    assert e.value.code == -1 and f"{which} must be even" in str(e.value)
 
 
 def test_namelist_writer_roundtrip():
