@@ -265,7 +265,11 @@ class Channel:
     def stats(self):
         s = L.Stats()
         self._check(self._lib.c3d_get_stats(self.handle, C.byref(s)))
-        return {n: getattr(s, n) for n, _ in L.Stats._fields_}
+        out = {}
+        for n, _ in L.Stats._fields_:
+            v = getattr(s, n)
+            out[n] = list(v) if isinstance(v, C.Array) else v
+        return out
 
     def check_divergence(self):
         v = C.c_double(0.0)

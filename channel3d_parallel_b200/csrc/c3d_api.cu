@@ -781,6 +781,8 @@ int c3d_get_stats(int id, c3d_stats* out) {
   if (rc) return rc;
   h->stats.dPdx = h->dPdx; h->stats.dPdy = h->dPdy; h->stats.dPdz = h->dPdz;
   h->stats.t = h->t; h->stats.dt = h->dt; h->stats.qflow_x_0 = h->Qflow_x_0;
+  h->stats.slab_cluster[0] = h->sp.cs64; h->stats.slab_cluster[1] = h->sp.cs32;
+  h->stats.slab_narrow[0] = h->sp.nw64; h->stats.slab_narrow[1] = h->sp.nw32;
   *out = h->stats;
   return 0;
 }

@@ -105,8 +105,8 @@ struct SpectralState {
   double* phi00 = nullptr;                   // mean solution / (Nx*Nz) per j
   // cluster decomposition of a kx slab: cs CTAs of jc rows of j, shared
   // memory row stride rs complex values, nt threads, smem bytes
-  int cs64 = 1, jc64 = 1, rs64 = 0, nt64 = 256, smem64 = 0;
-  int cs32 = 1, jc32 = 1, rs32 = 0, nt32 = 256, smem32 = 0;
+  int cs64 = 1, jc64 = 1, rs64 = 0, nt64 = 256, smem64 = 0, nw64 = 0;   // nw: narrow slab CTAs
+  int cs32 = 1, jc32 = 1, rs32 = 0, nt32 = 256, smem32 = 0, nw32 = 0;
 };
 
 struct Params {

@@ -287,10 +287,18 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
 // ---------------------------------------------------------------------------
 // kernel 2: z FFT, Thomas in y, inverse z FFT of one kx slab per cluster
 // ---------------------------------------------------------------------------
-// rows of j per CTA (register-resident pivots of one column)
-template <typename T>
-__host__ __device__ constexpr int yz_jmax() { return sizeof(T) == 8 ? 32 : 64; }
-constexpr int kYzThreads = 256;
+// Two launch shapes: wide CTAs (at most 256 threads, two per SM) and narrow
+// CTAs (at most 192 threads, three per SM, half the rows).  The whole FP64
+// spectrum does not fit the aggregate shared memory at once, so the grid runs
+// in two waves either way; narrow CTAs keep more warps per SM in flight and
+// shorten each CTA's sequential sweeps.  yz_jmax: rows of j per CTA (the
+// pivots of one column are held in registers).
+template <typename T, bool NARROW>
+__host__ __device__ constexpr int yz_jmax() { return (sizeof(T) == 8 ? 32 : 64) / (NARROW ? 2 : 1); }
+template <bool NARROW>
+__host__ __device__ constexpr int yz_threads() { return NARROW ? 192 : 256; }
+template <bool NARROW>
+__host__ __device__ constexpr int yz_min_blocks() { return NARROW ? 3 : 2; }
 
 template <typename T>
 struct YzArgs {
@@ -319,10 +327,10 @@ struct YzArgs {
 // 0, each CTA starting from the neighbour row read through distributed
 // shared memory.  After the forward transform column `col` holds wavenumber
 // kz = dif_position_to_k(col); the inverse transform takes that order back.
-template <typename T>
-__global__ void __launch_bounds__(kYzThreads, 2) k_spectral_yz(YzArgs<T> a) {
+template <typename T, bool NARROW>
+__global__ void __launch_bounds__(yz_threads<NARROW>(), yz_min_blocks<NARROW>()) k_spectral_yz(YzArgs<T> a) {
   using C = typename cplx<T>::t;
-  constexpr int JM = yz_jmax<T>();
+  constexpr int JM = yz_jmax<T, NARROW>();
   constexpr int kYzB = 4;   // FFT rows per batch
   constexpr int kRun = 128 / (int)sizeof(C);   // q-runs that fill a shared-memory wavefront
   extern __shared__ __align__(128) unsigned char yz_smem[];
@@ -742,30 +750,33 @@ static int xfft_smem(const Dims& d) {
                (sizeof(T) == 4 ? sizeof(double) * 2 * kLinesX * d.Nx : 0));
 }
 
-// cluster decomposition of a kx slab: smallest power-of-two cluster whose
-// CTAs own at most yz_jmax rows and fit two CTAs per SM (16-CTA clusters may
-// use up to one SM each).  Row stride: FP64 rows of 16-byte values padded to
-// rs = 1 (mod 8) make row-to-row steps conflict-free; FP32 rows stay 16-byte
-// aligned for the bulk copies (rs even) with rs = 2 (mod 4).
-template <typename T>
-static bool choose_cluster(const Dims& d, int pz, int& cs, int& jc, int& rs, int& nt, int& smem) {
+// cluster decomposition of a kx slab: the narrow shape when it fits (Nz <=
+// 192, a CTA within 72 KB so three share an SM), else the wide shape (two
+// CTAs per SM within 112 KB; 16-CTA clusters may use up to one SM each); in
+// each the smallest power-of-two cluster whose CTAs own at most yz_jmax rows.
+// Row stride: FP64 rows of 16-byte values padded to rs = 1 (mod 8) make
+// row-to-row steps conflict-free; FP32 rows stay 16-byte aligned for the
+// bulk copies (rs even) with rs = 2 (mod 4).
+template <typename T, bool NARROW>
+static bool choose_shape(const Dims& d, int rs, int& cs, int& jc, int& nt, int& smem) {
   const size_t esz = sizeof(typename cplx<T>::t);
-  rs = pz;
-  if (sizeof(T) == 8) { while (rs % 8 != 1) ++rs; }
-  else { while (rs % 4 != 2) ++rs; }
+  const int ntmax = yz_threads<NARROW>();
   // a multiple of Nz (one column per thread, fixed FFT butterflies) when
-  // Nz <= kYzThreads
-  nt = kYzThreads;
-  if (d.Nz <= kYzThreads) {
-    nt = d.Nz * (kYzThreads / d.Nz);
+  // Nz <= ntmax
+  nt = ntmax;
+  if (d.Nz <= ntmax) {
+    nt = d.Nz * (ntmax / d.Nz);
     if (nt > 128 && d.Nz >= 128) nt = d.Nz;
+  } else if (NARROW) {
+    return false;
   }
+  const size_t limit = NARROW ? 72 * 1024 : 112 * 1024;
   for (cs = 1; cs <= 16; cs *= 2) {
     jc = (d.Ny + cs - 1) / cs;
     if ((cs - 1) * jc >= d.Ny) continue;      // every CTA must own a row
-    if (jc > yz_jmax<T>()) continue;
+    if (jc > yz_jmax<T, NARROW>()) continue;
     const size_t bytes = esz * ((size_t)jc * rs + 4 * (size_t)d.Nz) + 2 * sizeof(T) * d.Ny;
-    if (bytes <= 112 * 1024 || (cs == 16 && bytes <= 224 * 1024)) {
+    if (bytes <= limit || (!NARROW && cs == 16 && bytes <= 224 * 1024)) {
       smem = (int)bytes;
       return true;
     }
@@ -773,10 +784,71 @@ static bool choose_cluster(const Dims& d, int pz, int& cs, int& jc, int& rs, int
   return false;
 }
 
+// Function attributes are process-wide and handles of different sizes share
+// them, so a kernel's dynamic shared-memory limit only ever grows (per
+// device; handles are created from one host thread at a time).
+template <auto KERN>
+static cudaError_t raise_smem_limit(int bytes) {
+  static int cur[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+  if (bytes <= cur[dev]) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(KERN, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) cur[dev] = bytes;
+  return e;
+}
+
+template <typename T, bool NARROW>
+static int active_clusters(int cs, int nt, int smem) {
+  if (raise_smem_limit<k_spectral_yz<T, NARROW>>(smem) != cudaSuccess) return 0;
+  if (cs > 8 &&
+      cudaFuncSetAttribute(k_spectral_yz<T, NARROW>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    return 0;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)cs, 1, 1);
+  cfg.blockDim = dim3((unsigned)nt, 1, 1);
+  cfg.dynamicSmemBytes = (size_t)smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k_spectral_yz<T, NARROW>, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+// Picks the shape whose kx slabs (one cluster each) run in fewer waves of
+// co-resident clusters, as the device reports them; the narrow shape on a tie.
+template <typename T>
+static bool choose_cluster(const Dims& d, int pz, int& cs, int& jc, int& rs, int& nt, int& smem, int& narrow) {
+  rs = pz;
+  if (sizeof(T) == 8) { while (rs % 8 != 1) ++rs; }
+  else { while (rs % 4 != 2) ++rs; }
+  int ncs, njc, nnt, nsm, wcs, wjc, wnt, wsm;
+  const bool okn = choose_shape<T, true>(d, rs, ncs, njc, nnt, nsm);
+  const bool okw = choose_shape<T, false>(d, rs, wcs, wjc, wnt, wsm);
+  auto waves = [&](int active) { return active > 0 ? (d.nkx + active - 1) / active : 1 << 30; };
+  const int wn = okn ? waves(active_clusters<T, true>(ncs, nnt, nsm)) : 1 << 30;
+  const int ww = okw ? waves(active_clusters<T, false>(wcs, wnt, wsm)) : 1 << 30;
+  if (okn && (!okw || wn <= ww)) {
+    narrow = 1; cs = ncs; jc = njc; nt = nnt; smem = nsm;
+    return true;
+  }
+  if (!okw) return false;
+  narrow = 0; cs = wcs; jc = wjc; nt = wnt; smem = wsm;
+  return true;
+}
+
 template <typename T>
 static int launch_yz(Handle* h, typename cplx<T>::t* spec, const typename cplx<T>::t* tw, const T* rdp,
-                     const T* dl, const T* du, int cs, int jc, int rs, int pz, int nt, int smem, int zero00,
-                     int rlo, int rhi) {
+                     const T* dl, const T* du, int cs, int jc, int rs, int pz, int nt, int smem, int narrow,
+                     int zero00, int rlo, int rhi) {
   const Dims& d = h->d;
   YzArgs<T> a{};
   a.d = d; a.spec = spec; a.tw = tw; a.rdp = rdp; a.dl = dl; a.du = du;
@@ -795,7 +867,8 @@ static int launch_yz(Handle* h, typename cplx<T>::t* spec, const typename cplx<T
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  C3D_CUDA_TRY(h, cudaLaunchKernelEx(&cfg, k_spectral_yz<T>, a));
+  if (narrow) C3D_CUDA_TRY(h, cudaLaunchKernelEx(&cfg, k_spectral_yz<T, true>, a));
+  else C3D_CUDA_TRY(h, cudaLaunchKernelEx(&cfg, k_spectral_yz<T, false>, a));
   C3D_LAUNCH_CHECK(h);
   return 0;
 }
@@ -804,12 +877,15 @@ template <typename T>
 static int set_limits(Handle* h, int smem_yz, int cs) {
   const Dims& d = h->d;
   const int smx = xfft_smem<T>(d);
-  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_xfft_fwd<true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
-  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_xfft_fwd<false, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
-  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_xfft_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx));
-  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_spectral_yz<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_yz));
-  if (cs > 8)
-    C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_spectral_yz<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  C3D_CUDA_TRY(h, (raise_smem_limit<k_xfft_fwd<true, T>>(smx)));
+  C3D_CUDA_TRY(h, (raise_smem_limit<k_xfft_fwd<false, T>>(smx)));
+  C3D_CUDA_TRY(h, (raise_smem_limit<k_xfft_inv<T>>(smx)));
+  C3D_CUDA_TRY(h, (raise_smem_limit<k_spectral_yz<T, true>>(smem_yz)));
+  C3D_CUDA_TRY(h, (raise_smem_limit<k_spectral_yz<T, false>>(smem_yz)));
+  if (cs > 8) {
+    C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_spectral_yz<T, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_spectral_yz<T, false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  }
   return 0;
 }
 
@@ -826,15 +902,15 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
   C* spec;
   const C *twx, *twz;
   const T *rdp, *dl, *du;
-  int cs, jc, rs, pz, nt, smem;
+  int cs, jc, rs, pz, nt, smem, narrow;
   if (f32) {
     spec = (C*)S.spec32; twx = (const C*)S.twx32; twz = (const C*)S.twz32;
     rdp = (const T*)S.rdp32; dl = (const T*)S.dl32; du = (const T*)S.du32;
-    cs = S.cs32; jc = S.jc32; rs = S.rs32; pz = S.pz32; nt = S.nt32; smem = S.smem32;
+    cs = S.cs32; jc = S.jc32; rs = S.rs32; pz = S.pz32; nt = S.nt32; smem = S.smem32; narrow = S.nw32;
   } else {
     spec = (C*)S.spec; twx = (const C*)S.twx; twz = (const C*)S.twz;
     rdp = (const T*)S.rdp; dl = (const T*)S.dl; du = (const T*)S.du;
-    cs = S.cs64; jc = S.jc64; rs = S.rs64; pz = S.pz64; nt = S.nt64; smem = S.smem64;
+    cs = S.cs64; jc = S.jc64; rs = S.rs64; pz = S.pz64; nt = S.nt64; smem = S.smem64; narrow = S.nw64;
   }
   const FftPasses Px = get_passes(d.Nx);
   if (bhi < 0) bhi = d.Ny - 1;                 // band of j rows (0-based j-2); full by default
@@ -858,7 +934,7 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     }
   }
   if (parts & 2) {
-    int rc = launch_yz<T>(h, spec, twz, rdp, dl, du, cs, jc, rs, pz, nt, smem, f32 ? 1 : 0, blo, bhi);
+    int rc = launch_yz<T>(h, spec, twz, rdp, dl, du, cs, jc, rs, pz, nt, smem, narrow, f32 ? 1 : 0, blo, bhi);
     if (rc) return rc;
   }
   if (parts & 4) {
@@ -1078,7 +1154,7 @@ int poisson_setup(Handle* h) {
   int rc;
   if (S.spec == nullptr) {
     S.pz64 = d.Nz;
-    if (!choose_cluster<double>(d, S.pz64, S.cs64, S.jc64, S.rs64, S.nt64, S.smem64)) {
+    if (!choose_cluster<double>(d, S.pz64, S.cs64, S.jc64, S.rs64, S.nt64, S.smem64, S.nw64)) {
       h->last_error = "ny_global too large for one 16-CTA cluster per kx slab";
       return C3D_ERR_UNSUPPORTED;
     }
@@ -1096,7 +1172,7 @@ int mixed_setup(Handle* h) {
   SpectralState& S = h->sp;
   if (S.spec32 != nullptr) return 0;
   S.pz32 = d.Nz + (d.Nz & 1);
-  if (!choose_cluster<float>(d, S.pz32, S.cs32, S.jc32, S.rs32, S.nt32, S.smem32)) {
+  if (!choose_cluster<float>(d, S.pz32, S.cs32, S.jc32, S.rs32, S.nt32, S.smem32, S.nw32)) {
     h->last_error = "ny_global too large for the FP32 cluster decomposition";
     return C3D_ERR_UNSUPPORTED;
   }

@@ -41,7 +41,8 @@ class Stats(C.Structure):
                 ("dPdx", C.c_double), ("dPdy", C.c_double), ("dPdz", C.c_double),
                 ("t", C.c_double), ("dt", C.c_double), ("qflow_x_0", C.c_double),
                 ("status", C.c_int32), ("precond_mode", C.c_int32),
-                ("last_bicgstab_ms", C.c_double), ("bicgstab_ms", C.c_double)]
+                ("last_bicgstab_ms", C.c_double), ("bicgstab_ms", C.c_double),
+                ("slab_cluster", C.c_int32 * 2), ("slab_narrow", C.c_int32 * 2)]
 
 
 _D = C.POINTER(C.c_double)

@@ -106,6 +106,8 @@ typedef struct c3d_stats {
   int32_t precond_mode;        /* preconditioner of the last Schur solve      */
   double  last_bicgstab_ms;    /* device time of the last Schur solve (ms)    */
   double  bicgstab_ms;         /* accumulated device time of Schur solves     */
+  int32_t slab_cluster[2];     /* CTAs per kx-slab cluster of the y-z solve: FP64, FP32 */
+  int32_t slab_narrow[2];      /* 1: narrow slab CTAs (<= 192 threads, 3 per SM); FP64, FP32 */
 } c3d_stats;
 
 /* ---- lifecycle ------------------------------------------------------------

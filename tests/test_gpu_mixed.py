@@ -19,6 +19,7 @@ CASES = {
     "tall_ny_clusters": (18, 129, 18, 1.0, 0.5),
     # Nz = 54 = 2 * 3^3
     "nz54_radix3": (26, 20, 56, 1.7, 0.9),
+    "nz256_wide_slab": (18, 17, 258, 1.0, 2.0),
 }
 
 
@@ -55,7 +56,9 @@ def test_mixed_refined_matches_fp64_oracle(case, nsteps):
         errs = {n: rel(ch.download(n), r[1:, 1:, 1:]) for n, r in (("U", st.U), ("V", st.V), ("W", st.W))}
         assert max(errs.values()) < 1e-10, errs
         assert ch.check_divergence() < 1e-12
-        assert ch.stats()["refinement_sweeps"] == 1
+        s = ch.stats()
+        assert s["refinement_sweeps"] == 1
+        assert s["slab_narrow"][1] == (0 if g.nz - 2 > 192 else 1)
     finally:
         ch.close()
 

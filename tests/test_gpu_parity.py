@@ -24,6 +24,8 @@ CASES = {
     "tall_ny_clusters": (18, 129, 18, 1.0, 0.5, 1),
     # Nz = 54 = 2 * 3^3: three radix-3 stages, 216-thread slab CTAs
     "nz54_radix3": (26, 20, 56, 1.7, 0.9, 1),
+    # Nz = 256 > 192: the wide slab CTAs (256 threads, two per SM)
+    "nz256_wide_slab": (18, 17, 258, 1.0, 2.0, 1),
 }
 
 
@@ -137,6 +139,9 @@ def test_rk3_steps(pair, nsteps):
     dt = 1e-3
     assert abs(s["dPdx"] - st.dPdx) <= 1e-9 * abs(st.dPdx) + 50 * 2.2e-16 * abs(st.Qflow_x_0) / dt
     assert s["steps"] == nsteps
+    # Nz > 192 only fits the wide slab CTAs; small grids run in one wave of
+    # clusters either way and take the narrow shape
+    assert s["slab_narrow"][0] == (0 if g.nz - 2 > 192 else 1)
     assert ch.check_divergence() < 1e-12
     assert ch.check_finite() == 0
 
@@ -211,5 +216,33 @@ def test_full_size_one_step_parity():
         for name, ref in (("U", st.U), ("V", st.V), ("W", st.W), ("P", st.P)):
             assert rel(ch.download(name), ref[1:, 1:, 1:]) < 1e-10, name
         ch.compute_time_step_RK3(4)
+        # 97 slabs: 4-CTA wide clusters run in two waves, 8-CTA narrow ones
+        # would take three
+        assert ch.stats()["slab_cluster"][0] == 4 and ch.stats()["slab_narrow"][0] == 0
         assert ch.check_divergence() < 1e-12
         assert abs(ch.compute_mean_mass_flow_U() - st.Qflow_x_0) < 1e-13
+
+
+def test_handles_of_different_sizes_coexist():
+    """Kernel shared-memory limits are process-wide: a small handle created
+    after a large one must not lower the large one's limits."""
+    import channel3d_parallel_b200 as c3d
+    nu = 1.0 / 5600.0
+    p = co.channel_params(194, 129, 194, 4 * math.pi, 4 * math.pi / 3, nu)
+    g = co.Grid(p)
+    st = co.seeded_initial_state(g, p["dpdx"])
+    with c3d.Channel(nx_global=194, ny_global=129, nz_global=194, Lxp=4 * math.pi,
+                     Lzp=4 * math.pi / 3, nu=nu, CFL=-1e-3, x_mass_cte=1, grid_type=1,
+                     alpha_stretch=2.0, dPdx=p["dpdx"]) as big:
+        big.set_grid(g.x[1:], g.y[1:], g.z[1:])
+        for name, ref in (("U", st.U), ("V", st.V), ("W", st.W)):
+            big.upload(name, ref[1:, 1:, 1:])
+        big.set_scalars(dPdx=st.dPdx, Qflow_x_0=st.Qflow_x_0)
+        ps, gs, sts, small = make_pair("uniform_small")
+        try:
+            small.compute_time_step_RK3(2)
+            big.compute_time_step_RK3(2)
+            assert big.check_divergence() < 1e-12
+            assert small.check_divergence() < 1e-12
+        finally:
+            small.close()
