@@ -12,6 +12,10 @@ instead by known-answer tests derived from the mathematics (single Fourier
 modes through the Poisson solve, Poiseuille balance, delta-function moment
 identities, E/R adjointness, ...) under ``tests/``.
 
+``cpu_rk3.cpp`` (with its ctypes wrapper ``cpu_rk3.py``) restates the same
+FP64 RK3 step in C++/OpenMP; it is the timed CPU baseline of ``bench.py`` and
+is itself checked against the NumPy restatement.
+
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
 leg may import this package, and only as the checker or as the timed CPU
 baseline.  The product path (``channel3d_parallel_b200``) never imports it.
