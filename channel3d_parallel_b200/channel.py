@@ -221,10 +221,37 @@ class Channel:
         self._check(self._lib.c3d_compute_dPx_for_constant_mass_flow(self.handle, C.byref(v)))
         return v.value
 
+    def compute_dPy_for_constant_mass_flow(self):
+        """src/mass_flow.f90:190-221: Qflow_y_0 - Int_V/norm."""
+        v = C.c_double(0.0)
+        self._check(self._lib.c3d_compute_dPy_for_constant_mass_flow(self.handle, C.byref(v)))
+        return v.value
+
+    def compute_dPz_for_constant_mass_flow(self):
+        """src/mass_flow.f90:236-267: Qflow_z_0 - Int_W/norm (W read through
+        the routine's declared extents, as the reference does)."""
+        v = C.c_double(0.0)
+        self._check(self._lib.c3d_compute_dPz_for_constant_mass_flow(self.handle, C.byref(v)))
+        return v.value
+
     def compute_mean_mass_flow_U(self):
         v = C.c_double(0.0)
         self._check(self._lib.c3d_compute_mean_mass_flow_u(self.handle, C.byref(v)))
         return v.value
+
+    def compute_mean_mass_flow_V(self):
+        v = C.c_double(0.0)
+        self._check(self._lib.c3d_compute_mean_mass_flow_v(self.handle, C.byref(v)))
+        return v.value
+
+    def compute_mean_mass_flow_W(self):
+        v = C.c_double(0.0)
+        self._check(self._lib.c3d_compute_mean_mass_flow_w(self.handle, C.byref(v)))
+        return v.value
+
+    def set_flow_targets(self, Qflow_x_0, Qflow_y_0=0.0, Qflow_z_0=0.0):
+        """Qflow_x_0, Qflow_y_0, Qflow_z_0 (src/global.f90:180)."""
+        self._check(self._lib.c3d_set_flow_targets(self.handle, Qflow_x_0, Qflow_y_0, Qflow_z_0))
 
     def compute_pressure(self):
         self._check(self._lib.c3d_compute_pressure(self.handle))
@@ -378,8 +405,8 @@ def laminar_perturbed_fields(grid, dims, dPdx, nu, Ly=2.0, amplitude=0.1, seed=0
 def seeded_initial_state(ch, dPdx, nu, amplitude=0.1, seed=0, dt=1e-3):
     """Set the seeded initial state on the device: host fields of
     ``laminar_perturbed_fields``, boundary conditions, one projection (dt
-    cancels), boundary conditions, and Qflow_x_0 from the result
-    (app/main.f90:90).  Returns Qflow_x_0."""
+    cancels), boundary conditions, and Qflow_x_0, Qflow_y_0, Qflow_z_0 from
+    the result (app/main.f90:90-92).  Returns Qflow_x_0."""
     g = ch.grid()
     U, V, W = laminar_perturbed_fields(g, ch.dims, dPdx, nu, amplitude=amplitude, seed=seed)
     ch.upload("U", U)
@@ -393,4 +420,5 @@ def seeded_initial_state(ch, dPdx, nu, amplitude=0.1, seed=0, dt=1e-3):
     ch.apply_boundary_conditions("UVW")
     q = ch.compute_mean_mass_flow_U()
     ch.set_scalars(dPdx=dPdx, t=0.0, Qflow_x_0=q)
+    ch.set_flow_targets(q, ch.compute_mean_mass_flow_V(), ch.compute_mean_mass_flow_W())
     return q

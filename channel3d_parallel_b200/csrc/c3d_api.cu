@@ -198,7 +198,8 @@ static int setup_metric(Handle* h, const double* xf, const double* yf, const dou
     cxpC[i] = nu / ((xg[i + 1] - xg[i]) * (x[i] - x[i - 1]));
     cxmC[i] = nu / ((xg[i] - xg[i - 1]) * (x[i] - x[i - 1]));
   }
-  std::vector<double> rdy(LY, 0), rdyg(LY, 0), cypC(LY, 0), cymC(LY, 0), cypF(LY, 0), cymF(LY, 0), wq(LY, 0);
+  std::vector<double> rdy(LY, 0), rdyg(LY, 0), cypC(LY, 0), cymC(LY, 0), cypF(LY, 0), cymF(LY, 0), wq(LY, 0),
+      wqv(LY, 0);
   for (int j = 2; j <= ny; ++j) rdy[j] = 1.0 / (y[j] - y[j - 1]);
   for (int j = 1; j <= nyg - 1; ++j) rdyg[j] = 1.0 / (yg[j + 1] - yg[j]);
   for (int j = 2; j <= nyg - 1; ++j) {
@@ -210,6 +211,7 @@ static int setup_metric(Handle* h, const double* xf, const double* yf, const dou
     cymF[j] = nu / ((y[j] - y[j - 1]) * (yg[j + 1] - yg[j]));
   }
   for (int j = 3; j <= nyg - 1; ++j) wq[j] = 0.5 * (yg[j] - yg[j - 1]);
+  for (int j = 2; j <= ny; ++j) wqv[j] = 0.5 * (y[j] - y[j - 1]);
   std::vector<double> rdz(LZ, 0), rdzg(LZ, 0), czpC(LZ, 0), czmC(LZ, 0), czpF(LZ, 0), czmF(LZ, 0);
   for (int k = 2; k <= nz; ++k) rdz[k] = 1.0 / (z[k] - z[k - 1]);
   for (int k = 1; k <= nzg - 1; ++k) rdzg[k] = 1.0 / (zg[k + 1] - zg[k]);
@@ -225,7 +227,7 @@ static int setup_metric(Handle* h, const double* xf, const double* yf, const dou
   add(rdx, &m.rdx); add(rdxg, &m.rdxg); add(cxpF, &m.cxpF); add(cxmF, &m.cxmF);
   add(cxpC, &m.cxpC); add(cxmC, &m.cxmC);
   add(rdy, &m.rdy); add(rdyg, &m.rdyg); add(cypC, &m.cypC); add(cymC, &m.cymC);
-  add(cypF, &m.cypF); add(cymF, &m.cymF); add(wq, &m.wq);
+  add(cypF, &m.cypF); add(cymF, &m.cymF); add(wq, &m.wq); add(wqv, &m.wqv);
   add(rdz, &m.rdz); add(rdzg, &m.rdzg); add(czpC, &m.czpC); add(czmC, &m.czmC);
   add(czpF, &m.czpF); add(czmF, &m.czmF);
   if (h->metric_buf == nullptr) {
@@ -315,6 +317,7 @@ static int build(Handle* h, const std::vector<double>* xg_in = nullptr) {
   h->dPdz = p.dPdz;
   h->dPdy = 0.0;
   h->Qflow_x_0 = p.Qflow_x_0;
+  h->Qflow_z_0 = p.Qflow_z_0;
   h->dt = p.CFL < 0 ? -p.CFL : 0.0;
   DevScalars s{};
   s.dPdx = h->dPdx; s.dPdy = h->dPdy; s.dPdz = h->dPdz;
@@ -477,7 +480,7 @@ static int enqueue_step(Handle* h, double dt, double to) {
       if (rc > 0) warn = rc;
     }
   }
-  if (h->p.x_mass_cte == 1) {                                  // :187-193
+  if (h->p.x_mass_cte == 1 || h->p.y_mass_cte == 1 || h->p.z_mass_cte == 1) {   // :187-211
     if ((rc = launch_massflow_correction(h, dt))) return rc;
   }
   return warn;
@@ -685,7 +688,26 @@ int c3d_compute_dt(int id, double* dt) {
 int c3d_compute_mean_mass_flow_u(int id, double* q) {
   GET_HANDLE(id);
   if (!q) return C3D_ERR_PARAM;
-  RET(h, massflow_u(h, h->U, h->ib ? ib_hu(h) : nullptr, q));
+  RET(h, massflow(h, 0, false, q));
+}
+
+int c3d_compute_mean_mass_flow_v(int id, double* q) {
+  GET_HANDLE(id);
+  if (!q) return C3D_ERR_PARAM;
+  RET(h, massflow(h, 1, false, q));
+}
+
+int c3d_compute_mean_mass_flow_w(int id, double* q) {
+  GET_HANDLE(id);
+  if (!q) return C3D_ERR_PARAM;
+  RET(h, massflow(h, 2, false, q));
+}
+
+int c3d_set_flow_targets(int id, double qx, double qy, double qz) {
+  GET_HANDLE(id);
+  h->Qflow_x_0 = qx; h->Qflow_y_0 = qy; h->Qflow_z_0 = qz;
+  if (h->step_exec) { cudaGraphExecDestroy(h->step_exec); h->step_exec = nullptr; }
+  RET(h, 0);
 }
 
 int c3d_compute_rhs_u(int id) { GET_HANDLE(id); RET(h, launch_rhs_only(h, 1)); }
@@ -744,9 +766,29 @@ int c3d_compute_dPx_for_constant_mass_flow(int id, double* dPdx) {
   GET_HANDLE(id);
   if (!dPdx) return C3D_ERR_PARAM;
   double q = 0;
-  int rc = massflow_u(h, h->U, h->ib ? ib_hu(h) : nullptr, &q);
+  int rc = massflow(h, 0, false, &q);
   if (rc) RET(h, rc);
   *dPdx = h->Qflow_x_0 - q;
+  RET(h, 0);
+}
+
+int c3d_compute_dPy_for_constant_mass_flow(int id, double* dPdy) {
+  GET_HANDLE(id);
+  if (!dPdy) return C3D_ERR_PARAM;
+  double q = 0;
+  int rc = massflow(h, 1, false, &q);
+  if (rc) RET(h, rc);
+  *dPdy = h->Qflow_y_0 - q;
+  RET(h, 0);
+}
+
+int c3d_compute_dPz_for_constant_mass_flow(int id, double* dPdz) {
+  GET_HANDLE(id);
+  if (!dPdz) return C3D_ERR_PARAM;
+  double q = 0;
+  int rc = massflow(h, 2, true, &q);
+  if (rc) RET(h, rc);
+  *dPdz = h->Qflow_z_0 - q;
   RET(h, 0);
 }
 
@@ -781,6 +823,7 @@ int c3d_get_stats(int id, c3d_stats* out) {
   if (rc) return rc;
   h->stats.dPdx = h->dPdx; h->stats.dPdy = h->dPdy; h->stats.dPdz = h->dPdz;
   h->stats.t = h->t; h->stats.dt = h->dt; h->stats.qflow_x_0 = h->Qflow_x_0;
+  h->stats.qflow_y_0 = h->Qflow_y_0; h->stats.qflow_z_0 = h->Qflow_z_0;
   h->stats.slab_cluster[0] = h->sp.cs64; h->stats.slab_cluster[1] = h->sp.cs32;
   h->stats.slab_narrow[0] = h->sp.nw64; h->stats.slab_narrow[1] = h->sp.nw32;
   *out = h->stats;

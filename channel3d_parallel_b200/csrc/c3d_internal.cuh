@@ -68,15 +68,16 @@ struct Metric {
   const double *rdzg;    // 1/(zg(k+1)-zg(k))
   const double *czpC, *czmC;   // viscous z for z-centre fields (U, V)
   const double *czpF, *czmF;   // viscous z for z-face fields (W)
-  // mass-flow weights 0.5*(yg(j)-yg(j-1))
-  const double *wq;
+  // mass-flow weights 0.5*(yg(j)-yg(j-1)) (U, W) and 0.5*(y(j)-y(j-1)) (V)
+  const double *wq, *wqv;
 };
 
 // device scalars shared by kernels of one step (kept on device so the step
 // can be captured in one CUDA graph)
 struct DevScalars {
   double dPdx, dPdy, dPdz;
-  double shift;          // last constant-mass-flow correction
+  double shift;          // last constant-mass-flow correction of U
+  double shift_v, shift_w;  // same for V and W (y_mass_cte, z_mass_cte)
   double qflow;          // last bulk flux (Int_U / norm)
   double dpdx_prev;
   unsigned long long err;   // sticky kernel error bits (bit 0: a bounded copy wait gave up)
@@ -169,7 +170,7 @@ struct Handle {
   int refine_sweeps = 1;          // mixed precision: refinement projections per stage
   // state
   double t = 0, dt = 0;
-  double dPdx = 0, dPdy = 0, dPdz = 0, Qflow_x_0 = 0;
+  double dPdx = 0, dPdy = 0, dPdz = 0, Qflow_x_0 = 0, Qflow_y_0 = 0, Qflow_z_0 = 0;
   bool P_pending = false;        // P must be rebuilt from phi1 before download
   double P_pending_dt = 0;
   int poisson_mode = C3D_POISSON_FP64;
@@ -248,7 +249,7 @@ int mixed_setup(Handle* h);
 void mixed_free(Handle* h);
 // mass flow and reductions (k_massflow.cu)
 int launch_massflow_correction(Handle* h, double dt);
-int massflow_u(Handle* h, const double* U, const double* Hu, double* q_out);
+int massflow(Handle* h, int comp, bool u_view, double* q_out);
 int max_abs_divergence(Handle* h, const double* U, const double* V, const double* W, double* out);
 int check_finite(Handle* h, bool* ok);
 int compute_dt_cfl(Handle* h, double* dt);

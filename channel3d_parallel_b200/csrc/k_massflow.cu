@@ -1,12 +1,14 @@
 // Constant-mass-flow correction and device reductions.
 //
-// compute_dPx_for_constant_mass_flow (src/mass_flow.f90:144-175) and its use
-// at the end of compute_time_step_RK3 (src/time_integration.f90:187-193):
+// compute_dP{x,y,z}_for_constant_mass_flow (src/mass_flow.f90:144-267) and
+// their use at the end of compute_time_step_RK3 (src/time_integration.f90:187-211);
+// for x:
 //   Int_U = sum_{k=2}^{nzg-1} sum_{j=3}^{nyg-1} sum_{i=2}^{nx-1}
 //              (Hu(j) U(j) + Hu(j-1) U(j-1)) * 0.5*(yg(j)-yg(j-1))
 //   norm  = same with U = 1
 //   shift = Qflow_x_0 - Int_U/norm;  U(interior) += shift;  BC;
-//   dPdx  = 0.5*(dPdx_prev + shift/dt).
+//   dPdx  = 0.5*(dPdx_prev + shift/dt);
+// y (V between the walls y(1:ny)) and z (W, yg weights) likewise.
 // The z range includes plane nzg-1, the periodic duplicate of plane 2, exactly
 // as the reference's last rank does.  Reductions are deterministic: a fixed
 // grid writes per-block partials that one block sums in a fixed order.
@@ -43,35 +45,76 @@ __device__ __forceinline__ double2 block_sum2(double2 v) {
   return r;
 }
 
-// (Int_U, norm) over rows (j, k), j = 3..nyg-1, k = 2..nzg-1, one warp per
-// x-row (i = 2..nx-1) so that a row's index arithmetic is done once; Hu may
-// be null (H = 1).  Every block writes its partial sum; the last block to
-// finish (ticket in DevScalars) adds the partials in block order and
-//   mode 0: stores qflow = Int_U/norm;
-//   mode 1: also the constant-flux correction shift and dPdx.
-__global__ void __launch_bounds__(kRedThreads) k_massflow(Dims d, Metric m, const double* __restrict__ U,
-                                                         const double* __restrict__ Hu,
-                                                         double2* __restrict__ part, DevScalars* sc,
-                                                         double q0, double dt, int mode) {
-  const int ni = d.Nx, nj = d.nyg - 3, nk = d.Nz + 1;
-  const int nrows = nj * nk;
+// Trapezoid flux of one field: sum over rows (j, k) and i of
+//   (H(j) F(j) + H(j-1) F(j-1)) * w(j)      and      (H(j) + H(j-1)) * w(j)
+// with F(i,j,k) at Fortran offset (i-1) + f1*((j-1) + f2*(k-1)) and H at the
+// same position of its own extents (h1, h2); H null means H = 1.
+struct FluxView {
+  const double* F;
+  int64_t f1, f2;
+  const double* H;
+  int64_t h1, h2;
+  const double* w;                // per-j weight
+  int i0, ni, j0, nj, k0, nk;     // i0..i0+ni-1, j0..j0+nj-1 (pairs j, j-1), k0..k0+nk-1
+};
+
+// the three fluxes of src/mass_flow.f90 on the handle's fields
+//   comp 0: U between yg(2:nyg-1), i = 2..nx-1, k = 2..nzg-1 (:24-53, :144-175)
+//   comp 1: V between y(1:ny),     i = 2..nxg-1, k = 2..nzg-1 (:62-91, :190-221)
+//   comp 2: W between yg(2:nyg-1), i = 2..nxg-1, k = 2..nz-1  (:100-129, :236-267)
+// For comp 2 the correction routine declares its dummy W with the extents of
+// U, Dimension(nx,nyg,nzg) (:238), so its W(i,j,k) is the real W's element at
+// offset (i-1) + nx*((j-1) + nyg*(k-1)); u_view = true reads that view (every
+// offset reached lies inside W), false the true layout (compute_mean_mass_flow_W).
+static FluxView flux_view(Handle* h, int comp, const double* F, const double* H, bool u_view) {
+  const Dims& d = h->d;
+  FluxView v{};
+  v.F = F;
+  v.H = H;
+  if (comp == 0) {
+    v.f1 = v.h1 = d.nx; v.f2 = v.h2 = d.nyg;
+    v.w = h->m.wq;
+    v.i0 = 2; v.ni = d.nx - 2; v.j0 = 3; v.nj = d.nyg - 3; v.k0 = 2; v.nk = d.nzg - 2;
+  } else if (comp == 1) {
+    v.f1 = v.h1 = d.nxg; v.f2 = v.h2 = d.ny;
+    v.w = h->m.wqv;
+    v.i0 = 2; v.ni = d.nxg - 2; v.j0 = 2; v.nj = d.ny - 1; v.k0 = 2; v.nk = d.nzg - 2;
+  } else {
+    v.f1 = u_view ? d.nx : d.nxg; v.f2 = d.nyg;
+    v.h1 = d.nxg; v.h2 = d.nyg;
+    v.w = h->m.wq;
+    v.i0 = 2; v.ni = d.nxg - 2; v.j0 = 3; v.nj = d.nyg - 3; v.k0 = 2; v.nk = d.nz - 2;
+  }
+  return v;
+}
+
+// One warp per x-row (j, k) so that a row's index arithmetic is done once.
+// Every block writes its partial sum; the last block to finish (ticket in
+// DevScalars) adds the partials in block order and
+//   mode 0: stores qflow = flux/norm;
+//   mode 1: also the constant-flux correction of component comp
+//           (shift = q0 - flux/norm) and dPd{x,y,z} = (dPd_prev + shift/dt)/2.
+__global__ void __launch_bounds__(kRedThreads) k_flux(FluxView v, double2* __restrict__ part, DevScalars* sc,
+                                                     double q0, double dt, int mode, int comp) {
+  const int nrows = v.nj * v.nk;
   const int lane = threadIdx.x & 31;
   const int wpb = kRedThreads / 32;
   double2 acc = make_double2(0.0, 0.0);
   for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < nrows; row += gridDim.x * wpb) {
-    const int kk = row / nj;
-    const int j = 3 + (row - kk * nj);
-    const int k = 2 + kk;
-    const double w = m.wq[j];
-    const int64_t a0 = idxU(d, 2, j, k), b0 = idxU(d, 2, j - 1, k);
-    for (int ii = lane; ii < ni; ii += 32) {
-      const int64_t a = a0 + ii, b = b0 + ii;
-      if (Hu) {
-        const double ha = Hu[a], hb = Hu[b];
-        acc.x += (ha * U[a] + hb * U[b]) * w;
+    const int kk = row / v.nj;
+    const int j = v.j0 + (row - kk * v.nj);
+    const int k = v.k0 + kk;
+    const double w = v.w[j];
+    const int64_t a0 = (v.i0 - 1) + v.f1 * ((j - 1) + v.f2 * (int64_t)(k - 1)), b0 = a0 - v.f1;
+    const int64_t ha0 = (v.i0 - 1) + v.h1 * ((j - 1) + v.h2 * (int64_t)(k - 1)), hb0 = ha0 - v.h1;
+    for (int ii = lane; ii < v.ni; ii += 32) {
+      const double fa = v.F[a0 + ii], fb = v.F[b0 + ii];
+      if (v.H) {
+        const double ha = v.H[ha0 + ii], hb = v.H[hb0 + ii];
+        acc.x += (ha * fa + hb * fb) * w;
         acc.y += (ha + hb) * w;
       } else {
-        acc.x += (U[a] + U[b]) * w;
+        acc.x += (fa + fb) * w;
         acc.y += 2.0 * w;
       }
     }
@@ -88,9 +131,9 @@ __global__ void __launch_bounds__(kRedThreads) k_massflow(Dims d, Metric m, cons
   __threadfence();
   double2 t = make_double2(0.0, 0.0);
   for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-    const double2 v = __ldcg(part + b);
-    t.x += v.x;
-    t.y += v.y;
+    const double2 pv = __ldcg(part + b);
+    t.x += pv.x;
+    t.y += pv.y;
   }
   t = block_sum2(t);
   if (threadIdx.x == 0) {
@@ -98,43 +141,73 @@ __global__ void __launch_bounds__(kRedThreads) k_massflow(Dims d, Metric m, cons
     sc->qflow = q;
     if (mode == 1) {
       const double shift = q0 - t.x / t.y;
-      sc->shift = shift;
-      sc->dpdx_prev = sc->dPdx;
-      sc->dPdx = 0.5 * (sc->dpdx_prev + shift / dt);
+      if (comp == 0) {
+        sc->shift = shift;
+        sc->dpdx_prev = sc->dPdx;
+        sc->dPdx = 0.5 * (sc->dpdx_prev + shift / dt);
+      } else if (comp == 1) {
+        sc->shift_v = shift;
+        sc->dPdy = 0.5 * (sc->dPdy + shift / dt);
+      } else {
+        sc->shift_w = shift;
+        sc->dPdz = 0.5 * (sc->dPdz + shift / dt);
+      }
     }
     sc->ticket = 0u;
   }
 }
 
-// U(2:nx-1,2:nyg-1,2:nzg-1) += shift followed by the boundary conditions is,
-// entry for entry, U += shift on every copy of an interior value and
-// U -= shift on the odd y ghosts.  One warp per x-row of the whole array.
-__global__ void __launch_bounds__(256) k_shift_u(Dims d, double* __restrict__ U, const DevScalars* sc) {
-  const double s = sc->shift;
-  const int nrows = d.nyg * d.nzg;
+// F(interior) += shift followed by the boundary conditions is, entry for
+// entry, F += shift on every copy of an interior value, and on the y ghost
+// rows (j = 1, n2): -shift for the odd ghosts of U and W, nothing for the
+// zero wall values of V (face = 1).  One warp per x-row of the whole array.
+__global__ void __launch_bounds__(256) k_shift_field(double* __restrict__ F, int n1, int n2, int n3, int face,
+                                                    const double* __restrict__ shift) {
+  const double s = *shift;
+  const int nrows = n2 * n3;
   const int lane = threadIdx.x & 31;
   for (int row = blockIdx.x * 8 + (threadIdx.x >> 5); row < nrows; row += gridDim.x * 8) {
-    const int j = 1 + row % d.nyg;
-    const double sr = (j == 1 || j == d.nyg) ? -s : s;
-    double* u = U + (int64_t)row * d.nx;
-    for (int i = lane; i < d.nx; i += 32) u[i] += sr;
+    const int j = 1 + row % n2;
+    const bool wall = (j == 1 || j == n2);
+    if (face && wall) continue;
+    const double sr = wall ? -s : s;
+    double* f = F + (int64_t)row * n1;
+    for (int i = lane; i < n1; i += 32) f[i] += sr;
   }
 }
 
+static const double* flux_weight(Handle* h, int comp) {
+  if (!h->ib) return nullptr;
+  return comp == 0 ? ib_hu(h) : (comp == 1 ? ib_hv(h) : ib_hw(h));
+}
+
+// constant mass flow at the end of compute_time_step_RK3,
+// src/time_integration.f90:187-211: x, then y, then z, each only when enabled
 int launch_massflow_correction(Handle* h, double dt) {
-  // with an immersed body the flux is H-weighted (src/mass_flow.f90:160-163)
-  const double* Hu = h->ib ? ib_hu(h) : nullptr;
-  k_massflow<<<kRedBlocks, kRedThreads, 0, h->stream>>>(h->d, h->m, h->U, Hu, (double2*)h->red, h->sc,
-                                                        h->Qflow_x_0, dt, 1);
-  C3D_LAUNCH_CHECK(h);
-  k_shift_u<<<148 * 8, 256, 0, h->stream>>>(h->d, h->U, h->sc);
-  C3D_LAUNCH_CHECK(h);
+  const Dims& d = h->d;
+  const int on[3] = {h->p.x_mass_cte, h->p.y_mass_cte, h->p.z_mass_cte};
+  const double q0[3] = {h->Qflow_x_0, h->Qflow_y_0, h->Qflow_z_0};
+  double* F[3] = {h->U, h->V, h->W};
+  const int n1[3] = {d.nx, d.nxg, d.nxg}, n2[3] = {d.nyg, d.ny, d.nyg}, n3[3] = {d.nzg, d.nzg, d.nz};
+  const double* sh[3] = {&h->sc->shift, &h->sc->shift_v, &h->sc->shift_w};
+  for (int c = 0; c < 3; ++c) {
+    if (on[c] != 1) continue;
+    // with an immersed body the flux is H-weighted (src/mass_flow.f90:160-163)
+    const FluxView v = flux_view(h, c, F[c], flux_weight(h, c), true);
+    k_flux<<<kRedBlocks, kRedThreads, 0, h->stream>>>(v, (double2*)h->red, h->sc, q0[c], dt, 1, c);
+    C3D_LAUNCH_CHECK(h);
+    k_shift_field<<<148 * 8, 256, 0, h->stream>>>(F[c], n1[c], n2[c], n3[c], c == 1 ? 1 : 0, sh[c]);
+    C3D_LAUNCH_CHECK(h);
+  }
   return 0;
 }
 
-int massflow_u(Handle* h, const double* U, const double* Hu, double* q_out) {
-  k_massflow<<<kRedBlocks, kRedThreads, 0, h->stream>>>(h->d, h->m, U, Hu, (double2*)h->red, h->sc, 0.0,
-                                                        1.0, 0);
+// bulk flux of component comp (flux/norm) of the handle's field; u_view: the
+// mis-shaped view of the z correction (comp 2 only)
+int massflow(Handle* h, int comp, bool u_view, double* q_out) {
+  const double* F = comp == 0 ? h->U : (comp == 1 ? h->V : h->W);
+  const FluxView v = flux_view(h, comp, F, flux_weight(h, comp), u_view);
+  k_flux<<<kRedBlocks, kRedThreads, 0, h->stream>>>(v, (double2*)h->red, h->sc, 0.0, 1.0, 0, comp);
   C3D_LAUNCH_CHECK(h);
   double q = 0;
   C3D_CUDA_TRY(h, cudaMemcpyAsync(&q, &h->sc->qflow, sizeof(double), cudaMemcpyDeviceToHost, h->stream));

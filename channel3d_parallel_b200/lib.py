@@ -42,7 +42,8 @@ class Stats(C.Structure):
                 ("t", C.c_double), ("dt", C.c_double), ("qflow_x_0", C.c_double),
                 ("status", C.c_int32), ("precond_mode", C.c_int32),
                 ("last_bicgstab_ms", C.c_double), ("bicgstab_ms", C.c_double),
-                ("slab_cluster", C.c_int32 * 2), ("slab_narrow", C.c_int32 * 2)]
+                ("slab_cluster", C.c_int32 * 2), ("slab_narrow", C.c_int32 * 2),
+                ("qflow_y_0", C.c_double), ("qflow_z_0", C.c_double)]
 
 
 _D = C.POINTER(C.c_double)
@@ -66,6 +67,9 @@ PROTOTYPES = {
     "c3d_time_step_rk3": [_INT, _INT],
     "c3d_compute_dt": [_INT, _D],
     "c3d_compute_mean_mass_flow_u": [_INT, _D],
+    "c3d_compute_mean_mass_flow_v": [_INT, _D],
+    "c3d_compute_mean_mass_flow_w": [_INT, _D],
+    "c3d_set_flow_targets": [_INT, C.c_double, C.c_double, C.c_double],
     "c3d_compute_rhs_u": [_INT],
     "c3d_compute_rhs_v": [_INT],
     "c3d_compute_rhs_w": [_INT],
@@ -74,6 +78,8 @@ PROTOTYPES = {
     "c3d_compute_non_IB_projection": [_INT, _INT],
     "c3d_apply_boundary_conditions": [_INT, _INT],
     "c3d_compute_dPx_for_constant_mass_flow": [_INT, _D],
+    "c3d_compute_dPy_for_constant_mass_flow": [_INT, _D],
+    "c3d_compute_dPz_for_constant_mass_flow": [_INT, _D],
     "c3d_compute_pressure": [_INT],
     "c3d_setup_IB_geometry": [_INT],
     "c3d_setup_IB_operators": [_INT],

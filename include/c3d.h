@@ -108,6 +108,7 @@ typedef struct c3d_stats {
   double  bicgstab_ms;         /* accumulated device time of Schur solves     */
   int32_t slab_cluster[2];     /* CTAs per kx-slab cluster of the y-z solve: FP64, FP32 */
   int32_t slab_narrow[2];      /* 1: narrow slab CTAs (<= 192 threads, 3 per SM); FP64, FP32 */
+  double  qflow_y_0, qflow_z_0;/* targets of the y and z constant-flux corrections */
 } c3d_stats;
 
 /* ---- lifecycle ------------------------------------------------------------
@@ -147,6 +148,12 @@ int c3d_time_step_rk3(int handle, int nsteps);
 int c3d_compute_dt(int handle, double* dt);
 /* compute_mean_mass_flow_U with Hu, src/mass_flow.f90:24-53 (app/main.f90:90) */
 int c3d_compute_mean_mass_flow_u(int handle, double* qflow);
+/* compute_mean_mass_flow_V / _W, src/mass_flow.f90:62-129 (app/main.f90:91-92) */
+int c3d_compute_mean_mass_flow_v(int handle, double* qflow);
+int c3d_compute_mean_mass_flow_w(int handle, double* qflow);
+/* Qflow_x_0, Qflow_y_0, Qflow_z_0 (src/global.f90:180): the targets of the
+ * constant-flux corrections enabled by x/y/z_mass_cte                       */
+int c3d_set_flow_targets(int handle, double qflow_x_0, double qflow_y_0, double qflow_z_0);
 
 /* ---- fine entries mirroring the module interfaces ------------------------- */
 /* compute_rhs_u/v/w(U,V,W,rhs), src/equations.f90:24,160,295: reads the
@@ -166,6 +173,12 @@ int c3d_compute_non_IB_projection(int handle, int rk_step);
 int c3d_apply_boundary_conditions(int handle, int which);
 /* compute_dPx_for_constant_mass_flow(U, dPdx), src/mass_flow.f90:144-175 */
 int c3d_compute_dPx_for_constant_mass_flow(int handle, double* dPdx);
+/* compute_dPy_for_constant_mass_flow(V, dPdy), src/mass_flow.f90:190-221 */
+int c3d_compute_dPy_for_constant_mass_flow(int handle, double* dPdy);
+/* compute_dPz_for_constant_mass_flow(W, dPdz), src/mass_flow.f90:236-267; reads
+ * W through the routine's declared extents Dimension(nx,nyg,nzg) (:238), as the
+ * reference does                                                            */
+int c3d_compute_dPz_for_constant_mass_flow(int handle, double* dPdz);
 /* compute_pressure, src/pressure.f90:21-29 -- interface kept; the reference
  * never calls it (src/statistics.f90:37) and it returns C3D_ERR_UNSUPPORTED. */
 int c3d_compute_pressure(int handle);

@@ -497,6 +497,66 @@ def compute_dPx_for_constant_mass_flow(g, U, Qflow_x_0, Hu=None):
     return Qflow_x_0 - q / norm
 
 
+def mean_mass_flow_v(g, V, Hv=None):
+    """src/mass_flow.f90:62-91 (also the integral of :190-221): trapezoid of
+    H*V between y(1:ny) over i = 2..nxg-1, k = 2..nzg-1."""
+    nxg, ny, nzg, y = g.nxg, g.ny, g.nzg, g.y
+    if Hv is None:
+        Hv = np.ones_like(V)
+    I, K = slice(2, nxg), slice(2, nzg)
+    w = _row(0.5 * (y[2:ny + 1] - y[1:ny]))
+    HV = Hv[I, 1:ny + 1, K] * V[I, 1:ny + 1, K]
+    q = float(np.sum((HV[:, 1:] + HV[:, :-1]) * w))
+    H = Hv[I, 1:ny + 1, K]
+    norm = float(np.sum((H[:, 1:] + H[:, :-1]) * w))
+    return q, norm
+
+
+def mean_mass_flow_w(g, W, Hw=None):
+    """src/mass_flow.f90:100-129: trapezoid of H*W between yg(2:nyg-1) over
+    i = 2..nxg-1, k = 2..nz-1."""
+    nxg, nyg, nz, yg = g.nxg, g.nyg, g.nz, g.yg
+    if Hw is None:
+        Hw = np.ones_like(W)
+    I, K = slice(2, nxg), slice(2, nz)
+    w = _row(0.5 * (yg[3:nyg] - yg[2:nyg - 1]))
+    HW = Hw[I, 2:nyg, K] * W[I, 2:nyg, K]
+    q = float(np.sum((HW[:, 1:] + HW[:, :-1]) * w))
+    H = Hw[I, 2:nyg, K]
+    norm = float(np.sum((H[:, 1:] + H[:, :-1]) * w))
+    return q, norm
+
+
+def compute_dPy_for_constant_mass_flow(g, V, Qflow_y_0, Hv=None):
+    """src/mass_flow.f90:190-221: dPdy = Qflow_y_0 - Int_V/norm."""
+    q, norm = mean_mass_flow_v(g, V, Hv)
+    return Qflow_y_0 - q / norm
+
+
+def compute_dPz_for_constant_mass_flow(g, W, Qflow_z_0, Hw=None):
+    """src/mass_flow.f90:236-267: dPdz = Qflow_z_0 - Int_W/norm.
+
+    The routine declares its dummy W with the extents of U,
+    ``Dimension(nx,nyg,nzg)`` (:238), while the actual argument is W(nxg,nyg,nz):
+    its W(i,j,k) is the element at Fortran offset (i-1) + nx*((j-1) + nyg*(k-1))
+    of the real W.  That is what is read here (every offset the loops reach
+    lies inside W).  Hw_interior is the module array with its own extents."""
+    nx, nxg, nyg, nz, yg = g.nx, g.nxg, g.nyg, g.nz, g.yg
+    flat = np.asarray(W)[1:, 1:, 1:].ravel(order="F")
+    if Hw is None:
+        Hw = np.ones_like(W)
+    i = np.arange(2, nxg)[:, None, None]
+    j = np.arange(3, nyg)[None, :, None]
+    k = np.arange(2, nz)[None, None, :]
+    off = lambda ii, jj, kk: (ii - 1) + nx * ((jj - 1) + nyg * (kk - 1))
+    Wa, Wb = flat[off(i, j, k)], flat[off(i, j - 1, k)]
+    Ha, Hb = Hw[2:nxg, 3:nyg, 2:nz], Hw[2:nxg, 2:nyg - 1, 2:nz]
+    w = _row(0.5 * (yg[3:nyg] - yg[2:nyg - 1]))
+    q = float(np.sum((Ha * Wa + Hb * Wb) * w))
+    norm = float(np.sum((Ha + Hb) * w))
+    return Qflow_z_0 - q / norm
+
+
 # --------------------------------------------------------------------------
 # full state and the RK3 step
 # --------------------------------------------------------------------------
@@ -511,6 +571,8 @@ class State:
         self.dPdy = 0.0
         self.dPdz = 0.0
         self.Qflow_x_0 = 0.0
+        self.Qflow_y_0 = 0.0
+        self.Qflow_z_0 = 0.0
 
     def copy(self):
         s = State.__new__(State)
@@ -576,6 +638,18 @@ def compute_time_step_RK3(g, st, dt):
         shift = compute_dPx_for_constant_mass_flow(g, st.U, st.Qflow_x_0)
         st.U[Iu, Ju, Ku] = st.U[Iu, Ju, Ku] + shift
         st.dPdx = 0.5 * (dPdx_prev + shift / dt)
+        apply_boundary_conditions(g, st.U, st.V, st.W)
+    if p.get("y_mass_cte", 0) == 1:                      # :196-202
+        dPdy_prev = st.dPdy
+        shift = compute_dPy_for_constant_mass_flow(g, st.V, st.Qflow_y_0)
+        st.V[Iv, Jv, Kv] = st.V[Iv, Jv, Kv] + shift
+        st.dPdy = 0.5 * (dPdy_prev + shift / dt)
+        apply_boundary_conditions(g, st.U, st.V, st.W)
+    if p.get("z_mass_cte", 0) == 1:                      # :205-211
+        dPdz_prev = st.dPdz
+        shift = compute_dPz_for_constant_mass_flow(g, st.W, st.Qflow_z_0)
+        st.W[Iw, Jw, Kw] = st.W[Iw, Jw, Kw] + shift
+        st.dPdz = 0.5 * (dPdz_prev + shift / dt)
         apply_boundary_conditions(g, st.U, st.V, st.W)
     return st
 
@@ -643,6 +717,10 @@ def seeded_initial_state(g, dPdx, amplitude=0.1, seed=0, project=True, dt=1e-3):
         st.P_interim[...] = 0.0
     q, norm = mean_mass_flow_u(g, st.U)
     st.Qflow_x_0 = q / norm
+    q, norm = mean_mass_flow_v(g, st.V)                  # app/main.f90:91-92
+    st.Qflow_y_0 = q / norm
+    q, norm = mean_mass_flow_w(g, st.W)
+    st.Qflow_z_0 = q / norm
     return st
 
 

@@ -246,3 +246,62 @@ def test_handles_of_different_sizes_coexist():
             assert small.check_divergence() < 1e-12
         finally:
             small.close()
+
+
+def make_flux_pair(case):
+    """A pair with the y and z constant-flux corrections enabled."""
+    import channel3d_parallel_b200 as c3d
+    nx, ny, nz, lx, lz, gt = CASES[case]
+    nu = 1.0 / 5600.0
+    p = co.channel_params(nx, ny, nz, lx, lz, nu, grid_type=gt, y_mass_cte=1, z_mass_cte=1)
+    g = co.Grid(p)
+    st = co.seeded_initial_state(g, p["dpdx"])
+    ch = c3d.Channel(nx_global=nx, ny_global=ny, nz_global=nz, Lxp=lx, Lzp=lz, nu=nu,
+                     CFL=-1e-3, x_mass_cte=1, y_mass_cte=1, z_mass_cte=1, grid_type=gt,
+                     alpha_stretch=2.0, dPdx=p["dpdx"])
+    ch.set_grid(g.x[1:], g.y[1:], g.z[1:])
+    for name in ("U", "V", "W"):
+        ch.upload(name, getattr(st, name)[1:, 1:, 1:])
+    ch.set_scalars(dPdx=st.dPdx, t=0.0, Qflow_x_0=st.Qflow_x_0)
+    ch.set_flow_targets(st.Qflow_x_0, st.Qflow_y_0, st.Qflow_z_0)
+    return g, st, ch
+
+
+@pytest.mark.parametrize("case", ["cfg0_34x65x34", "odd_ny_radix3", "uniform_small"])
+def test_flux_entries_y_z(case):
+    """compute_mean_mass_flow_V/W and compute_dPy/dPz (the latter through the
+    routine's declared W extents) against the oracle."""
+    g, st, ch = make_flux_pair(case)
+    try:
+        q, n = co.mean_mass_flow_v(g, st.V)
+        assert abs(ch.compute_mean_mass_flow_V() - q / n) < 1e-15
+        q, n = co.mean_mass_flow_w(g, st.W)
+        assert abs(ch.compute_mean_mass_flow_W() - q / n) < 1e-15
+        assert abs(ch.compute_dPy_for_constant_mass_flow()
+                   - co.compute_dPy_for_constant_mass_flow(g, st.V, st.Qflow_y_0)) < 1e-15
+        assert abs(ch.compute_dPz_for_constant_mass_flow()
+                   - co.compute_dPz_for_constant_mass_flow(g, st.W, st.Qflow_z_0)) < 1e-15
+    finally:
+        ch.close()
+
+
+@pytest.mark.parametrize("case", ["cfg0_34x65x34", "uniform_small"])
+@pytest.mark.parametrize("nsteps", [1, 10])
+def test_rk3_steps_with_y_and_z_flux_corrections(case, nsteps):
+    """x, y and z constant-flux corrections (src/time_integration.f90:187-211)."""
+    g, st, ch = make_flux_pair(case)
+    try:
+        ch.compute_time_step_RK3(nsteps)
+        for _ in range(nsteps):
+            co.compute_time_step_RK3(g, st, 1e-3)
+        errs = {name: rel(ch.download(name), ref[1:, 1:, 1:])
+                for name, ref in (("U", st.U), ("V", st.V), ("W", st.W))}
+        assert max(errs.values()) < 1e-10, errs
+        s = ch.stats()
+        tol = lambda ref, q: 1e-9 * abs(ref) + 50 * 2.2e-16 * max(abs(q), 1.0) / 1e-3
+        assert abs(s["dPdx"] - st.dPdx) <= tol(st.dPdx, st.Qflow_x_0)
+        assert abs(s["dPdy"] - st.dPdy) <= tol(st.dPdy, st.Qflow_y_0)
+        assert abs(s["dPdz"] - st.dPdz) <= tol(st.dPdz, st.Qflow_z_0)
+        assert abs(s["qflow_y_0"] - st.Qflow_y_0) == 0.0
+    finally:
+        ch.close()
