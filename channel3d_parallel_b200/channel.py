@@ -169,6 +169,10 @@ class Channel:
         """compute_dt + compute_time_step_RK3 (src/time_integration.f90:86-267)."""
         return self._check(self._lib.c3d_time_step_rk3(self.handle, int(nsteps)))
 
+    def compute_time_step_Euler(self, nsteps=1):
+        """compute_dt + compute_time_step_Euler (src/time_integration.f90:25-81)."""
+        return self._check(self._lib.c3d_time_step_euler(self.handle, int(nsteps)))
+
     def compute_dt(self):
         dt = C.c_double(0.0)
         self._check(self._lib.c3d_compute_dt(self.handle, C.byref(dt)))

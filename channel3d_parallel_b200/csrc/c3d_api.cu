@@ -486,7 +486,21 @@ static int enqueue_step(Handle* h, double dt, double to) {
   return warn;
 }
 
-static int run_steps(Handle* h, int nsteps) {
+// one explicit Euler step, src/time_integration.f90:25-81: rk_step = 3 (no
+// P side effect), the non-IB projection only (the reference's Euler never
+// calls the IB projection), x and y constant-flux corrections
+static int enqueue_euler_step(Handle* h, double dt) {
+  int rc;
+  if ((rc = launch_rhs_euler(h, dt))) return rc;                // :34-52
+  if ((rc = launch_fill_ghosts3(h, h->Us, h->Vs, h->Ws))) return rc;
+  if ((rc = launch_projection_step(h, 3, dt))) return rc;       // :58-61
+  if (h->p.x_mass_cte == 1 || h->p.y_mass_cte == 1) {           // :65-78
+    if ((rc = launch_massflow_correction(h, dt, true))) return rc;
+  }
+  return 0;
+}
+
+static int run_steps(Handle* h, int nsteps, bool euler = false) {
   int rc, warn = 0;
   C3D_CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
   for (int n = 0; n < nsteps; ++n) {
@@ -494,6 +508,12 @@ static int run_steps(Handle* h, int nsteps) {
     if ((rc = compute_dt_cfl(h, &dt))) return rc;   // compute_dt, app/main.f90:105
     h->dt = dt;
     const double to = h->t;
+    if (euler) {
+      if ((rc = enqueue_euler_step(h, dt))) return rc;
+      h->t = to + dt;
+      h->stats.steps++;
+      continue;
+    }
     const bool graphable = h->use_graph && h->ib == nullptr;
     if (graphable) {
       if (h->step_exec == nullptr || h->graph_dt != dt) {
@@ -677,6 +697,12 @@ int c3d_time_step_rk3(int id, int nsteps) {
   RET(h, run_steps(h, nsteps));
 }
 
+int c3d_time_step_euler(int id, int nsteps) {
+  GET_HANDLE(id);
+  if (nsteps < 0) return C3D_ERR_PARAM;
+  RET(h, run_steps(h, nsteps, true));
+}
+
 int c3d_compute_dt(int id, double* dt) {
   GET_HANDLE(id);
   if (!dt) return C3D_ERR_PARAM;
@@ -794,9 +820,7 @@ int c3d_compute_dPz_for_constant_mass_flow(int id, double* dPdz) {
 
 int c3d_compute_pressure(int id) {
   GET_HANDLE(id);
-  h->last_error = "compute_pressure is not on the time-step path (its call sites are commented out "
-                  "in the reference); not provided";
-  RET(h, C3D_ERR_UNSUPPORTED);
+  RET(h, compute_pressure(h));
 }
 
 int c3d_set_mode(int id, int poisson_mode, int precond_mode) {

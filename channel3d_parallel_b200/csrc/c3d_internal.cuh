@@ -158,6 +158,7 @@ struct Handle {
   Metric m{};
   double *U = nullptr, *V = nullptr, *W = nullptr, *P = nullptr;
   double *Us = nullptr, *Vs = nullptr, *Ws = nullptr;       // star / work fields
+  double* pbc = nullptr;          // compute_pressure wall conditions bc_1, bc_2 (2 x nxg x nzg)
   double *Gu = nullptr, *Gv = nullptr, *Gw = nullptr;       // RK accumulators
   double *rhs_p = nullptr;                                  // rhs_p / phi
   double *P_interim = nullptr;
@@ -231,6 +232,7 @@ int launch_fill_ghosts3(Handle* h, double* U, double* V, double* W);
 // rhs (k_rhs.cu)
 int rhs_setup(Handle* h);
 int launch_rhs_stage(Handle* h, int stage, double dt);
+int launch_rhs_euler(Handle* h, double dt);
 int launch_rhs_only(Handle* h, int component);
 // poisson + projection (k_poisson.cu)
 int poisson_setup(Handle* h);
@@ -244,11 +246,12 @@ int launch_projection_step(Handle* h, int rk_step, double dt);
 int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, const double* Wi,
                              const double* phi, double dt, double* Uo, double* Vo, double* Wo);
 int rebuild_pressure(Handle* h);
+int compute_pressure(Handle* h);
 int profile_spectral(Handle* h, int part);   // 0 div_xfft, 1 spectral_yz, 2 xfft inv
 int mixed_setup(Handle* h);
 void mixed_free(Handle* h);
 // mass flow and reductions (k_massflow.cu)
-int launch_massflow_correction(Handle* h, double dt);
+int launch_massflow_correction(Handle* h, double dt, bool euler = false);
 int massflow(Handle* h, int comp, bool u_view, double* q_out);
 int max_abs_divergence(Handle* h, const double* U, const double* V, const double* W, double* out);
 int check_finite(Handle* h, bool* ok);

@@ -93,7 +93,9 @@ static FluxView flux_view(Handle* h, int comp, const double* F, const double* H,
 // DevScalars) adds the partials in block order and
 //   mode 0: stores qflow = flux/norm;
 //   mode 1: also the constant-flux correction of component comp
-//           (shift = q0 - flux/norm) and dPd{x,y,z} = (dPd_prev + shift/dt)/2.
+//           (shift = q0 - flux/norm) and dPd{x,y,z} = (dPd_prev + shift/dt)/2
+//           (RK3, src/time_integration.f90:187-211);
+//   mode 2: the same with dPd{x,y} = shift/dt (Euler, :65-78).
 __global__ void __launch_bounds__(kRedThreads) k_flux(FluxView v, double2* __restrict__ part, DevScalars* sc,
                                                      double q0, double dt, int mode, int comp) {
   const int nrows = v.nj * v.nk;
@@ -139,19 +141,18 @@ __global__ void __launch_bounds__(kRedThreads) k_flux(FluxView v, double2* __res
   if (threadIdx.x == 0) {
     const double q = t.x / t.y;
     sc->qflow = q;
-    if (mode == 1) {
+    if (mode >= 1) {
       const double shift = q0 - t.x / t.y;
+      double* dp = comp == 0 ? &sc->dPdx : (comp == 1 ? &sc->dPdy : &sc->dPdz);
       if (comp == 0) {
         sc->shift = shift;
         sc->dpdx_prev = sc->dPdx;
-        sc->dPdx = 0.5 * (sc->dpdx_prev + shift / dt);
       } else if (comp == 1) {
         sc->shift_v = shift;
-        sc->dPdy = 0.5 * (sc->dPdy + shift / dt);
       } else {
         sc->shift_w = shift;
-        sc->dPdz = 0.5 * (sc->dPdz + shift / dt);
       }
+      *dp = mode == 1 ? 0.5 * (*dp + shift / dt) : shift / dt;
     }
     sc->ticket = 0u;
   }
@@ -182,10 +183,12 @@ static const double* flux_weight(Handle* h, int comp) {
 }
 
 // constant mass flow at the end of compute_time_step_RK3,
-// src/time_integration.f90:187-211: x, then y, then z, each only when enabled
-int launch_massflow_correction(Handle* h, double dt) {
+// src/time_integration.f90:187-211: x, then y, then z, each only when
+// enabled; euler: that of compute_time_step_Euler (:65-78, x and y only,
+// dPd = shift/dt)
+int launch_massflow_correction(Handle* h, double dt, bool euler) {
   const Dims& d = h->d;
-  const int on[3] = {h->p.x_mass_cte, h->p.y_mass_cte, h->p.z_mass_cte};
+  const int on[3] = {h->p.x_mass_cte, h->p.y_mass_cte, euler ? 0 : h->p.z_mass_cte};
   const double q0[3] = {h->Qflow_x_0, h->Qflow_y_0, h->Qflow_z_0};
   double* F[3] = {h->U, h->V, h->W};
   const int n1[3] = {d.nx, d.nxg, d.nxg}, n2[3] = {d.nyg, d.ny, d.nyg}, n3[3] = {d.nzg, d.nzg, d.nz};
@@ -194,7 +197,7 @@ int launch_massflow_correction(Handle* h, double dt) {
     if (on[c] != 1) continue;
     // with an immersed body the flux is H-weighted (src/mass_flow.f90:160-163)
     const FluxView v = flux_view(h, c, F[c], flux_weight(h, c), true);
-    k_flux<<<kRedBlocks, kRedThreads, 0, h->stream>>>(v, (double2*)h->red, h->sc, q0[c], dt, 1, c);
+    k_flux<<<kRedBlocks, kRedThreads, 0, h->stream>>>(v, (double2*)h->red, h->sc, q0[c], dt, euler ? 2 : 1, c);
     C3D_LAUNCH_CHECK(h);
     k_shift_field<<<148 * 8, 256, 0, h->stream>>>(F[c], n1[c], n2[c], n3[c], c == 1 ? 1 : 0, sh[c]);
     C3D_LAUNCH_CHECK(h);

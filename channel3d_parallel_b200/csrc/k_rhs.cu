@@ -403,6 +403,24 @@ int launch_rhs_stage(Handle* h, int stage, double dt) {
   return 0;
 }
 
+// compute_time_step_Euler (src/time_integration.f90:34-52): U* = U + dt*F
+// for the three components (the stage-1 kernel with its accumulator output
+// sent to the G work fields, which Euler does not read)
+int launch_rhs_euler(Handle* h, double dt) {
+  RhsArgs a = base_args(h);
+  a.Us = h->Us; a.Vs = h->Vs; a.Ws = h->Ws;
+  a.Gu_out = h->Gu; a.Gv_out = h->Gv; a.Gw_out = h->Gw;
+  a.cs = dt;
+  a.cg = dt;
+  const Dims& d = h->d;
+  const dim3 tb(TX, TY, 1);
+  const dim3 tg((d.Nx + TX - 1) / TX, (d.Ny + TY - 1) / TY, (d.Nz + KC - 1) / KC);
+  if (h->rhs_kernel == 0) k_rhs_tiled<1><<<tg, tb, kRhsSmem, h->stream>>>(a);
+  else k_rhs<1><<<rhs_grid(d), rhs_block(), 0, h->stream>>>(a);
+  C3D_LAUNCH_CHECK(h);
+  return 0;
+}
+
 // fine entries: component 1/2/3 -> rhsU/rhsV/rhsW
 int launch_rhs_only(Handle* h, int component) {
   RhsArgs a = base_args(h);

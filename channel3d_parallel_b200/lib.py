@@ -65,6 +65,7 @@ PROTOTYPES = {
     "c3d_set_scalars": [_INT, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double],
     "c3d_synchronize": [_INT],
     "c3d_time_step_rk3": [_INT, _INT],
+    "c3d_time_step_euler": [_INT, _INT],
     "c3d_compute_dt": [_INT, _D],
     "c3d_compute_mean_mass_flow_u": [_INT, _D],
     "c3d_compute_mean_mass_flow_v": [_INT, _D],

@@ -144,6 +144,10 @@ int c3d_synchronize(int handle);
 /* compute_time_step_RK3, src/time_integration.f90:86-213; nsteps steps, each
  * preceded by compute_dt (src/time_integration.f90:219-267).               */
 int c3d_time_step_rk3(int handle, int nsteps);
+/* compute_time_step_Euler, src/time_integration.f90:25-81 (explicit Euler,
+ * non-IB projection, x and y constant-flux corrections); nsteps steps, each
+ * preceded by compute_dt.                                                   */
+int c3d_time_step_euler(int handle, int nsteps);
 /* compute_dt, src/time_integration.f90:219-267 */
 int c3d_compute_dt(int handle, double* dt);
 /* compute_mean_mass_flow_U with Hu, src/mass_flow.f90:24-53 (app/main.f90:90) */
@@ -179,8 +183,10 @@ int c3d_compute_dPy_for_constant_mass_flow(int handle, double* dPdy);
  * W through the routine's declared extents Dimension(nx,nyg,nzg) (:238), as the
  * reference does                                                            */
 int c3d_compute_dPz_for_constant_mass_flow(int handle, double* dPdz);
-/* compute_pressure, src/pressure.f90:21-29 -- interface kept; the reference
- * never calls it (src/statistics.f90:37) and it returns C3D_ERR_UNSUPPORTED. */
+/* compute_pressure, src/pressure.f90:21-341: the actual pressure into P
+ * (wall conditions d/dy(nu dV/dy), divergence of the right-hand sides, the
+ * Poisson solve with inhomogeneous Neumann rows); the reference's call sites
+ * are commented out (src/statistics.f90:37, src/input_output.f90:508).       */
 int c3d_compute_pressure(int handle);
 
 /* ---- immersed boundary ---------------------------------------------------- */

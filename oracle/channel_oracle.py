@@ -475,6 +475,111 @@ def _pressure_side_effect(g, st, rhs, dt):
 
 
 # --------------------------------------------------------------------------
+# actual pressure, src/pressure.f90:21-341
+# --------------------------------------------------------------------------
+def compute_pressure_bc(g, V):
+    """src/pressure.f90:270-341: bc_1, bc_2 = d/dy(nu dV/dy) at the walls by
+    one-sided second-order differences in the grid index (dzeta = 1), as
+    arrays over (i, k) = (2..nxg-1, 2..nzg-1) (shape (nxg+1, nzg+1), Fortran
+    indexed)."""
+    y, ny, nxg, nzg, nu = g.y, g.ny, g.nxg, g.nzg, g.p["nu"]
+    dzeta = 1.0
+    bc1 = np.zeros((nxg + 1, nzg + 1))
+    bc2 = np.zeros((nxg + 1, nzg + 1))
+    I, K = slice(2, nxg), slice(2, nzg)
+    gm = (-3.0 * y[1] + 4.0 * y[2] - y[3]) / (2.0 * dzeta)
+    g2 = (2.0 * y[1] - 5.0 * y[2] + 4.0 * y[3] - 1.0 * y[4]) / dzeta ** 2.0
+    dV = (-3.0 * V[I, 1, K] + 4.0 * V[I, 2, K] - V[I, 3, K]) / (2.0 * dzeta) * 1.0 / gm
+    ddV = (2.0 * V[I, 1, K] - 5.0 * V[I, 2, K] + 4.0 * V[I, 3, K] - 1.0 * V[I, 4, K]) / dzeta ** 2.0
+    ddV = (ddV - dV * g2) / gm ** 2.0
+    bc1[I, K] = 0.0 * dV + nu * ddV
+    gm = (3.0 * y[ny] - 4.0 * y[ny - 1] + y[ny - 2]) / (2.0 * dzeta)
+    g2 = (2.0 * y[ny] - 5.0 * y[ny - 1] + 4.0 * y[ny - 2] - 1.0 * y[ny - 3]) / dzeta ** 2.0
+    dV = (3.0 * V[I, ny, K] - 4.0 * V[I, ny - 1, K] + V[I, ny - 2, K]) / (2.0 * dzeta) * 1.0 / gm
+    ddV = (2.0 * V[I, ny, K] - 5.0 * V[I, ny - 1, K] + 4.0 * V[I, ny - 2, K]
+           - 1.0 * V[I, ny - 3, K]) / dzeta ** 2.0
+    ddV = (ddV - dV * g2) / gm ** 2.0
+    bc2[I, K] = 0.0 * dV + nu * ddV
+    return bc1, bc2
+
+
+def compute_pressure_rhs(g, st, bc1, bc2, Hu=None, Hv=None, Hw=None):
+    """src/pressure.f90:42-70: rhs_p = div(rhs_uf, rhs_vf, rhs_wf) with the
+    periodic copies of rhs_uf in x and rhs_wf in z and bc_1/bc_2 as the wall
+    values of rhs_vf."""
+    nx, ny, nz, nxg, nyg, nzg = g.nx, g.ny, g.nz, g.nxg, g.nyg, g.nzg
+    epg = g.p["exterior_pressure_gradient"]
+    ruf, rvf, rwf = g.u_array(), g.v_array(), g.w_array()
+    ruf[2:nx, 2:nyg, 2:nzg] = compute_rhs_u(g, st.U, st.V, st.W, st.dPdx, Hu, epg)
+    rvf[2:nxg, 2:ny, 2:nzg] = compute_rhs_v(g, st.U, st.V, st.W, st.dPdy, Hv, epg)
+    rwf[2:nxg, 2:nyg, 2:nz] = compute_rhs_w(g, st.U, st.V, st.W, st.dPdz, Hw, epg)
+    apply_periodic_bc_x(g, ruf, True)                  # compute_rhs_v_boundary (:237-247)
+    rvf[2:nxg, 1, 2:nzg] = bc1[2:nxg, 2:nzg]
+    rvf[2:nxg, ny, 2:nzg] = bc2[2:nxg, 2:nzg]
+    apply_periodic_bc_z(g, rwf, True)
+    x, y, z = g.x, g.y, g.z
+    rhs = g.rhs_p_array()
+    I, J, K = slice(2, nxg), slice(2, nyg), slice(2, nzg)
+    rhs[I, J, K] = ((ruf[I, J, K] - ruf[1:nxg - 1, J, K]) / _col(x[2:nxg] - x[1:nxg - 1])
+                    + (rvf[I, J, K] - rvf[I, 1:nyg - 1, K]) / _row(y[2:nyg] - y[1:nyg - 1])
+                    + (rwf[I, J, K] - rwf[I, J, 1:nzg - 1]) / _dep(z[2:nzg] - z[1:nzg - 1]))
+    return rhs
+
+
+def solve_poisson_equation_for_pressure(g, rhs, bc1, bc2, P):
+    """src/pressure.f90:90-165: the Poisson solve of the projection with the
+    inhomogeneous Neumann rows (coef_bc_1, coef_bc_2 of
+    src/initialization.f90:374,383), then P(2:nxg-2, 2:nyg-1, 2:nzg-2), its
+    y ghosts P(1) = P(2) - (yg(2)-yg(1)) bc_1 and P(nyg) = P(nyg-1) +
+    (yg(nyg)-yg(nyg-1)) bc_2, and the periodic copies (:173-187).
+
+    The y-ghost assignment of the reference (:160-161) takes a whole (nxg, nzg)
+    section of P from bc_1, which is allocated (2:nxg-1, 2:nzg-1)
+    (src/initialization.f90:385): the shapes do not conform.  It is applied
+    here over bc_1's domain (i, k) = (2..nxg-1, 2..nzg-1); the x and z ghost
+    planes of P (i = 1, nxg; k = 1, nzg) keep their values."""
+    nxp, nzp, nyg, nxg, nzg = g.nxp, g.nzp, g.nyg, g.nxg, g.nzg
+    y, yg = g.y, g.yg
+    J = slice(2, nyg)
+    hat = np.fft.fft2(rhs[2:nxp + 2, J, 2:nzp + 2], axes=(0, 2))
+    b1 = np.fft.fft2(bc1[2:nxp + 2, 2:nzp + 2])
+    b2 = np.fft.fft2(bc2[2:nxp + 2, 2:nzp + 2])
+    j = 2
+    coef_bc_1 = 1.0 / (y[j] - y[j - 1]) / (yg[j] - yg[j - 1])
+    j = nyg - 1
+    coef_bc_2 = 1.0 / (y[j] - y[j - 1]) / (yg[j + 1] - yg[j])
+    dd, dl, du = g.Dd[2:nyg], g.Dl[3:nyg], g.Du[2:nyg - 1]
+    for i in range(nxp):
+        ia = min(i, nxp - i)
+        for k in range(nzp):
+            ka = min(k, nzp - k)
+            D = (dd + g.kxx[ia]) + g.kzz[ka]
+            if i == 0 and k == 0:
+                D = D.copy()
+                D[0] = 3.0 / 2.0 * D[0]
+            r = hat[i, :, k].copy()
+            r[0] = r[0] + coef_bc_1 * (yg[2] - yg[1]) * b1[i, k]
+            r[-1] = r[-1] - coef_bc_2 * (yg[nyg] - yg[nyg - 1]) * b2[i, k]
+            hat[i, :, k] = _zgtsv(dl, D, du, r.reshape(-1, 1))[:, 0]
+    out = np.fft.ifft2(hat, axes=(0, 2))
+    P[2:nxp + 2, J, 2:nzp + 2] = out.real
+    I, K = slice(2, nxg), slice(2, nzg)
+    P[I, 1, K] = P[I, 2, K] - (yg[2] - yg[1]) * bc1[I, K]
+    P[I, nyg, K] = P[I, nyg - 1, K] + (yg[nyg] - yg[nyg - 1]) * bc2[I, K]
+    P[nxg - 1, :, :] = P[2, :, :]                      # apply_periodic_xz_pressure
+    P[2:nxg, :, nzp + 2] = P[2:nxg, :, 2]
+    return P
+
+
+def compute_pressure(g, st, Hu=None, Hv=None, Hw=None):
+    """src/pressure.f90:21-29 on st.P (in place)."""
+    bc1, bc2 = compute_pressure_bc(g, st.V)
+    rhs = compute_pressure_rhs(g, st, bc1, bc2, Hu, Hv, Hw)
+    solve_poisson_equation_for_pressure(g, rhs, bc1, bc2, st.P)
+    return st.P
+
+
+# --------------------------------------------------------------------------
 # mass flow, src/mass_flow.f90
 # --------------------------------------------------------------------------
 def mean_mass_flow_u(g, U, Hu=None):
@@ -650,6 +755,37 @@ def compute_time_step_RK3(g, st, dt):
         shift = compute_dPz_for_constant_mass_flow(g, st.W, st.Qflow_z_0)
         st.W[Iw, Jw, Kw] = st.W[Iw, Jw, Kw] + shift
         st.dPdz = 0.5 * (dPdz_prev + shift / dt)
+        apply_boundary_conditions(g, st.U, st.V, st.W)
+    return st
+
+
+def compute_time_step_Euler(g, st, dt, Hu=None, Hv=None, Hw=None):
+    """src/time_integration.f90:25-81: explicit Euler with rk_step = 3 (no P
+    side effect), the non-IB projection, and the x and y constant-flux
+    corrections with dPd = shift/dt (no averaging; no z correction)."""
+    p = g.p
+    nx, ny, nz, nxg, nyg, nzg = g.nx, g.ny, g.nz, g.nxg, g.nyg, g.nzg
+    Uo, Vo, Wo = st.U.copy(), st.V.copy(), st.W.copy()
+    epg = p["exterior_pressure_gradient"]
+    ru = compute_rhs_u(g, Uo, Vo, Wo, st.dPdx, Hu, epg)
+    st.U[2:nx, 2:nyg, 2:nzg] = Uo[2:nx, 2:nyg, 2:nzg] + dt * ru
+    rv = compute_rhs_v(g, Uo, Vo, Wo, st.dPdy, Hv, epg)
+    st.V[2:nxg, 2:ny, 2:nzg] = Vo[2:nxg, 2:ny, 2:nzg] + dt * rv
+    rw = compute_rhs_w(g, Uo, Vo, Wo, st.dPdz, Hw, epg)
+    st.W[2:nxg, 2:nyg, 2:nz] = Wo[2:nxg, 2:nyg, 2:nz] + dt * rw
+    st.t = st.t + dt
+    apply_boundary_conditions(g, st.U, st.V, st.W)
+    compute_non_IB_projection(g, st, dt, rk_step=3)
+    apply_boundary_conditions(g, st.U, st.V, st.W)
+    if p["x_mass_cte"] == 1:                             # :65-70
+        shift = compute_dPx_for_constant_mass_flow(g, st.U, st.Qflow_x_0, Hu)
+        st.U[2:nx, 2:nyg, 2:nzg] = st.U[2:nx, 2:nyg, 2:nzg] + shift
+        st.dPdx = shift / dt
+        apply_boundary_conditions(g, st.U, st.V, st.W)
+    if p.get("y_mass_cte", 0) == 1:                      # :73-78 (walls included)
+        shift = compute_dPy_for_constant_mass_flow(g, st.V, st.Qflow_y_0, Hv)
+        st.V[2:nxg, 1:ny + 1, 2:nzg] = st.V[2:nxg, 1:ny + 1, 2:nzg] + shift
+        st.dPdy = shift / dt
         apply_boundary_conditions(g, st.U, st.V, st.W)
     return st
 

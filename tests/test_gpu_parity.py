@@ -305,3 +305,56 @@ def test_rk3_steps_with_y_and_z_flux_corrections(case, nsteps):
         assert abs(s["qflow_y_0"] - st.Qflow_y_0) == 0.0
     finally:
         ch.close()
+
+
+@pytest.mark.parametrize("case", ["cfg0_34x65x34", "odd_ny_radix3", "uniform_small"])
+@pytest.mark.parametrize("nsteps", [1, 10])
+def test_euler_steps(case, nsteps):
+    """compute_time_step_Euler (src/time_integration.f90:25-81)."""
+    p, g, st, ch = make_pair(case)
+    try:
+        ch.compute_time_step_Euler(nsteps)
+        for _ in range(nsteps):
+            co.compute_time_step_Euler(g, st, 1e-3)
+        errs = {name: rel(ch.download(name), ref[1:, 1:, 1:])
+                for name, ref in (("U", st.U), ("V", st.V), ("W", st.W))}
+        assert max(errs.values()) < 1e-10, errs
+        s = ch.stats()
+        assert abs(s["dPdx"] - st.dPdx) <= 1e-9 * abs(st.dPdx) + 50 * 2.2e-16 * abs(st.Qflow_x_0) / 1e-3
+        assert abs(s["t"] - st.t) < 1e-15
+        assert ch.check_divergence() < 1e-12
+    finally:
+        ch.close()
+
+
+def test_euler_steps_with_y_flux_correction():
+    g, st, ch = make_flux_pair("cfg0_34x65x34")
+    try:
+        ch.compute_time_step_Euler(3)
+        for _ in range(3):
+            co.compute_time_step_Euler(g, st, 1e-3)
+        errs = {name: rel(ch.download(name), ref[1:, 1:, 1:])
+                for name, ref in (("U", st.U), ("V", st.V), ("W", st.W))}
+        assert max(errs.values()) < 1e-10, errs
+        s = ch.stats()
+        assert abs(s["dPdy"] - st.dPdy) <= 1e-9 * abs(st.dPdy) + 50 * 2.2e-16 / 1e-3
+        # Euler has no z correction: dPdz stays at its initial value
+        assert s["dPdz"] == st.dPdz
+    finally:
+        ch.close()
+
+
+@pytest.mark.parametrize("case", ["cfg0_34x65x34", "odd_ny_radix3", "uniform_small", "nz256_wide_slab"])
+def test_compute_pressure(case):
+    """compute_pressure (src/pressure.f90:21-341) after two RK3 steps: the whole
+    P array (solution, wall ghosts, periodic copies, untouched x/z ghost planes)."""
+    p, g, st, ch = make_pair(case)
+    try:
+        ch.compute_time_step_RK3(2)
+        for _ in range(2):
+            co.compute_time_step_RK3(g, st, 1e-3)
+        ch.compute_pressure()
+        co.compute_pressure(g, st)
+        assert rel(ch.download("P"), st.P[1:, 1:, 1:]) < 1e-10
+    finally:
+        ch.close()

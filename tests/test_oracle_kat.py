@@ -139,3 +139,37 @@ def test_thomas_matches_zgtsv_to_roundoff():
         for j in range(len(D) - 2, -1, -1):
             bb[j] = (bb[j] - du[j] * bb[j + 1]) / dm[j]
         assert np.abs(bb - x1).max() / np.abs(x1).max() < 1e-11
+
+
+def test_pressure_solves_the_inhomogeneous_neumann_problem():
+    """compute_pressure (src/pressure.f90): the 3-point Laplacian of P, with the
+    y ghosts P(1) = P(2) - dy*bc_1 and P(nyg) = P(nyg-1) + dy*bc_2, equals the
+    divergence of the right-hand sides in every (x, z) Fourier mode except the
+    pinned mean (whose row 2 carries the factor 3/2)."""
+    import math
+    p = co.channel_params(34, 33, 26, math.pi, 1.0, 1 / 5600)
+    g = co.Grid(p)
+    st = co.seeded_initial_state(g, p["dpdx"])
+    co.compute_time_step_RK3(g, st, 1e-3)
+    bc1, bc2 = co.compute_pressure_bc(g, st.V)
+    rhs = co.compute_pressure_rhs(g, st, bc1, bc2)
+    P = co.compute_pressure(g, st).copy()
+    nxp, nzp, nyg = g.nxp, g.nzp, g.nyg
+    Pi = P[2:nxp + 2, :, 2:nzp + 2]                  # periodic interior, all j
+    lap_xz = ((np.roll(Pi, -1, 0) - 2 * Pi + np.roll(Pi, 1, 0)) / g.dx ** 2
+              + (np.roll(Pi, -1, 2) - 2 * Pi + np.roll(Pi, 1, 2)) / g.dz ** 2)
+    y, yg = g.y, g.yg
+    res = np.zeros((nxp, nyg - 2, nzp))
+    for j in range(2, nyg):
+        a = 1.0 / (y[j] - y[j - 1]) / (yg[j + 1] - yg[j])
+        c = 1.0 / (y[j] - y[j - 1]) / (yg[j] - yg[j - 1])
+        lap_y = a * Pi[:, j + 1, :] - (a + c) * Pi[:, j, :] + c * Pi[:, j - 1, :]
+        res[:, j - 2, :] = lap_xz[:, j, :] + lap_y - rhs[2:nxp + 2, j, 2:nzp + 2]
+    scale = np.abs(rhs[2:nxp + 2, 2:nyg, 2:nzp + 2]).max()
+    # every non-mean mode solves the discrete problem
+    fluct = res - res.mean(axis=(0, 2), keepdims=True)
+    assert np.abs(fluct).max() < 1e-9 * scale
+    # the mean mode solves it on every row but the pinned one
+    assert np.abs(res.mean(axis=(0, 2))[1:]).max() < 1e-9 * scale
+    # the wall conditions are not trivial for this state
+    assert np.abs(bc1[2:g.nxg, 2:g.nzg]).max() > 0
