@@ -10,6 +10,7 @@ index bounds (see ``bounds``).
 """
 import ctypes as C
 import math
+import os
 
 import numpy as np
 
@@ -257,6 +258,42 @@ class Channel:
         """Qflow_x_0, Qflow_y_0, Qflow_z_0 (src/global.f90:180)."""
         self._check(self._lib.c3d_set_flow_targets(self.handle, Qflow_x_0, Qflow_y_0, Qflow_z_0))
 
+    # ------------------------------------- input_output, statistics, monitor
+    def write_snapshot(self, path, original_format=False):
+        """output_data (src/input_output.f90:498-728) to ``path``."""
+        self._check(self._lib.c3d_write_snapshot(self.handle, os.fsencode(path), int(bool(original_format))))
+
+    def read_snapshot(self, path):
+        """read_input_data (src/input_output.f90:335-489): mesh and U, V, W."""
+        self._check(self._lib.c3d_read_snapshot(self.handle, os.fsencode(path)))
+
+    STAT_NAMES = ("Umean", "Vmean", "Wmean", "U2mean", "V2mean", "W2mean", "UVmean")
+
+    def compute_statistics(self):
+        """compute_statistics (src/statistics.f90:22-148): the seven y
+        profiles at yg(1:nyg) and utau, wtau, Retau_u, Retau_w, Qflow_x/y/z."""
+        nyg = self.dims["nyg"]
+        prof = np.zeros(7 * nyg)
+        sc = np.zeros(8)
+        self._check(self._lib.c3d_compute_statistics(self.handle, prof.ctypes.data_as(L._D),
+                                                      sc.ctypes.data_as(L._D)))
+        out = {n: prof[q * nyg:(q + 1) * nyg].copy() for q, n in enumerate(self.STAT_NAMES)}
+        out.update(dict(zip(("utau", "wtau", "Retau_u", "Retau_w", "Qflow_x", "Qflow_y", "Qflow_z"),
+                            map(float, sc[:7]))))
+        out["nonfinite"] = bool(sc[7])
+        return out
+
+    def write_statistics(self, path, istep):
+        """output_statistics (src/input_output.f90:733-754) to ``path``."""
+        self._check(self._lib.c3d_write_statistics(self.handle, os.fsencode(path), int(istep)))
+
+    def output_monitor(self):
+        """The values output_monitor prints (src/monitor.f90:21-110)."""
+        out = np.zeros(8)
+        self._check(self._lib.c3d_monitor(self.handle, out.ctypes.data_as(L._D)))
+        return dict(zip(("meanU", "meanV", "meanW", "maxU", "maxV", "maxW", "max_divergence", "max_slip"),
+                        map(float, out)))
+
     def compute_pressure(self):
         self._check(self._lib.c3d_compute_pressure(self.handle))
 
@@ -409,8 +446,9 @@ def laminar_perturbed_fields(grid, dims, dPdx, nu, Ly=2.0, amplitude=0.1, seed=0
 def seeded_initial_state(ch, dPdx, nu, amplitude=0.1, seed=0, dt=1e-3):
     """Set the seeded initial state on the device: host fields of
     ``laminar_perturbed_fields``, boundary conditions, one projection (dt
-    cancels), boundary conditions, and Qflow_x_0, Qflow_y_0, Qflow_z_0 from
-    the result (app/main.f90:90-92).  Returns Qflow_x_0."""
+    cancels), boundary conditions, and Qflow_x_0 and Qflow_z_0 from the
+    result (app/main.f90:90-92); Qflow_y_0 and dPdy are zero (:93-94).
+    Returns Qflow_x_0."""
     g = ch.grid()
     U, V, W = laminar_perturbed_fields(g, ch.dims, dPdx, nu, amplitude=amplitude, seed=seed)
     ch.upload("U", U)
@@ -424,5 +462,5 @@ def seeded_initial_state(ch, dPdx, nu, amplitude=0.1, seed=0, dt=1e-3):
     ch.apply_boundary_conditions("UVW")
     q = ch.compute_mean_mass_flow_U()
     ch.set_scalars(dPdx=dPdx, t=0.0, Qflow_x_0=q)
-    ch.set_flow_targets(q, ch.compute_mean_mass_flow_V(), ch.compute_mean_mass_flow_W())
+    ch.set_flow_targets(q, 0.0, ch.compute_mean_mass_flow_W())
     return q

@@ -4,7 +4,9 @@
 // create_grid, initialize) and of the control flow of
 // compute_time_step_RK3 (src/time_integration.f90:86-213); all field
 // arithmetic runs in the kernels of k_*.cu on the handle's stream.
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <mutex>
@@ -815,6 +817,63 @@ int c3d_compute_dPz_for_constant_mass_flow(int id, double* dPdz) {
   int rc = massflow(h, 2, true, &q);
   if (rc) RET(h, rc);
   *dPdz = h->Qflow_z_0 - q;
+  RET(h, 0);
+}
+
+static int marker_out(Handle* h, double* dev, double* host, int64_t n);
+
+int c3d_compute_statistics(int id, double* profiles, double* scalars) {
+  GET_HANDLE(id);
+  if (!profiles || !scalars) return C3D_ERR_PARAM;
+  RET(h, compute_statistics(h, profiles, scalars));
+}
+
+int c3d_write_statistics(int id, const char* path, int istep) {
+  GET_HANDLE(id);
+  if (!path) return C3D_ERR_PARAM;
+  const int nyg = h->d.nyg;
+  std::vector<double> prof(7 * (size_t)nyg);
+  double sc[8];
+  int rc = compute_statistics(h, prof.data(), sc);
+  if (rc) RET(h, rc);
+  // output_statistics, src/input_output.f90:733-754
+  FILE* f = std::fopen(path, "w");
+  if (!f) { h->last_error = std::string("cannot open ") + path; RET(h, C3D_ERR_IO); }
+  std::fprintf(f, "%%%15.8f%15.8f%15.8f%15.8f%12d%12d%12d%12d\n", h->t, sc[2], sc[0], h->p.nu, h->p.nx_global,
+               h->p.ny_global, h->p.nz_global, istep);
+  for (int j = 0; j < nyg; ++j) {
+    std::fprintf(f, "%15.8f", h->yg[j + 1]);
+    for (int q = 0; q < 7; ++q) std::fprintf(f, "%15.8f", prof[(size_t)q * nyg + j]);
+    std::fprintf(f, "\n");
+  }
+  if (std::fclose(f) != 0) { h->last_error = std::string("write error on ") + path; RET(h, C3D_ERR_IO); }
+  RET(h, 0);
+}
+
+int c3d_monitor(int id, double* out) {
+  GET_HANDLE(id);
+  if (!out) return C3D_ERR_PARAM;
+  int rc = monitor_values(h, out);
+  if (rc) RET(h, rc);
+  out[7] = 0.0;
+  if (h->ib) {
+    // check_slip, src/monitor.f90:223-231: max |E u - E1nH_exterior dudn_jump - ub|
+    const int nb = ib_nb(h);
+    std::vector<double> Eu(3 * (size_t)nb), e1(3 * (size_t)nb), fb(4 * (size_t)nb), ub(3 * (size_t)nb);
+    double* dev = ib_scratch(h, 0);
+    if ((rc = ib_regT(h, h->U, h->V, h->W, dev))) RET(h, rc);
+    if ((rc = marker_out(h, dev, Eu.data(), 3 * (int64_t)nb))) RET(h, rc);
+    int64_t len = 0;
+    double* p = ib_marker_ptr(h, C3D_MARKER_E1NH_EXT, &len);
+    if ((rc = marker_out(h, p, e1.data(), 3 * (int64_t)nb))) RET(h, rc);
+    p = ib_marker_ptr(h, C3D_MARKER_FB, &len);
+    if ((rc = marker_out(h, p, fb.data(), 4 * (int64_t)nb))) RET(h, rc);
+    p = ib_marker_ptr(h, C3D_MARKER_UB, &len);
+    if ((rc = marker_out(h, p, ub.data(), 3 * (int64_t)nb))) RET(h, rc);
+    double mx = 0.0;
+    for (size_t q = 0; q < 3 * (size_t)nb; ++q) mx = std::max(mx, std::fabs(Eu[q] - e1[q] * fb[q] - ub[q]));
+    out[7] = mx;
+  }
   RET(h, 0);
 }
 

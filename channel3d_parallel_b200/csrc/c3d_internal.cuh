@@ -159,6 +159,8 @@ struct Handle {
   double *U = nullptr, *V = nullptr, *W = nullptr, *P = nullptr;
   double *Us = nullptr, *Vs = nullptr, *Ws = nullptr;       // star / work fields
   double* pbc = nullptr;          // compute_pressure wall conditions bc_1, bc_2 (2 x nxg x nzg)
+  double* stat_buf = nullptr;     // compute_statistics partials and profiles
+  int64_t stat_cap = 0;
   double *Gu = nullptr, *Gv = nullptr, *Gw = nullptr;       // RK accumulators
   double *rhs_p = nullptr;                                  // rhs_p / phi
   double *P_interim = nullptr;
@@ -253,6 +255,10 @@ void mixed_free(Handle* h);
 // mass flow and reductions (k_massflow.cu)
 int launch_massflow_correction(Handle* h, double dt, bool euler = false);
 int massflow(Handle* h, int comp, bool u_view, double* q_out);
+int massflow_w_as_v(Handle* h, double* q_out);
+// diagnostics (k_stats.cu)
+int compute_statistics(Handle* h, double* profiles, double* scalars);
+int monitor_values(Handle* h, double* out);
 int max_abs_divergence(Handle* h, const double* U, const double* V, const double* W, double* out);
 int check_finite(Handle* h, bool* ok);
 int compute_dt_cfl(Handle* h, double* dt);

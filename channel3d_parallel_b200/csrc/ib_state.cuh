@@ -14,6 +14,7 @@ struct IbState {
   int nb = 0, nbodies = 0;
   // host geometry
   std::vector<double> xb, yb, zb, ub, nrm, sb;
+  std::vector<double> tan1, tan2;   // tangents_1, tangents_2 (3*nb; written to snapshots only)
   std::vector<int> yref, body;
   std::vector<int> body_count;
   // device geometry

@@ -38,6 +38,7 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
     s->nb = nb;
     s->xb.assign(nb, 0); s->yb.assign(nb, 0); s->zb.assign(nb, 0);
     s->ub.assign(3 * nb, 0); s->nrm.assign(3 * nb, 0); s->sb.assign(nb, 0);
+    s->tan1.assign(3 * nb, 0); s->tan2.assign(3 * nb, 0);
     s->yref.assign(nb, 1); s->body.assign(nb, 0);
     s->lat_nx = nb;
   };
@@ -55,7 +56,12 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
         s->zb[k] = ((double)j - 0.5) * dzb;
         s->yref[k] = p.ny_global / 2;
       }
-    for (int k = 0; k < nb; ++k) { s->sb[k] = dxb * dzb; s->nrm[nb + k] = -1.0; }
+    for (int k = 0; k < nb; ++k) {                                  // :108-115
+      s->sb[k] = dxb * dzb;
+      s->nrm[nb + k] = -1.0;
+      s->tan1[k] = 1.0;
+      s->tan2[2 * nb + k] = -1.0;
+    }
     s->nbodies = 1;
   } else if (s->kind == "standing_wave" || s->kind == "wall_standing_wave") {   // :176-269
     const bool two = (s->kind == "standing_wave");
@@ -98,10 +104,16 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
         s->ub[nb + k] = vy;
         s->nrm[k] = t1y;
         s->nrm[nb + k] = -t1x;
+        s->tan1[k] = t1x;                                            // :236-244
+        s->tan1[nb + k] = t1y;
+        s->tan2[2 * nb + k] = 1.0;
         if (two) {
           s->ub[nb + k + nxb] = vy;
           s->nrm[k + nxb] = -t1y;
           s->nrm[nb + k + nxb] = t1x;
+          s->tan1[k + nxb] = t1x;
+          s->tan1[nb + k + nxb] = t1y;
+          s->tan2[2 * nb + k + nxb] = 1.0;
         }
       }
     for (int j = 1; j <= nzb; ++j)
@@ -156,6 +168,9 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
         const double ttx = 1.0 / std::sqrt(1.0 + stop * stop), tty = stop / std::sqrt(1.0 + stop * stop);
         s->nrm[k] = tby; s->nrm[k + nxb] = -tty;
         s->nrm[nb + k] = -tbx; s->nrm[nb + k + nxb] = ttx;
+        s->tan1[k] = tbx; s->tan1[k + nxb] = ttx;                    // :344-352
+        s->tan1[nb + k] = tby; s->tan1[nb + k + nxb] = tty;
+        s->tan2[2 * nb + k] = 1.0; s->tan2[2 * nb + k + nxb] = 1.0;
       }
     for (int j = 1; j <= nzb; ++j)
       for (int i = 1; i <= nxb; ++i)
@@ -202,6 +217,8 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
         s->sb[k] = dsb1 * dzb;
         s->nrm[k] = -std::cos(th);
         s->nrm[nb + k] = -std::sin(th);
+        s->tan1[k] = std::sin(th);                                   // :146-147
+        s->tan1[nb + k] = -std::cos(th);
         s->body[k] = 0;
       }
       for (int i = 1; i <= nxb2; ++i) {
@@ -213,9 +230,12 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
         s->sb[k] = dsb2 * dzb;
         s->nrm[k] = std::cos(th);
         s->nrm[nb + k] = std::sin(th);
+        s->tan1[k] = -std::sin(th);                                  // :160-161
+        s->tan1[nb + k] = std::cos(th);
         s->body[k] = 1;
       }
     }
+    for (int k = 0; k < nb; ++k) s->tan2[2 * nb + k] = 1.0;         // :164-166
     s->nbodies = 2;
   } else if (s->kind == "two_cylinders_z") {
     // extension: two separate spanwise cylinders of radius body_param_1,
@@ -246,6 +266,9 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
           s->sb[k] = dsb * dzb;
           s->nrm[k] = -std::cos(th);
           s->nrm[nb + k] = -std::sin(th);
+          s->tan1[k] = std::sin(th);
+          s->tan1[nb + k] = -std::cos(th);
+          s->tan2[2 * nb + k] = 1.0;
           s->body[k] = c;
         }
     s->nbodies = 2;
@@ -294,6 +317,9 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
             const double nn = std::sqrt(1.0 + slope * slope);
             s->nrm[k] = 1.0 / nn;
             s->nrm[nb + k] = -slope / nn;
+            s->tan1[k] = slope / nn;                                    // along the plate, up
+            s->tan1[nb + k] = 1.0 / nn;
+            s->tan2[2 * nb + k] = 1.0;
             s->sb[k] = ((hh - 3.0 * h->dymin) / (my - 1)) * (wz / mz);
             s->yref[k] = 1;
             s->body[k] = 0;

@@ -219,6 +219,18 @@ int massflow(Handle* h, int comp, bool u_view, double* q_out) {
   return 0;
 }
 
+// compute_mean_mass_flow_V applied to W, as compute_statistics calls it
+// (src/statistics.f90:133): W read through V's declared extents (nxg, ny,
+// nzg) with V's loops and weights (every offset reached lies inside W)
+int massflow_w_as_v(Handle* h, double* q_out) {
+  FluxView v = flux_view(h, 1, h->W, flux_weight(h, 1), false);
+  k_flux<<<kRedBlocks, kRedThreads, 0, h->stream>>>(v, (double2*)h->red, h->sc, 0.0, 1.0, 0, 1);
+  C3D_LAUNCH_CHECK(h);
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(q_out, &h->sc->qflow, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
 // ---- max |div u| over cells (i,j,k) in 2..nxg-1 x 2..nyg-1 x 2..nzg-1 ----
 __global__ void __launch_bounds__(kRedThreads) k_maxdiv(Dims d, Metric m, const double* __restrict__ U,
                                                        const double* __restrict__ V,

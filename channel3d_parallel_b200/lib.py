@@ -66,6 +66,11 @@ PROTOTYPES = {
     "c3d_synchronize": [_INT],
     "c3d_time_step_rk3": [_INT, _INT],
     "c3d_time_step_euler": [_INT, _INT],
+    "c3d_write_snapshot": [_INT, C.c_char_p, _INT],
+    "c3d_read_snapshot": [_INT, C.c_char_p],
+    "c3d_compute_statistics": [_INT, _D, _D],
+    "c3d_write_statistics": [_INT, C.c_char_p, _INT],
+    "c3d_monitor": [_INT, _D],
     "c3d_compute_dt": [_INT, _D],
     "c3d_compute_mean_mass_flow_u": [_INT, _D],
     "c3d_compute_mean_mass_flow_v": [_INT, _D],

@@ -189,6 +189,28 @@ int c3d_compute_dPz_for_constant_mass_flow(int handle, double* dPdz);
  * are commented out (src/statistics.f90:37, src/input_output.f90:508).       */
 int c3d_compute_pressure(int handle);
 
+/* ---- snapshots and diagnostics (the calls of app/main.f90:97-118) --------- */
+/* output_data, src/input_output.f90:498-728: binary snapshot of the current
+ * state (big-endian stream: mesh, U, V, W, P, Hu/Hv/Hw_interior, t, dt, dPdx,
+ * nu, marker arrays); original_format = 1 stops after P (tools/file_io.py's
+ * original format).                                                          */
+int c3d_write_snapshot(int handle, const char* path, int original_format);
+/* read_input_data, src/input_output.f90:335-489: mesh and U, V, W of a
+ * snapshot; every size must match the handle (C3D_ERR_PARAM otherwise, with
+ * the reference's message); replaces the grid (as c3d_set_grid) and fields.  */
+int c3d_read_snapshot(int handle, const char* path);
+/* compute_statistics, src/statistics.f90:22-148: profiles[7*nyg] = Umean,
+ * Vmean, Wmean, U2mean, V2mean, W2mean, UVmean at yg(1:nyg); scalars[8] =
+ * utau, wtau, Retau_u, Retau_w, Qflow_x, Qflow_y, Qflow_z, and 1 if U, V or
+ * W holds a non-finite value (the reference stops there).                    */
+int c3d_compute_statistics(int handle, double* profiles, double* scalars);
+/* output_statistics, src/input_output.f90:733-754: the statistics text file */
+int c3d_write_statistics(int handle, const char* path, int istep);
+/* output_monitor reductions, src/monitor.f90:21-110: out[8] = mean U, V, W
+ * (divided by nxm*nym*nzm as printed), max U, V, W, max |div u|, max IB slip
+ * (check_slip, :223-231; 0 without a body).                                 */
+int c3d_monitor(int handle, double* out);
+
 /* ---- immersed boundary ---------------------------------------------------- */
 /* setup_IB_geometry (src/immersed_boundary_geometry.f90:70-398) at time t   */
 int c3d_setup_IB_geometry(int handle);

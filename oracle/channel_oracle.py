@@ -853,10 +853,10 @@ def seeded_initial_state(g, dPdx, amplitude=0.1, seed=0, project=True, dt=1e-3):
         st.P_interim[...] = 0.0
     q, norm = mean_mass_flow_u(g, st.U)
     st.Qflow_x_0 = q / norm
-    q, norm = mean_mass_flow_v(g, st.V)                  # app/main.f90:91-92
-    st.Qflow_y_0 = q / norm
-    q, norm = mean_mass_flow_w(g, st.W)
+    q, norm = mean_mass_flow_w(g, st.W)                  # app/main.f90:91-92
     st.Qflow_z_0 = q / norm
+    st.Qflow_y_0 = 0.0                                   # :93-94 (the V flux is
+    st.dPdy = 0.0                                        # computed, then reset)
     return st
 
 

@@ -55,6 +55,10 @@ class Body:
             self.sb = np.full(nb, dxb * dzb)
             self.normals = np.zeros(3 * nb)
             self.normals[nb:2 * nb] = -1.0
+            self.tangents_1 = np.zeros(3 * nb)                  # :111-115
+            self.tangents_1[:nb] = 1.0
+            self.tangents_2 = np.zeros(3 * nb)
+            self.tangents_2[2 * nb:] = -1.0
             self.blocks = [np.arange(nb)]
         elif kind in ("standing_wave", "wall_standing_wave"):       # :176-269
             self._standing_wave(t, two_walls=(kind == "standing_wave"))
@@ -70,6 +74,8 @@ class Body:
             m = self.markers
             self.xb, self.yb, self.zb = m["xb"].copy(), m["yb"].copy(), m["zb"].copy()
             self.ub, self.normals, self.sb = m["ub"].copy(), m["normals"].copy(), m["sb"].copy()
+            self.tangents_1 = np.asarray(m.get("tangents_1", np.zeros(3 * len(m["xb"])))).copy()
+            self.tangents_2 = np.asarray(m.get("tangents_2", np.zeros(3 * len(m["xb"])))).copy()
             self.y_ref = m["y_ref"].copy()
             self.blocks = [np.asarray(b) for b in m["blocks"]]
         else:
@@ -140,6 +146,9 @@ class Body:
                 if two_walls:
                     sb[k + nxb] = dzb * (0.5 * a1 + 0.5 * a2)
         self.xb, self.yb, self.zb, self.ub, self.normals, self.sb = xb, yb, zb, ub, nrm, sb
+        self.tangents_1 = t1                                        # :236-244
+        self.tangents_2 = np.zeros(3 * nb)
+        self.tangents_2[2 * nb:] = 1.0
         self.y_ref = yref
         self.blocks = [np.array(bot)] + ([np.array(top)] if two_walls else [])
 
@@ -205,6 +214,9 @@ class Body:
                         a2 = math.sqrt((xb[k] - xb[k + 1]) ** 2 + (yb[k] - yb[k + 1]) ** 2)
                     sb[k] = dzb * (0.5 * a1 + 0.5 * a2)
         self.xb, self.yb, self.zb, self.ub, self.normals, self.sb = xb, yb, zb, ub, nrm, sb
+        self.tangents_1 = t1                                        # :344-352
+        self.tangents_2 = np.zeros(3 * nb)
+        self.tangents_2[2 * nb:] = 1.0
         self.y_ref = yref
         self.blocks = [np.array(bot), np.array(top)]
 
@@ -224,6 +236,7 @@ class Body:
         dsb2 = 2 * 3.14159 * r2 / nxb2
         xb, yb, zb = np.zeros(nb), np.zeros(nb), np.zeros(nb)
         ub, nrm, sb = np.zeros(3 * nb), np.zeros(3 * nb), np.zeros(nb)
+        t1 = np.zeros(3 * nb)
         inner, outer = [], []
         for j in range(1, nzb + 1):
             for i in range(1, nxb1 + 1):
@@ -237,6 +250,8 @@ class Body:
                 sb[k] = dsb1 * dzb
                 nrm[k] = -math.cos(th)
                 nrm[nb + k] = -math.sin(th)
+                t1[k] = math.sin(th)                                # :146-147
+                t1[nb + k] = -math.cos(th)
                 inner.append(k)
             for i in range(1, nxb2 + 1):
                 k = i + (j - 1) * nxb + nxb1 - 1
@@ -247,8 +262,13 @@ class Body:
                 sb[k] = dsb2 * dzb
                 nrm[k] = math.cos(th)
                 nrm[nb + k] = math.sin(th)
+                t1[k] = -math.sin(th)                               # :160-161
+                t1[nb + k] = math.cos(th)
                 outer.append(k)
         self.xb, self.yb, self.zb, self.ub, self.normals, self.sb = xb, yb, zb, ub, nrm, sb
+        self.tangents_1 = t1
+        self.tangents_2 = np.zeros(3 * nb)                          # :164-166
+        self.tangents_2[2 * nb:] = 1.0
         self.y_ref = np.ones(nb, dtype=np.int64)
         self.blocks = [np.array(inner), np.array(outer)]
 
@@ -269,6 +289,7 @@ class Body:
         sgn = (1.0, -1.0)
         xb, yb, zb = np.zeros(nb), np.zeros(nb), np.zeros(nb)
         ub, nrm, sb = np.zeros(3 * nb), np.zeros(3 * nb), np.zeros(nb)
+        t1 = np.zeros(3 * nb)
         blocks = ([], [])
         for j in range(1, nzb + 1):
             for c in range(2):
@@ -283,8 +304,13 @@ class Body:
                     sb[k] = dsb * dzb
                     nrm[k] = -math.cos(th)
                     nrm[nb + k] = -math.sin(th)
+                    t1[k] = math.sin(th)
+                    t1[nb + k] = -math.cos(th)
                     blocks[c].append(k)
         self.xb, self.yb, self.zb, self.ub, self.normals, self.sb = xb, yb, zb, ub, nrm, sb
+        self.tangents_1 = t1
+        self.tangents_2 = np.zeros(3 * nb)
+        self.tangents_2[2 * nb:] = 1.0
         self.y_ref = np.ones(nb, dtype=np.int64)
         self.blocks = [np.array(blocks[0]), np.array(blocks[1])]
 
@@ -305,6 +331,7 @@ class Body:
         phase = splitmix64_phases(int(round(p["body_param_4"])), nxb * nzb)
         xb, yb, zb = np.zeros(nb), np.zeros(nb), np.zeros(nb)
         ub, nrm, sb = np.zeros(3 * nb), np.zeros(3 * nb), np.zeros(nb)
+        t1 = np.zeros(3 * nb)
         for pj in range(1, nzb + 1):
             for m in range(1, mz + 1):
                 for pi_ in range(1, nxb + 1):
@@ -324,8 +351,13 @@ class Body:
                         nn = math.sqrt(1.0 + slope * slope)
                         nrm[k] = 1.0 / nn
                         nrm[nb + k] = -slope / nn
+                        t1[k] = slope / nn                          # along the plate, up
+                        t1[nb + k] = 1.0 / nn
                         sb[k] = ((hh - 3.0 * g.dymin) / (my - 1)) * (wz / mz)
         self.xb, self.yb, self.zb, self.ub, self.normals, self.sb = xb, yb, zb, ub, nrm, sb
+        self.tangents_1 = t1
+        self.tangents_2 = np.zeros(3 * nb)
+        self.tangents_2[2 * nb:] = 1.0
         self.y_ref = np.ones(nb, dtype=np.int64)
         self.blocks = [np.arange(nb)]
 
