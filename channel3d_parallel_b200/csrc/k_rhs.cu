@@ -292,15 +292,16 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
       {
         const double v1m = AV(s0, 1, -1);
         const double w1m = AW(sm, 1, 0);
+        // independent partial sums (short dependency chains)
         const double ap = u0 + uxp, am = uxm + u0;
-        double r = (am * am - ap * ap) * (0.25 * rdxg_i);
-        r += ((uym + u0) * (vym + v1m) - (u0 + uyp) * (v0 + vxp)) * (0.25 * rdy_j);
-        r += ((uzm + u0) * (wzm + w1m) - (u0 + uzp) * (w0 + wxp)) * (0.25 * rdz_k);
-        r += cxpF_i * (uxp - u0) - cxmF_i * (u0 - uxm)
-           + cypC_j * (uyp - u0) - cymC_j * (u0 - uym)
-           + czpC_k * (uzp - u0) - czmC_k * (u0 - uzm);
-        r += a.Hu ? dPdx * __ldg(a.Hu + iu) : dPdx;
-        Fu = r;
+        const double cx = (am * am - ap * ap) * (0.25 * rdxg_i);
+        const double cy = ((uym + u0) * (vym + v1m) - (u0 + uyp) * (v0 + vxp)) * (0.25 * rdy_j);
+        const double cz = ((uzm + u0) * (wzm + w1m) - (u0 + uzp) * (w0 + wxp)) * (0.25 * rdz_k);
+        const double vx = cxpF_i * (uxp - u0) - cxmF_i * (u0 - uxm);
+        const double vy = cypC_j * (uyp - u0) - cymC_j * (u0 - uym);
+        const double vz = czpC_k * (uzp - u0) - czmC_k * (u0 - uzm);
+        const double f = a.Hu ? dPdx * __ldg(a.Hu + iu) : dPdx;
+        Fu = ((cx + cy) + (cz + f)) + ((vx + vy) + vz);
       }
       {
         const double wxm = AW(s0, -1, 0), wym = AW(s0, 0, -1), wyp = AW(s0, 0, 1);
@@ -308,14 +309,14 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
         const double umzp = AU(sp, -1, 0);
         const double vzp = AV(sp, 0, 0), vymzp = AV(sp, 0, -1);
         const double am = wzm + w0, ap = w0 + wzp;
-        double r = (am * am - ap * ap) * (0.25 * rdzg_k);
-        r += ((uxm + umzp) * (wxm + w0) - (u0 + uzp) * (w0 + wxp)) * (0.25 * rdx_i);
-        r += ((vym + vymzp) * (wym + w0) - (v0 + vzp) * (w0 + wyp)) * (0.25 * rdy_j);
-        r += cxpC_i * (wxp - w0) - cxmC_i * (w0 - wxm)
-           + cypC_j * (wyp - w0) - cymC_j * (w0 - wym)
-           + czpF_k * (wzp - w0) - czmF_k * (w0 - wzm);
-        r += a.Hw ? dPdz * __ldg(a.Hw + iw) : dPdz;
-        Fw = r;
+        const double cz = (am * am - ap * ap) * (0.25 * rdzg_k);
+        const double cx = ((uxm + umzp) * (wxm + w0) - (u0 + uzp) * (w0 + wxp)) * (0.25 * rdx_i);
+        const double cy = ((vym + vymzp) * (wym + w0) - (v0 + vzp) * (w0 + wyp)) * (0.25 * rdy_j);
+        const double vx = cxpC_i * (wxp - w0) - cxmC_i * (w0 - wxm);
+        const double vy = cypC_j * (wyp - w0) - cymC_j * (w0 - wym);
+        const double vz = czpF_k * (wzp - w0) - czmF_k * (w0 - wzm);
+        const double f = a.Hw ? dPdz * __ldg(a.Hw + iw) : dPdz;
+        Fw = ((cz + cx) + (cy + f)) + ((vx + vy) + vz);
       }
       if (hasv) {
         const double vxm = AV(s0, -1, 0), vyp = AV(s0, 0, 1);
@@ -323,14 +324,14 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
         const double um1 = AU(s0, -1, 1);
         const double wyp = AW(s0, 0, 1), wypzm = AW(sm, 0, 1);
         const double am = vym + v0, ap = v0 + vyp;
-        double r = (am * am - ap * ap) * (0.25 * rdyg_j);
-        r += ((uxm + um1) * (vxm + v0) - (u0 + uyp) * (v0 + vxp)) * (0.25 * rdx_i);
-        r += ((vzm + v0) * (wzm + wypzm) - (v0 + vzp) * (w0 + wyp)) * (0.25 * rdz_k);
-        r += cxpC_i * (vxp - v0) - cxmC_i * (v0 - vxm)
-           + cypF_j * (vyp - v0) - cymF_j * (v0 - vym)
-           + czpC_k * (vzp - v0) - czmC_k * (v0 - vzm);
-        r += a.Hv ? dPdy * __ldg(a.Hv + iv) : dPdy;
-        Fv = r;
+        const double cy = (am * am - ap * ap) * (0.25 * rdyg_j);
+        const double cx = ((uxm + um1) * (vxm + v0) - (u0 + uyp) * (v0 + vxp)) * (0.25 * rdx_i);
+        const double cz = ((vzm + v0) * (wzm + wypzm) - (v0 + vzp) * (w0 + wyp)) * (0.25 * rdz_k);
+        const double vx = cxpC_i * (vxp - v0) - cxmC_i * (v0 - vxm);
+        const double vy = cypF_j * (vyp - v0) - cymF_j * (v0 - vym);
+        const double vz = czpC_k * (vzp - v0) - czmC_k * (v0 - vzm);
+        const double f = a.Hv ? dPdy * __ldg(a.Hv + iv) : dPdy;
+        Fv = ((cy + cx) + (cz + f)) + ((vx + vy) + vz);
       }
 #undef AU
 #undef AV
@@ -350,7 +351,9 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
         if (hasv) a.Vs[iv] = gv + a.cs * Fv;
       }
     }
-    __syncthreads();   // plane k-1's slot is refilled by the next iteration
+    // No barrier here: the slot the next iteration refills, (k+5) mod 8, held
+    // plane k-3, last read in iteration k-2; every thread finished that
+    // iteration before it reached this iteration's barrier.
   }
 }
 
