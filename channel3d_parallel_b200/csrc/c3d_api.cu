@@ -466,7 +466,9 @@ static int enqueue_step(Handle* h, double dt, double to) {
   int rc, warn = 0;
   for (int s = 1; s <= 3; ++s) {
     if ((rc = launch_rhs_stage(h, s, dt))) return rc;
-    if ((rc = launch_fill_ghosts3(h, h->Us, h->Vs, h->Ws))) return rc;
+    // the projection reads the ghosts of U*, V*, W* as the boundary
+    // conditions define them; the immersed-boundary operators need them set
+    if (h->ib && (rc = launch_fill_ghosts3(h, h->Us, h->Vs, h->Ws))) return rc;
     const double ts = to + rk_t[s - 1] * dt;
     if (h->ib && ib_moving(h)) {                         // :111-115
       if ((rc = ib_setup_geometry(h, ts))) return rc;
@@ -494,7 +496,7 @@ static int enqueue_step(Handle* h, double dt, double to) {
 static int enqueue_euler_step(Handle* h, double dt) {
   int rc;
   if ((rc = launch_rhs_euler(h, dt))) return rc;                // :34-52
-  if ((rc = launch_fill_ghosts3(h, h->Us, h->Vs, h->Ws))) return rc;
+  if (h->ib && (rc = launch_fill_ghosts3(h, h->Us, h->Vs, h->Ws))) return rc;
   if ((rc = launch_projection_step(h, 3, dt))) return rc;       // :58-61
   if (h->p.x_mass_cte == 1 || h->p.y_mass_cte == 1) {           // :65-78
     if ((rc = launch_massflow_correction(h, dt, true))) return rc;
@@ -958,7 +960,7 @@ int c3d_profile_kernels(int id, int nrep, double* ms, int nmax) {
         case 0: rc = launch_rhs_stage(h, 2, dt); break;
         case 1: rc = launch_fill_ghosts3(h, h->Us, h->Vs, h->Ws); break;
         case 2: case 3: case 4: rc = profile_spectral(h, c - 2); break;
-        case 5: rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W); break;
+        case 5: rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W, false); break;
         case 6: rc = launch_massflow_correction(h, dt); break;
       }
       if (rc) RET(h, rc);

@@ -230,10 +230,14 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
       x0[q] = x1[q] = y0[q] = y1[q] = z0[q] = z1[q] = 0.0;
       if (j > 0) {
         if (FROM_DIV) {
+          // the ghost values are read as the boundary conditions define them
+          // (periodic images in x and z, zero V walls), so the fields need
+          // no ghost fill after the stage update
           const int64_t iu = idxU(d, i, j, k), iv = idxV(d, i, j, k), iw = idxW(d, i, j, k);
-          x1[q] = a.U[iu]; x0[q] = a.U[iu - 1];
-          y1[q] = a.V[iv]; y0[q] = a.V[iv - d.nxg];
-          z1[q] = a.W[iw]; z0[q] = a.W[iw - (int64_t)d.nxg * d.nyg];
+          const int64_t plw = (int64_t)d.nxg * d.nyg;
+          x1[q] = a.U[iu]; x0[q] = a.U[i == 2 ? iu + (N - 1) : iu - 1];
+          y1[q] = j == d.ny ? 0.0 : a.V[iv]; y0[q] = j == 2 ? 0.0 : a.V[iv - d.nxg];
+          z1[q] = a.W[iw]; z0[q] = a.W[k == 2 ? iw + (int64_t)(d.Nz - 1) * plw : iw - plw];
         } else {
           x1[q] = a.rhs[idxR(d, i, j, k)];
         }
@@ -1018,13 +1022,13 @@ int launch_poisson_of_div_band(Handle* h, const double* U, const double* V, cons
 // projection: U = Ui - G phi at interior points (src/projection.f90:40-44),
 // optional P_interim = phi/dt; ghosts are filled by the caller
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_grad_sub(Dims d, Metric m, const double* __restrict__ Ui,
+__global__ void __launch_bounds__(256, 6) k_grad_sub(Dims d, Metric m, const double* __restrict__ Ui,
                                                   const double* __restrict__ Vi,
                                                   const double* __restrict__ Wi,
                                                   const double* __restrict__ phi,
                                                   double* __restrict__ Uo, double* __restrict__ Vo,
                                                   double* __restrict__ Wo,
-                                                  double* __restrict__ Pint, double rdt) {
+                                                  double* __restrict__ Pint, double rdt, int dup) {
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 2 + blockIdx.z * blockDim.z + threadIdx.z;
@@ -1043,15 +1047,14 @@ __global__ void __launch_bounds__(256) k_grad_sub(Dims d, Metric m, const double
   Uo[iu] = un;
   Wo[iw] = wn;
   if (j <= d.Ny) Vo[idxV(d, i, j, k)] = vn;
-  if (k == 2) {
+  if (dup && k == 2) {
     // the reference's gradient also covers plane nzg-1 (the duplicate of
-    // plane 2) for the x and y components (src/differential_operators.f90:38-52)
+    // plane 2) for the x and y components (src/differential_operators.f90:38-52);
+    // the input's duplicate plane is read as the periodic image of plane 2.
+    // Skipped (dup = 0) where the boundary conditions are applied next.
     const int kd = d.Nz + 2;
-    Uo[idxU(d, i, j, kd)] = __ldg(Ui + idxU(d, i, j, kd)) - (px - p0) * m.rdxg[i];
-    if (j <= d.Ny) {
-      const int64_t ivd = idxV(d, i, j, kd);
-      Vo[ivd] = __ldg(Vi + ivd) - (py - p0) * m.rdyg[j];
-    }
+    Uo[idxU(d, i, j, kd)] = __ldg(Ui + iu) - (px - p0) * m.rdxg[i];
+    if (j <= d.Ny) Vo[idxV(d, i, j, kd)] = __ldg(Vi + idxV(d, i, j, k)) - (py - p0) * m.rdyg[j];
   }
   if (Pint) {
     Pint[idxR(d, i, j, k)] = p0 * rdt;
@@ -1064,12 +1067,13 @@ __global__ void __launch_bounds__(256) k_grad_sub(Dims d, Metric m, const double
 }
 
 int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, const double* Wi,
-                             const double* phi, double dt, double* Uo, double* Vo, double* Wo) {
+                             const double* phi, double dt, double* Uo, double* Vo, double* Wo,
+                             bool dup_plane) {
   const Dims& d = h->d;
   dim3 b(32, 4, 2);
   dim3 g((d.Nx + 31) / 32, (d.Ny + 3) / 4, (d.Nz + 1) / 2);
   double* Pint = (h->ib != nullptr || h->write_pinterim) ? h->P_interim : nullptr;
-  k_grad_sub<<<g, b, 0, h->stream>>>(d, h->m, Ui, Vi, Wi, phi, Uo, Vo, Wo, Pint, 1.0 / dt);
+  k_grad_sub<<<g, b, 0, h->stream>>>(d, h->m, Ui, Vi, Wi, phi, Uo, Vo, Wo, Pint, 1.0 / dt, dup_plane ? 1 : 0);
   C3D_LAUNCH_CHECK(h);
   return 0;
 }
@@ -1087,7 +1091,7 @@ int launch_projection_step(Handle* h, int rk_step, double dt) {
                                (stage1 && sweeps == 0) ? h->phi1 : nullptr, 0, 7);
     if (rc) return rc;
     for (int sw = 1; sw <= sweeps; ++sw) {
-      rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W);
+      rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W, false);
       if (rc) return rc;
       rc = launch_fill_ghosts3(h, h->U, h->V, h->W);
       if (rc) return rc;
@@ -1102,7 +1106,7 @@ int launch_projection_step(Handle* h, int rk_step, double dt) {
     if (rc) return rc;
   }
   if (stage1) { h->P_pending = true; h->P_pending_dt = dt; }
-  rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W);
+  rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W, false);
   if (rc) return rc;
   return launch_fill_ghosts3(h, h->U, h->V, h->W);
 }
