@@ -1066,6 +1066,52 @@ __global__ void __launch_bounds__(256, 6) k_grad_sub(Dims d, Metric m, const dou
   }
 }
 
+// The same update for two cells (k, k+1) per thread, without the duplicate
+// plane and P_interim (the time step's case): both cells' loads are issued
+// before any store, and phi(k+1) serves both.
+__global__ void __launch_bounds__(256, 4) k_grad_sub2(Dims d, Metric m, const double* __restrict__ Ui,
+                                                   const double* __restrict__ Vi,
+                                                   const double* __restrict__ Wi,
+                                                   const double* __restrict__ phi,
+                                                   double* __restrict__ Uo, double* __restrict__ Vo,
+                                                   double* __restrict__ Wo) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = 2 + 2 * (int)blockIdx.z;
+  if (i > d.Nx + 1 || j > d.Ny + 1) return;
+  const bool two = k + 1 <= d.Nz + 1;
+  const bool hv = j <= d.Ny;
+  const int64_t pr = idxR(d, i, j, k), plr = (int64_t)(d.nxg - 2) * (d.nyg - 2);
+  const int64_t iu = idxU(d, i, j, k), iv = idxV(d, i, j, k), iw = idxW(d, i, j, k);
+  const int64_t plu = (int64_t)d.nx * d.nyg, plv = (int64_t)d.nxg * d.ny, plw = (int64_t)d.nxg * d.nyg;
+  const double p0 = __ldg(phi + pr), px = __ldg(phi + pr + 1), p1 = __ldg(phi + pr + plr);
+  const double u0 = __ldg(Ui + iu), w0 = __ldg(Wi + iw);
+  double py = 0.0, v0 = 0.0, p1x = 0.0, p2 = 0.0, u1 = 0.0, w1 = 0.0, p1y = 0.0, v1 = 0.0;
+  if (hv) {
+    py = __ldg(phi + pr + (d.nxg - 2));
+    v0 = __ldg(Vi + iv);
+  }
+  if (two) {
+    p1x = __ldg(phi + pr + plr + 1);
+    p2 = __ldg(phi + pr + 2 * plr);
+    u1 = __ldg(Ui + iu + plu);
+    w1 = __ldg(Wi + iw + plw);
+    if (hv) {
+      p1y = __ldg(phi + pr + plr + (d.nxg - 2));
+      v1 = __ldg(Vi + iv + plv);
+    }
+  }
+  const double rx = m.rdxg[i], ry = m.rdyg[j];
+  Uo[iu] = u0 - (px - p0) * rx;
+  Wo[iw] = w0 - (p1 - p0) * m.rdzg[k];
+  if (hv) Vo[iv] = v0 - (py - p0) * ry;
+  if (two) {
+    Uo[iu + plu] = u1 - (p1x - p1) * rx;
+    Wo[iw + plw] = w1 - (p2 - p1) * m.rdzg[k + 1];
+    if (hv) Vo[iv + plv] = v1 - (p1y - p1) * ry;
+  }
+}
+
 int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, const double* Wi,
                              const double* phi, double dt, double* Uo, double* Vo, double* Wo,
                              bool dup_plane) {
@@ -1073,6 +1119,12 @@ int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, cons
   dim3 b(32, 4, 2);
   dim3 g((d.Nx + 31) / 32, (d.Ny + 3) / 4, (d.Nz + 1) / 2);
   double* Pint = (h->ib != nullptr || h->write_pinterim) ? h->P_interim : nullptr;
+  if (!dup_plane && !Pint) {
+    const dim3 b2(32, 8, 1), g2((d.Nx + 31) / 32, (d.Ny + 7) / 8, (d.Nz + 1) / 2);
+    k_grad_sub2<<<g2, b2, 0, h->stream>>>(d, h->m, Ui, Vi, Wi, phi, Uo, Vo, Wo);
+    C3D_LAUNCH_CHECK(h);
+    return 0;
+  }
   k_grad_sub<<<g, b, 0, h->stream>>>(d, h->m, Ui, Vi, Wi, phi, Uo, Vo, Wo, Pint, 1.0 / dt, dup_plane ? 1 : 0);
   C3D_LAUNCH_CHECK(h);
   return 0;
