@@ -90,6 +90,7 @@ struct DevScalars {
 struct SpectralState {
   double2 *twx = nullptr, *twz = nullptr;    // exp(-2 pi i m / n) (device)
   float2 *twx32 = nullptr, *twz32 = nullptr;
+  int* posx = nullptr;                       // digit-reversed position of x coefficient m
   // Thomas factors of every (kx, kz') mode, layout [(m*Ny + j)*nkzs + kz']:
   // multipliers DL(j)/D'(j) and reciprocal pivots 1/D'(j)
   double *mult = nullptr, *rdp = nullptr;

@@ -156,6 +156,7 @@ struct XfwdArgs {
   typename cplx<T>::t* __restrict__ spec;
   const typename cplx<T>::t* __restrict__ tw;
   double* __restrict__ linesum;               // FP64 line sums (mixed path) or null
+  const int* __restrict__ pos;                // digit-reversed position of coefficient m
   FftPasses P;
   int pz;                                     // spectrum row pitch
   int rs;                                     // shared-memory row stride
@@ -195,51 +196,76 @@ template <bool FROM_DIV, typename T>
 __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
   using C = typename cplx<T>::t;
   extern __shared__ __align__(16) unsigned char xf_smem[];
-  __shared__ int s_j[2 * kLinesX], s_k[2 * kLinesX], s_off[2 * kLinesX];
+  __shared__ int s_j[2 * kLinesX], s_off[2 * kLinesX];
+  // per real line: offsets of the x = 2 cell of u(j,k), v(j,k), v(j-1,k),
+  // w(j,k), w(j,k-1) (FROM_DIV) or of the right-hand side; -1: a zero wall
+  // value of v (j-1 = 1 or j = ny), or no line
+  __shared__ int64_t s_bu[2 * kLinesX], s_bv[2 * kLinesX], s_bvm[2 * kLinesX];
+  __shared__ int64_t s_bw[2 * kLinesX], s_bwm[2 * kLinesX];
+  __shared__ double s_ry[2 * kLinesX], s_rz[2 * kLinesX];
   const Dims& d = a.d;
   const int N = d.Nx, RS = a.rs;
   const int tid = threadIdx.x, nt = blockDim.x;
   XfftSmem<T> sm = xfft_carve<T>(xf_smem, N, RS);
   for (int t = tid; t < N; t += nt) {
     sm.tw[t] = a.tw[t];
-    sm.pos[t] = dif_k_to_position(t, a.P);
+    sm.pos[t] = a.pos[t];
   }
   const int64_t nreal = a.rbase + a.nlines;
   const int64_t r0 = a.rbase + (int64_t)blockIdx.x * kLinesX * 2;
   if (tid < 2 * kLinesX) {
     const int64_t r = r0 + tid;
     int j = -1, k = -1, off = 0;
-    if (r < nreal) line_info(d, a.pz, r, &j, &k, &off);
+    int64_t bu = -1, bv = -1, bvm = -1, bw = 0, bwm = 0;
+    double ry = 0.0, rz = 0.0;
+    if (r < nreal) {
+      line_info(d, a.pz, r, &j, &k, &off);
+      if (FROM_DIV) {
+        // the ghost values are read as the boundary conditions define them
+        // (periodic images in x and z, zero V walls), so the fields need no
+        // ghost fill after the stage update
+        const int64_t plw = (int64_t)d.nxg * d.nyg;
+        const int64_t iv = idxV(d, 2, j, k), iw = idxW(d, 2, j, k);
+        bu = idxU(d, 2, j, k);
+        bv = j == d.ny ? -1 : iv;
+        bvm = j == 2 ? -1 : iv - d.nxg;
+        bw = iw;
+        bwm = k == 2 ? iw + (int64_t)(d.Nz - 1) * plw : iw - plw;
+        ry = a.m.rdy[j];
+        rz = a.m.rdz[k];
+      } else {
+        bu = idxR(d, 2, j, k);
+      }
+    }
     s_j[tid] = j;
-    s_k[tid] = k;
     s_off[tid] = off;
+    s_bu[tid] = bu; s_bv[tid] = bv; s_bvm[tid] = bvm; s_bw[tid] = bw; s_bwm[tid] = bwm;
+    s_ry[tid] = ry; s_rz[tid] = rz;
   }
   __syncthreads();
   // nt is a multiple of N: thread -> x index ii, real lines rl0, rl0 + nt/N, ...
-  // taken four at a time: all loads of a batch are issued before any use
+  // taken four at a time: all loads of a batch are issued before any use.
+  // u(i-1) of i = 2 is the periodic image i = N+1.
   const int ii = tid % N, rls = nt / N;
-  const int i = 2 + ii;
-  const double rdx_i = FROM_DIV ? a.m.rdx[i] : 0.0;
+  const int xo = ii == 0 ? N - 1 : ii - 1;
+  const double rdx_i = FROM_DIV ? a.m.rdx[2 + ii] : 0.0;
   constexpr int kBatch = 4;
   for (int rb = tid / N; rb < 2 * kLinesX; rb += kBatch * rls) {
     double x0[kBatch], x1[kBatch], y0[kBatch], y1[kBatch], z0[kBatch], z1[kBatch];
 #pragma unroll
     for (int q = 0; q < kBatch; ++q) {
       const int rl = rb + q * rls;
-      const int j = rl < 2 * kLinesX ? s_j[rl] : -1, k = rl < 2 * kLinesX ? s_k[rl] : -1;
+      const int64_t bu = rl < 2 * kLinesX ? s_bu[rl] : -1;
       x0[q] = x1[q] = y0[q] = y1[q] = z0[q] = z1[q] = 0.0;
-      if (j > 0) {
+      if (bu >= 0) {
         if (FROM_DIV) {
-          // the ghost values are read as the boundary conditions define them
-          // (periodic images in x and z, zero V walls), so the fields need
-          // no ghost fill after the stage update
-          const int64_t iu = idxU(d, i, j, k), iv = idxV(d, i, j, k), iw = idxW(d, i, j, k);
-          const int64_t plw = (int64_t)d.nxg * d.nyg;
-          x1[q] = a.U[iu]; x0[q] = a.U[i == 2 ? iu + (N - 1) : iu - 1];
-          y1[q] = j == d.ny ? 0.0 : a.V[iv]; y0[q] = j == 2 ? 0.0 : a.V[iv - d.nxg];
-          z1[q] = a.W[iw]; z0[q] = a.W[k == 2 ? iw + (int64_t)(d.Nz - 1) * plw : iw - plw];
+          const int64_t bv = s_bv[rl], bvm = s_bvm[rl];
+          x1[q] = a.U[bu + ii]; x0[q] = a.U[bu + xo];
+          if (bv >= 0) y1[q] = a.V[bv + ii];
+          if (bvm >= 0) y0[q] = a.V[bvm + ii];
+          z1[q] = a.W[s_bw[rl] + ii]; z0[q] = a.W[s_bwm[rl] + ii];
         } else {
-          x1[q] = a.rhs[idxR(d, i, j, k)];
+          x1[q] = a.rhs[bu + ii];
         }
       }
     }
@@ -247,11 +273,8 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
     for (int q = 0; q < kBatch; ++q) {
       const int rl = rb + q * rls;
       if (rl >= 2 * kLinesX) continue;
-      const int j = s_j[rl], k = s_k[rl];
-      double val = 0.0;
-      if (j > 0)
-        val = FROM_DIV ? (x1[q] - x0[q]) * rdx_i + (y1[q] - y0[q]) * a.m.rdy[j] + (z1[q] - z0[q]) * a.m.rdz[k]
-                       : x1[q];
+      const double val = FROM_DIV ? (x1[q] - x0[q]) * rdx_i + (y1[q] - y0[q]) * s_ry[rl] + (z1[q] - z0[q]) * s_rz[rl]
+                                  : x1[q];
       C& zz = sm.buf[(rl >> 1) * RS + ii];
       if (rl & 1) zz.y = (T)val; else zz.x = (T)val;
       if (a.linesum) sm.sval[rl * N + ii] = val;
@@ -641,6 +664,7 @@ struct XinvArgs {
   double* __restrict__ phi1;     // optional second copy (P side effect)
   const double* __restrict__ phi00;   // FP64 mean mode added to the output (mixed path)
   int accumulate;                // 1: rhs += result (refinement)
+  const int* __restrict__ pos;   // digit-reversed position of coefficient m
   FftPasses P;
   int pz;                        // spectrum row pitch
   int rs;                        // shared-memory row stride
@@ -652,24 +676,33 @@ template <typename T>
 __global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
   using C = typename cplx<T>::t;
   extern __shared__ __align__(16) unsigned char xi_smem[];
-  __shared__ int s_j[2 * kLinesX], s_k[2 * kLinesX], s_off[2 * kLinesX];
+  __shared__ int s_j[2 * kLinesX], s_off[2 * kLinesX];
+  // per real line: offset of the x = 2 value of phi(j,k), and of phi(j,nzp+2)
+  // for the plane k = 2 that the reference duplicates (else -1)
+  __shared__ int64_t s_bo[2 * kLinesX], s_bo2[2 * kLinesX];
   const Dims& d = a.d;
   const int N = d.Nx, nk = d.nkx, RS = a.rs;
   const int tid = threadIdx.x, nt = blockDim.x;
   XfftSmem<T> sm = xfft_carve<T>(xi_smem, N, RS);
   for (int t = tid; t < N; t += nt) {
     sm.tw[t] = a.tw[t];
-    sm.pos[t] = dif_k_to_position(t, a.P);
+    sm.pos[t] = a.pos[t];
   }
   const int64_t nreal = a.rbase + a.nlines;
   const int64_t r0 = a.rbase + (int64_t)blockIdx.x * kLinesX * 2;
   if (tid < 2 * kLinesX) {
     const int64_t r = r0 + tid;
     int j = -1, k = -1, off = 0;
-    if (r < nreal) line_info(d, a.pz, r, &j, &k, &off);
+    int64_t bo = -1, bo2 = -1;
+    if (r < nreal) {
+      line_info(d, a.pz, r, &j, &k, &off);
+      bo = idxR(d, 2, j, k);
+      if (k == 2) bo2 = idxR(d, 2, j, d.Nz + 2);
+    }
     s_j[tid] = j;
-    s_k[tid] = k;
     s_off[tid] = off;
+    s_bo[tid] = bo;
+    s_bo2[tid] = bo2;
   }
   __syncthreads();
   // Z = A + iB on the full circle from the two half spectra, placed at the
@@ -698,30 +731,29 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
   fft_rows_dit_inv<T, 1>(sm.buf, kLinesX, RS, sm.tw, a.P, 128 / (int)sizeof(C));
   const double rsd = a.inv_scale;
   const int ii = tid % N, rls = nt / N;
-  const int i = 2 + ii;
+  // apply_periodic_xz_centers (src/poisson.f90:106-125): x plane nxg-1 and
+  // z plane nzp+2 duplicate plane 2
 #pragma unroll 4
   for (int rl = tid / N; rl < 2 * kLinesX; rl += rls) {
-    const int j = s_j[rl], k = s_k[rl];
-    if (j < 0) continue;
+    const int64_t bo = s_bo[rl], bo2 = s_bo2[rl];
+    if (bo < 0) continue;
     const C z = sm.buf[(rl >> 1) * RS + ii];
     double v = (double)((rl & 1) ? z.y : z.x) * rsd;
-    if (a.phi00) v += a.phi00[j - 2];
-    const int64_t o = idxR(d, i, j, k);
+    if (a.phi00) v += a.phi00[s_j[rl] - 2];
+    const int64_t o = bo + ii;
     if (a.accumulate) v += a.rhs[o];
-    // apply_periodic_xz_centers (src/poisson.f90:106-125): x plane nxg-1 and
-    // z plane nzp+2 duplicate plane 2
     a.rhs[o] = v;
-    if (i == 2) a.rhs[idxR(d, d.Nx + 2, j, k)] = v;
-    if (k == 2) {
-      a.rhs[idxR(d, i, j, d.Nz + 2)] = v;
-      if (i == 2) a.rhs[idxR(d, d.Nx + 2, j, d.Nz + 2)] = v;
+    if (ii == 0) a.rhs[bo + N] = v;
+    if (bo2 >= 0) {
+      a.rhs[bo2 + ii] = v;
+      if (ii == 0) a.rhs[bo2 + N] = v;
     }
     if (a.phi1) {
       a.phi1[o] = v;
-      if (i == 2) a.phi1[idxR(d, d.Nx + 2, j, k)] = v;
-      if (k == 2) {
-        a.phi1[idxR(d, i, j, d.Nz + 2)] = v;
-        if (i == 2) a.phi1[idxR(d, d.Nx + 2, j, d.Nz + 2)] = v;
+      if (ii == 0) a.phi1[bo + N] = v;
+      if (bo2 >= 0) {
+        a.phi1[bo2 + ii] = v;
+        if (ii == 0) a.phi1[bo2 + N] = v;
       }
     }
   }
@@ -929,6 +961,7 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     a.d = d; a.m = h->m; a.U = U; a.V = V; a.W = W; a.rhs = rhs_in;
     a.spec = spec; a.tw = twx; a.P = Px; a.pz = pz; a.rs = rsx; a.rbase = rbase; a.nlines = nlines;
     a.linesum = f32 ? S.linesum : nullptr;
+    a.pos = S.posx;
     if (from_div) k_xfft_fwd<true, T><<<nbx, ntx, smx, s>>>(a);
     else k_xfft_fwd<false, T><<<nbx, ntx, smx, s>>>(a);
     C3D_LAUNCH_CHECK(h);
@@ -945,6 +978,7 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     XinvArgs<T> a{};
     a.d = d; a.spec = spec; a.tw = twx; a.rhs = out; a.phi1 = phi1;
     a.phi00 = f32 ? S.phi00 : nullptr; a.accumulate = accumulate;
+    a.pos = S.posx;
     a.P = Px; a.pz = pz; a.rs = rsx; a.rbase = rbase; a.nlines = nlines;
     a.inv_scale = 1.0 / ((double)d.Nx * (double)d.Nz);
     k_xfft_inv<T><<<nbx, ntx, smx, s>>>(a);
@@ -1216,6 +1250,13 @@ int poisson_setup(Handle* h) {
     }
     if ((rc = make_twiddles(h, d.Nx, &S.twx))) return rc;
     if ((rc = make_twiddles(h, d.Nz, &S.twz))) return rc;
+    {
+      const FftPasses Px = get_passes(d.Nx);
+      std::vector<int> pos(d.Nx);
+      for (int m = 0; m < d.Nx; ++m) pos[m] = dif_k_to_position(m, Px);
+      if ((rc = dev_alloc(h, &S.posx, d.Nx))) return rc;
+      C3D_CUDA_TRY(h, cudaMemcpy(S.posx, pos.data(), sizeof(int) * d.Nx, cudaMemcpyHostToDevice));
+    }
     const int64_t ns = (int64_t)d.Ny * S.pz64 * d.nkx;
     if ((rc = dev_alloc(h, &S.spec, ns))) return rc;
     if ((rc = set_limits<double>(h, S.smem64, S.cs64))) return rc;
