@@ -43,19 +43,18 @@ namespace c3d {
 // ---------------------------------------------------------------------------
 // host set-up
 // ---------------------------------------------------------------------------
-static bool make_passes(int n, FftPasses& P) {
-  P.n = n;
-  P.npass = 0;
-  int m = n;
-  while (m % 4 == 0 && P.npass < 8) { P.radix[P.npass++] = 4; m /= 4; }
-  while (m % 2 == 0 && P.npass < 8) { P.radix[P.npass++] = 2; m /= 2; }
-  while (m % 3 == 0 && P.npass < 8) { P.radix[P.npass++] = 3; m /= 3; }
-  return m == 1 && n >= 2;
-}
+// largest FFT radix compiled into the x-FFT kernels and the two slab shapes
+// (register budgets: 64-96 registers for the x kernels and the narrow slab
+// CTAs, 128 for the wide ones)
+constexpr int kXMaxR = 8;
+constexpr int kYzMaxRWide = 16;
+constexpr int kYzMaxRNarrow = 8;
 
-static FftPasses get_passes(int n) {
+static bool make_passes(int n, FftPasses& P) { return make_fft_passes(n, P, 8); }
+
+static FftPasses get_passes(int n, int maxr) {
   FftPasses P{};
-  make_passes(n, P);
+  make_fft_passes(n, P, maxr);
   return P;
 }
 
@@ -289,7 +288,7 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
       a.linesum[r] = sum;
     }
   }
-  fft_rows_dif<T, 1>(sm.buf, kLinesX, RS, sm.tw, a.P, 128 / (int)sizeof(C));
+  fft_rows_dif<T, kXMaxR>(sm.buf, kLinesX, RS, sm.tw, a.P);
   // split Z = A + iB of the two real lines: A = (Z_m + conj Z_{N-m})/2,
   // B = (Z_m - conj Z_{N-m})/(2i), m = 0..N/2
   const int nk = d.nkx;
@@ -358,8 +357,6 @@ template <typename T, bool NARROW>
 __global__ void __launch_bounds__(yz_threads<NARROW>(), yz_min_blocks<NARROW>()) k_spectral_yz(YzArgs<T> a) {
   using C = typename cplx<T>::t;
   constexpr int JM = yz_jmax<T, NARROW>();
-  constexpr int kYzB = 4;   // FFT rows per batch
-  constexpr int kRun = 128 / (int)sizeof(C);   // q-runs that fill a shared-memory wavefront
   extern __shared__ __align__(128) unsigned char yz_smem[];
   __shared__ __align__(8) uint64_t bar;
   cg::cluster_group cl = cg::this_cluster();
@@ -407,7 +404,7 @@ __global__ void __launch_bounds__(yz_threads<NARROW>(), yz_min_blocks<NARROW>())
   if (!loaded) atomicOr(a.err, 1ull);
   __syncthreads();
 
-  fft_rows_dif<T, kYzB>(data + (size_t)blo * RS, bhi - blo, RS, tw, a.P, kRun);
+  fft_rows_dif<T, (NARROW ? kYzMaxRNarrow : kYzMaxRWide)>(data + (size_t)blo * RS, bhi - blo, RS, tw, a.P);
 
   // pivots of this thread's column for rows j0-1 .. j0+jn-1 (one column per
   // thread when Nz <= blockDim; otherwise reloaded per column below)
@@ -605,7 +602,7 @@ __global__ void __launch_bounds__(yz_threads<NARROW>(), yz_min_blocks<NARROW>())
   }
   __syncthreads();
 
-  fft_rows_dit_inv<T, kYzB>(data + (size_t)blo * RS, bhi - blo, RS, tw, a.P, kRun);
+  fft_rows_dit_inv<T, (NARROW ? kYzMaxRNarrow : kYzMaxRWide)>(data + (size_t)blo * RS, bhi - blo, RS, tw, a.P);
   // no CTA leaves while another may still read its ylast / xfirst
   cl.sync();
 
@@ -728,7 +725,7 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
     }
   }
   __syncthreads();
-  fft_rows_dit_inv<T, 1>(sm.buf, kLinesX, RS, sm.tw, a.P, 128 / (int)sizeof(C));
+  fft_rows_dit_inv<T, kXMaxR>(sm.buf, kLinesX, RS, sm.tw, a.P);
   const double rsd = a.inv_scale;
   const int ii = tid % N, rls = nt / N;
   // apply_periodic_xz_centers (src/poisson.f90:106-125): x plane nxg-1 and
@@ -889,7 +886,7 @@ static int launch_yz(Handle* h, typename cplx<T>::t* spec, const typename cplx<T
   YzArgs<T> a{};
   a.d = d; a.spec = spec; a.tw = tw; a.rdp = rdp; a.dl = dl; a.du = du;
   a.err = &h->sc->err;
-  a.P = get_passes(d.Nz); a.cs = cs; a.jc = jc; a.rs = rs; a.pz = pz; a.zero00 = zero00;
+  a.P = get_passes(d.Nz, narrow ? kYzMaxRNarrow : kYzMaxRWide); a.cs = cs; a.jc = jc; a.rs = rs; a.pz = pz; a.zero00 = zero00;
   a.rlo = rlo; a.rhi = rhi;
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)(cs * d.nkx), 1, 1);
@@ -948,7 +945,7 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     rdp = (const T*)S.rdp; dl = (const T*)S.dl; du = (const T*)S.du;
     cs = S.cs64; jc = S.jc64; rs = S.rs64; pz = S.pz64; nt = S.nt64; smem = S.smem64; narrow = S.nw64;
   }
-  const FftPasses Px = get_passes(d.Nx);
+  const FftPasses Px = get_passes(d.Nx, kXMaxR);
   if (bhi < 0) bhi = d.Ny - 1;                 // band of j rows (0-based j-2); full by default
   const int64_t rbase = (int64_t)blo * d.Nz, nlines = (int64_t)(bhi - blo + 1) * d.Nz;
   const int64_t npairs = (nlines + 1) / 2;
@@ -1251,7 +1248,7 @@ int poisson_setup(Handle* h) {
     if ((rc = make_twiddles(h, d.Nx, &S.twx))) return rc;
     if ((rc = make_twiddles(h, d.Nz, &S.twz))) return rc;
     {
-      const FftPasses Px = get_passes(d.Nx);
+      const FftPasses Px = get_passes(d.Nx, kXMaxR);
       std::vector<int> pos(d.Nx);
       for (int m = 0; m < d.Nx; ++m) pos[m] = dif_k_to_position(m, Px);
       if ((rc = dev_alloc(h, &S.posx, d.Nx))) return rc;

@@ -1,0 +1,13 @@
+// Host stand-in for the few CUDA names the shared-memory FFT header uses, so
+// that its stages can run on the CPU with one thread doing every butterfly
+// (a stage's butterflies touch disjoint elements, so sequential order is
+// valid and the barrier is a no-op).
+#pragma once
+#define __device__
+#define __host__
+#define __forceinline__ inline
+struct double2 { double x, y; };
+struct float2 { float x, y; };
+struct HostDim3 { unsigned x, y, z; };
+static HostDim3 threadIdx{0, 0, 0}, blockDim{1, 1, 1};
+inline void __syncthreads() {}
