@@ -960,7 +960,7 @@ int c3d_profile_kernels(int id, int nrep, double* ms, int nmax) {
         case 0: rc = launch_rhs_stage(h, 2, dt); break;
         case 1: rc = launch_fill_ghosts3(h, h->Us, h->Vs, h->Ws); break;
         case 2: case 3: case 4: rc = profile_spectral(h, c - 2); break;
-        case 5: rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W, false); break;
+        case 5: rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W, false, true); break;
         case 6: rc = launch_massflow_correction(h, dt); break;
       }
       if (rc) RET(h, rc);

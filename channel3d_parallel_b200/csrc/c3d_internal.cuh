@@ -248,7 +248,7 @@ int launch_poisson_of_div_band(Handle* h, const double* U, const double* V, cons
 int launch_projection_step(Handle* h, int rk_step, double dt);
 int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, const double* Wi,
                              const double* phi, double dt, double* Uo, double* Vo, double* Wo,
-                             bool dup_plane = true);
+                             bool dup_plane = true, bool with_ghosts = false);
 int rebuild_pressure(Handle* h);
 int compute_pressure(Handle* h);
 int profile_spectral(Handle* h, int part);   // 0 div_xfft, 1 spectral_yz, 2 xfft inv

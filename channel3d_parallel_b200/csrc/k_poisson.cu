@@ -1097,15 +1097,54 @@ __global__ void __launch_bounds__(256, 6) k_grad_sub(Dims d, Metric m, const dou
   }
 }
 
+// Ghost entries written by the thread that owns their source point
+// (apply_boundary_conditions, src/boundary_conditions.f90:20-55): every
+// ghost entry of a field of extents n1 x n2 x n3 is sign * F(fold(i), mapy(j),
+// fold(k)) of one interior point, with the periodic folds 1 <- N+1,
+// N+2 <- 2, N+3 <- 3 in x and z, and in y the odd reflections j = 1 <- -F(2),
+// j = n2 <- -F(n2-1) (cell-centred y) or zero wall values (y faces, V).
+// x images of interior index i in a field of x extent n1 (0: none)
+struct XImages {
+  int a, b;
+};
+__device__ __forceinline__ XImages x_images(int i, int Nx, int n1) {
+  return XImages{i == Nx + 1 ? 1 : 0, i + Nx <= n1 ? i + Nx : 0};
+}
+// row1: the entry x = 1 of the row
+__device__ __forceinline__ void put_row(double* __restrict__ row1, int i, XImages xi, double v) {
+  row1[i - 1] = v;
+  if (xi.a) row1[0] = v;
+  if (xi.b) row1[xi.b - 1] = v;
+}
+// v at interior point (i, j, k) and every ghost entry whose source it is
+__device__ __noinline__ void put_images_all(double* __restrict__ F, int n1, int n2, int n3, int Nx, int Nz,
+                                            bool yface, int i, int j, int k, double v) {
+  const XImages xi = x_images(i, Nx, n1);
+  const int za = k == Nz + 1 ? 1 : 0, zb = k + Nz <= n3 ? k + Nz : 0;
+  const int ja = yface ? 0 : (j == 2 ? 1 : (j == n2 - 1 ? n2 : 0));
+  auto row = [&](int jj, int kk) { return F + (int64_t)n1 * ((jj - 1) + (int64_t)n2 * (kk - 1)); };
+  put_row(row(j, k), i, xi, v);
+  if (za) put_row(row(j, za), i, xi, v);
+  if (zb) put_row(row(j, zb), i, xi, v);
+  if (ja) {
+    put_row(row(ja, k), i, xi, -v);
+    if (za) put_row(row(ja, za), i, xi, -v);
+    if (zb) put_row(row(ja, zb), i, xi, -v);
+  }
+}
+
 // The same update for two cells (k, k+1) per thread, without the duplicate
 // plane and P_interim (the time step's case): both cells' loads are issued
-// before any store, and phi(k+1) serves both.
+// before any store, and phi(k+1) serves both.  With ghosts = 1 every ghost
+// entry of the results is written as well (the boundary conditions of the
+// projected field): the x images by the threads of the boundary columns,
+// the z and y images (whole blocks and warps) out of line.
 __global__ void __launch_bounds__(256, 4) k_grad_sub2(Dims d, Metric m, const double* __restrict__ Ui,
                                                    const double* __restrict__ Vi,
                                                    const double* __restrict__ Wi,
                                                    const double* __restrict__ phi,
                                                    double* __restrict__ Uo, double* __restrict__ Vo,
-                                                   double* __restrict__ Wo) {
+                                                   double* __restrict__ Wo, int ghosts) {
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 2 + 2 * (int)blockIdx.z;
@@ -1133,32 +1172,59 @@ __global__ void __launch_bounds__(256, 4) k_grad_sub2(Dims d, Metric m, const do
     }
   }
   const double rx = m.rdxg[i], ry = m.rdyg[j];
-  Uo[iu] = u0 - (px - p0) * rx;
-  Wo[iw] = w0 - (p1 - p0) * m.rdzg[k];
-  if (hv) Vo[iv] = v0 - (py - p0) * ry;
-  if (two) {
-    Uo[iu + plu] = u1 - (p1x - p1) * rx;
-    Wo[iw + plw] = w1 - (p2 - p1) * m.rdzg[k + 1];
-    if (hv) Vo[iv + plv] = v1 - (p1y - p1) * ry;
+  const double un0 = u0 - (px - p0) * rx, wn0 = w0 - (p1 - p0) * m.rdzg[k], vn0 = v0 - (py - p0) * ry;
+  const double un1 = u1 - (p1x - p1) * rx, wn1 = w1 - (p2 - p1) * m.rdzg[k + 1], vn1 = v1 - (p1y - p1) * ry;
+  if (!ghosts) {
+    Uo[iu] = un0;
+    Wo[iw] = wn0;
+    if (hv) Vo[iv] = vn0;
+    if (two) {
+      Uo[iu + plu] = un1;
+      Wo[iw + plw] = wn1;
+      if (hv) Vo[iv + plv] = vn1;
+    }
+    return;
+  }
+  // cells k (c = 0) and k+1 (c = 1)
+  const bool yu = j == 2 || j == d.nyg - 1;                 // u, w: odd y reflections
+  const bool yv = j == 2 || j == d.Ny;                      // v: next to a zero wall
+  const XImages xu = x_images(i, d.Nx, d.nx), xw = x_images(i, d.Nx, d.nxg);
+  for (int c = 0; c <= (two ? 1 : 0); ++c) {
+    const int kc = k + c;
+    const double un = c ? un1 : un0, wn = c ? wn1 : wn0, vn = c ? vn1 : vn0;
+    const int64_t ou = iu + c * plu, ow = iw + c * plw, ov = iv + c * plv;
+    if (yu || kc == d.Nz + 1 || kc + d.Nz <= d.nzg) put_images_all(Uo, d.nx, d.nyg, d.nzg, d.Nx, d.Nz, false, i, j, kc, un);
+    else put_row(Uo + ou - (i - 1), i, xu, un);
+    if (yu || kc == d.Nz + 1 || kc + d.Nz <= d.nz) put_images_all(Wo, d.nxg, d.nyg, d.nz, d.Nx, d.Nz, false, i, j, kc, wn);
+    else put_row(Wo + ow - (i - 1), i, xw, wn);
+    if (hv) {
+      if (yv || kc == d.Nz + 1 || kc + d.Nz <= d.nzg) {
+        put_images_all(Vo, d.nxg, d.ny, d.nzg, d.Nx, d.Nz, true, i, j, kc, vn);
+        if (j == 2) put_images_all(Vo, d.nxg, d.ny, d.nzg, d.Nx, d.Nz, true, i, 1, kc, 0.0);
+        if (j == d.Ny) put_images_all(Vo, d.nxg, d.ny, d.nzg, d.Nx, d.Nz, true, i, d.ny, kc, 0.0);
+      } else {
+        put_row(Vo + ov - (i - 1), i, xw, vn);
+      }
+    }
   }
 }
 
 int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, const double* Wi,
                              const double* phi, double dt, double* Uo, double* Vo, double* Wo,
-                             bool dup_plane) {
+                             bool dup_plane, bool with_ghosts) {
   const Dims& d = h->d;
   dim3 b(32, 4, 2);
   dim3 g((d.Nx + 31) / 32, (d.Ny + 3) / 4, (d.Nz + 1) / 2);
   double* Pint = (h->ib != nullptr || h->write_pinterim) ? h->P_interim : nullptr;
   if (!dup_plane && !Pint) {
     const dim3 b2(32, 8, 1), g2((d.Nx + 31) / 32, (d.Ny + 7) / 8, (d.Nz + 1) / 2);
-    k_grad_sub2<<<g2, b2, 0, h->stream>>>(d, h->m, Ui, Vi, Wi, phi, Uo, Vo, Wo);
+    k_grad_sub2<<<g2, b2, 0, h->stream>>>(d, h->m, Ui, Vi, Wi, phi, Uo, Vo, Wo, with_ghosts ? 1 : 0);
     C3D_LAUNCH_CHECK(h);
     return 0;
   }
   k_grad_sub<<<g, b, 0, h->stream>>>(d, h->m, Ui, Vi, Wi, phi, Uo, Vo, Wo, Pint, 1.0 / dt, dup_plane ? 1 : 0);
   C3D_LAUNCH_CHECK(h);
-  return 0;
+  return with_ghosts ? launch_fill_ghosts3(h, Uo, Vo, Wo) : 0;
 }
 
 // compute_non_IB_projection with U* in (Us,Vs,Ws) and the result in (U,V,W),
@@ -1174,9 +1240,7 @@ int launch_projection_step(Handle* h, int rk_step, double dt) {
                                (stage1 && sweeps == 0) ? h->phi1 : nullptr, 0, 7);
     if (rc) return rc;
     for (int sw = 1; sw <= sweeps; ++sw) {
-      rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W, false);
-      if (rc) return rc;
-      rc = launch_fill_ghosts3(h, h->U, h->V, h->W);
+      rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W, false, true);
       if (rc) return rc;
       rc = run_spectral_t<float>(h, true, h->U, h->V, h->W, nullptr, h->rhs_p,
                                  (stage1 && sw == sweeps) ? h->phi1 : nullptr, 1, 7);
@@ -1189,9 +1253,8 @@ int launch_projection_step(Handle* h, int rk_step, double dt) {
     if (rc) return rc;
   }
   if (stage1) { h->P_pending = true; h->P_pending_dt = dt; }
-  rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W, false);
-  if (rc) return rc;
-  return launch_fill_ghosts3(h, h->U, h->V, h->W);
+  // the projected fields with all their ghost entries
+  return launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W, false, true);
 }
 
 // P = phi1/(dt*rk_coef(1,1)) with the copies of src/poisson.f90:92-98
