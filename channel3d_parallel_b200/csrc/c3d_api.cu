@@ -214,6 +214,18 @@ static int setup_metric(Handle* h, const double* xf, const double* yf, const dou
   }
   for (int j = 3; j <= nyg - 1; ++j) wq[j] = 0.5 * (yg[j] - yg[j - 1]);
   for (int j = 2; j <= ny; ++j) wqv[j] = 0.5 * (y[j] - y[j - 1]);
+  std::vector<double> cqu(LY, 0);
+  for (int j = 2; j <= nyg - 1; ++j) cqu[j] = wq[j] + wq[j + 1];
+  {
+    // norm of compute_mean_mass_flow_U (src/mass_flow.f90:24-53): rows
+    // j = 3..nyg-1 and k = 2..nzg-1, nx-2 points each, weight 2 wq(j)
+    double sw = 0.0;
+    for (int j = 3; j <= nyg - 1; ++j) sw += 2.0 * wq[j];
+    h->norm_u = sw * (double)(nx - 2) * (double)(nzg - 2);
+    double dev = 0.0;
+    for (int i = 2; i <= nx - 1; ++i) dev = std::max(dev, std::fabs(rdxg[i] - rdxg[2]));
+    h->x_uniform = dev <= 1e-9 * std::fabs(rdxg[2]);
+  }
   std::vector<double> rdz(LZ, 0), rdzg(LZ, 0), czpC(LZ, 0), czmC(LZ, 0), czpF(LZ, 0), czmF(LZ, 0);
   for (int k = 2; k <= nz; ++k) rdz[k] = 1.0 / (z[k] - z[k - 1]);
   for (int k = 1; k <= nzg - 1; ++k) rdzg[k] = 1.0 / (zg[k + 1] - zg[k]);
@@ -229,7 +241,7 @@ static int setup_metric(Handle* h, const double* xf, const double* yf, const dou
   add(rdx, &m.rdx); add(rdxg, &m.rdxg); add(cxpF, &m.cxpF); add(cxmF, &m.cxmF);
   add(cxpC, &m.cxpC); add(cxmC, &m.cxmC);
   add(rdy, &m.rdy); add(rdyg, &m.rdyg); add(cypC, &m.cypC); add(cymC, &m.cymC);
-  add(cypF, &m.cypF); add(cymF, &m.cymF); add(wq, &m.wq); add(wqv, &m.wqv);
+  add(cypF, &m.cypF); add(cymF, &m.cymF); add(wq, &m.wq); add(wqv, &m.wqv); add(cqu, &m.cqu);
   add(rdz, &m.rdz); add(rdzg, &m.rdzg); add(czpC, &m.czpC); add(czmC, &m.czmC);
   add(czpF, &m.czpF); add(czmF, &m.czmF);
   if (h->metric_buf == nullptr) {
@@ -464,7 +476,14 @@ static int sync_scalars_from_device(Handle* h) {
 static int enqueue_step(Handle* h, double dt, double to) {
   static const double rk_t[3] = {8.0 / 15.0, 2.0 / 3.0, 1.0};
   int rc, warn = 0;
+  // The constant x mass flow (:187-193) inside the last stage: over the
+  // periodic, uniformly spaced x grid the bulk flux of d(phi)/dx telescopes
+  // to zero, so the flux of the projected u is that of U* (up to rounding);
+  // the stage-3 divergence kernel reduces it and the projection adds the shift.
+  const bool xflux = h->p.x_mass_cte == 1 && h->ib == nullptr && h->x_uniform &&
+                     h->poisson_mode == C3D_POISSON_FP64 && !h->write_pinterim;
   for (int s = 1; s <= 3; ++s) {
+    const bool fx = xflux && s == 3;
     if ((rc = launch_rhs_stage(h, s, dt))) return rc;
     // the projection reads the ghosts of U*, V*, W* as the boundary
     // conditions define them; the immersed-boundary operators need them set
@@ -475,7 +494,7 @@ static int enqueue_step(Handle* h, double dt, double to) {
       if ((rc = ib_setup_operators(h))) return rc;
       if ((rc = ib_heaviside(h))) return rc;
     }
-    if ((rc = launch_projection_step(h, s, dt))) return rc;   // :117-118, :123
+    if ((rc = launch_projection_step(h, s, dt, fx ? &h->sc->shift : nullptr))) return rc;   // :117-118, :123
     if (h->ib) {
       // a Schur solve that reached cg_max_iter is a warning: the reference
       // stops iterating and completes the step (src/projection.f90:60)
@@ -484,8 +503,8 @@ static int enqueue_step(Handle* h, double dt, double to) {
       if (rc > 0) warn = rc;
     }
   }
-  if (h->p.x_mass_cte == 1 || h->p.y_mass_cte == 1 || h->p.z_mass_cte == 1) {   // :187-211
-    if ((rc = launch_massflow_correction(h, dt))) return rc;
+  if ((h->p.x_mass_cte == 1 && !xflux) || h->p.y_mass_cte == 1 || h->p.z_mass_cte == 1) {   // :187-211
+    if ((rc = launch_massflow_correction(h, dt, false, xflux))) return rc;
   }
   return warn;
 }

@@ -70,6 +70,8 @@ struct Metric {
   const double *czpF, *czmF;   // viscous z for z-face fields (W)
   // mass-flow weights 0.5*(yg(j)-yg(j-1)) (U, W) and 0.5*(y(j)-y(j-1)) (V)
   const double *wq, *wqv;
+  // weight of u(j) in the x bulk flux, wq(j) + wq(j+1) (zero outside the pairs)
+  const double *cqu;
 };
 
 // device scalars shared by kernels of one step (kept on device so the step
@@ -168,6 +170,10 @@ struct Handle {
   double *phi1 = nullptr;                                   // stage-1 phi for P
   double *rhsU = nullptr, *rhsV = nullptr, *rhsW = nullptr; // fine-entry rhs arrays
   double* red = nullptr;                                    // reduction partials
+  double* flux_part = nullptr;    // per-block x bulk-flux partials (forward x FFT of the last stage)
+  int64_t flux_part_len = 0;
+  double norm_u = 0;             // norm of the x bulk flux (the flux of u = 1)
+  bool x_uniform = false;        // x spacing uniform (the flux of d(phi)/dx telescopes to zero)
   int red_len = 0;
   DevScalars* sc = nullptr;
   SpectralState sp;
@@ -245,17 +251,18 @@ int launch_poisson_of_div(Handle* h, const double* U, const double* V, const dou
                           int rk_step, double dt);
 int launch_poisson_of_div_band(Handle* h, const double* U, const double* V, const double* W, double* out,
                                int jlo, int jhi);
-int launch_projection_step(Handle* h, int rk_step, double dt);
+int launch_projection_step(Handle* h, int rk_step, double dt, const double* ushift = nullptr);
 int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, const double* Wi,
                              const double* phi, double dt, double* Uo, double* Vo, double* Wo,
-                             bool dup_plane = true, bool with_ghosts = false);
+                             bool dup_plane = true, bool with_ghosts = false,
+                             const double* ushift = nullptr);
 int rebuild_pressure(Handle* h);
 int compute_pressure(Handle* h);
 int profile_spectral(Handle* h, int part);   // 0 div_xfft, 1 spectral_yz, 2 xfft inv
 int mixed_setup(Handle* h);
 void mixed_free(Handle* h);
 // mass flow and reductions (k_massflow.cu)
-int launch_massflow_correction(Handle* h, double dt, bool euler = false);
+int launch_massflow_correction(Handle* h, double dt, bool euler = false, bool skip_x = false);
 int massflow(Handle* h, int comp, bool u_view, double* q_out);
 int massflow_w_as_v(Handle* h, double* q_out);
 // diagnostics (k_stats.cu)

@@ -186,9 +186,9 @@ static const double* flux_weight(Handle* h, int comp) {
 // src/time_integration.f90:187-211: x, then y, then z, each only when
 // enabled; euler: that of compute_time_step_Euler (:65-78, x and y only,
 // dPd = shift/dt)
-int launch_massflow_correction(Handle* h, double dt, bool euler) {
+int launch_massflow_correction(Handle* h, double dt, bool euler, bool skip_x) {
   const Dims& d = h->d;
-  const int on[3] = {h->p.x_mass_cte, h->p.y_mass_cte, euler ? 0 : h->p.z_mass_cte};
+  const int on[3] = {skip_x ? 0 : h->p.x_mass_cte, h->p.y_mass_cte, euler ? 0 : h->p.z_mass_cte};
   const double q0[3] = {h->Qflow_x_0, h->Qflow_y_0, h->Qflow_z_0};
   double* F[3] = {h->U, h->V, h->W};
   const int n1[3] = {d.nx, d.nxg, d.nxg}, n2[3] = {d.nyg, d.ny, d.nyg}, n3[3] = {d.nzg, d.nzg, d.nz};

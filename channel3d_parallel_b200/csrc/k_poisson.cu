@@ -160,6 +160,11 @@ struct XfwdArgs {
   int pz;                                     // spectrum row pitch
   int rs;                                     // shared-memory row stride
   int64_t rbase, nlines;                      // lines rbase .. rbase+nlines-1 (a band of j rows)
+  // x bulk flux of u (FLUX kernels): per-block partials, the last block
+  // writes the constant-mass-flow correction to scw
+  double* flux_part;
+  DevScalars* scw;
+  double q0, norm, dt;
 };
 
 // real x-line r = (k-2) + Nz*(j-2); its spectrum goes to slab offset
@@ -191,11 +196,16 @@ __device__ __forceinline__ XfftSmem<T> xfft_carve(unsigned char* base, int N, in
   return s;
 }
 
-template <bool FROM_DIV, typename T>
+// FLUX: the bulk flux of u (src/mass_flow.f90:24-53, 144-175) is reduced
+// from the u values this kernel reads (compute_time_step_RK3's correction,
+// src/time_integration.f90:187-193, then needs no pass of its own): weights
+// wq(j) + wq(j+1) per row and plane 2 twice (plane nzg-1 is its copy).
+template <bool FROM_DIV, typename T, bool FLUX = false>
 __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
   using C = typename cplx<T>::t;
   extern __shared__ __align__(16) unsigned char xf_smem[];
   __shared__ int s_j[2 * kLinesX], s_off[2 * kLinesX];
+  __shared__ double s_cq[FLUX ? 2 * kLinesX : 1];
   // per real line: offsets of the x = 2 cell of u(j,k), v(j,k), v(j-1,k),
   // w(j,k), w(j,k-1) (FROM_DIV) or of the right-hand side; -1: a zero wall
   // value of v (j-1 = 1 or j = ny), or no line
@@ -232,6 +242,7 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
         bwm = k == 2 ? iw + (int64_t)(d.Nz - 1) * plw : iw - plw;
         ry = a.m.rdy[j];
         rz = a.m.rdz[k];
+        if (FLUX) s_cq[tid] = a.m.cqu[j] * (k == 2 ? 2.0 : 1.0);
       } else {
         bu = idxR(d, 2, j, k);
       }
@@ -240,8 +251,10 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
     s_off[tid] = off;
     s_bu[tid] = bu; s_bv[tid] = bv; s_bvm[tid] = bvm; s_bw[tid] = bw; s_bwm[tid] = bwm;
     s_ry[tid] = ry; s_rz[tid] = rz;
+    if (FLUX && r >= nreal) s_cq[tid] = 0.0;
   }
   __syncthreads();
+  double facc = 0.0;
   // nt is a multiple of N: thread -> x index ii, real lines rl0, rl0 + nt/N, ...
   // taken four at a time: all loads of a batch are issued before any use.
   // u(i-1) of i = 2 is the periodic image i = N+1.
@@ -274,6 +287,7 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
       if (rl >= 2 * kLinesX) continue;
       const double val = FROM_DIV ? (x1[q] - x0[q]) * rdx_i + (y1[q] - y0[q]) * s_ry[rl] + (z1[q] - z0[q]) * s_rz[rl]
                                   : x1[q];
+      if (FLUX) facc += s_cq[rl] * x1[q];
       C& zz = sm.buf[(rl >> 1) * RS + ii];
       if (rl & 1) zz.y = (T)val; else zz.x = (T)val;
       if (a.linesum) sm.sval[rl * N + ii] = val;
@@ -307,6 +321,46 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
     C* out = a.spec + (int64_t)mm * d.Ny * a.pz;
     out[s_off[2 * pl]] = A;
     if (ra + 1 < nreal) out[s_off[2 * pl + 1]] = B;
+  }
+  if (FLUX) {
+    // block partial by a fixed tree (any thread count up to kMaxNx); the last
+    // block adds the partials the same way, then shift = Qflow_x_0 -
+    // flux/norm and dPdx = (dPdx + shift/dt)/2
+    __shared__ double red[kMaxNx];
+    __shared__ bool last;
+    auto tree = [&](double v) {
+      red[tid] = v;
+      __syncthreads();
+      for (int st = kMaxNx / 2; st > 0; st >>= 1) {
+        if (tid < st && tid + st < nt) red[tid] += red[tid + st];
+        __syncthreads();
+      }
+      const double r = red[0];
+      __syncthreads();
+      return r;
+    };
+    const double bsum = tree(facc);
+    if (tid == 0) {
+      a.flux_part[blockIdx.x] = bsum;
+      __threadfence();
+      last = atomicAdd(&a.scw->ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last) {
+      __threadfence();
+      double t = 0.0;
+      for (unsigned b = tid; b < gridDim.x; b += nt) t += __ldcg(a.flux_part + b);
+      const double q = tree(t) / a.norm;
+      if (tid == 0) {
+        const double shift = a.q0 - q;
+        DevScalars* sc = a.scw;
+        sc->qflow = q;
+        sc->shift = shift;
+        sc->dpdx_prev = sc->dPdx;
+        sc->dPdx = 0.5 * (sc->dPdx + shift / a.dt);
+        sc->ticket = 0u;
+      }
+    }
   }
 }
 
@@ -912,6 +966,7 @@ static int set_limits(Handle* h, int smem_yz, int cs) {
   const int smx = xfft_smem<T>(d);
   C3D_CUDA_TRY(h, (raise_smem_limit<k_xfft_fwd<true, T>>(smx)));
   C3D_CUDA_TRY(h, (raise_smem_limit<k_xfft_fwd<false, T>>(smx)));
+  if (sizeof(T) == 8) C3D_CUDA_TRY(h, (raise_smem_limit<k_xfft_fwd<true, T, true>>(smx)));
   C3D_CUDA_TRY(h, (raise_smem_limit<k_xfft_inv<T>>(smx)));
   C3D_CUDA_TRY(h, (raise_smem_limit<k_spectral_yz<T, true>>(smem_yz)));
   C3D_CUDA_TRY(h, (raise_smem_limit<k_spectral_yz<T, false>>(smem_yz)));
@@ -926,7 +981,7 @@ static int set_limits(Handle* h, int smem_yz, int cs) {
 template <typename T>
 static int run_spectral_t(Handle* h, bool from_div, const double* U, const double* V, const double* W,
                           const double* rhs_in, double* out, double* phi1, int accumulate, int parts,
-                          int blo = 0, int bhi = -1) {
+                          int blo = 0, int bhi = -1, double flux_dt = 0.0) {
   const Dims& d = h->d;
   SpectralState& S = h->sp;
   cudaStream_t s = h->stream;
@@ -959,8 +1014,20 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     a.spec = spec; a.tw = twx; a.P = Px; a.pz = pz; a.rs = rsx; a.rbase = rbase; a.nlines = nlines;
     a.linesum = f32 ? S.linesum : nullptr;
     a.pos = S.posx;
-    if (from_div) k_xfft_fwd<true, T><<<nbx, ntx, smx, s>>>(a);
-    else k_xfft_fwd<false, T><<<nbx, ntx, smx, s>>>(a);
+    if (flux_dt > 0.0 && !f32 && from_div && nlines == (int64_t)d.Ny * d.Nz) {
+      // the x bulk flux of U reduced on the way (constant x mass flow)
+      if (h->flux_part_len < (int64_t)nbx) {
+        h->last_error = "x bulk-flux partials not allocated";
+        return C3D_ERR_CUDA;
+      }
+      a.flux_part = h->flux_part; a.scw = h->sc;
+      a.q0 = h->Qflow_x_0; a.norm = h->norm_u; a.dt = flux_dt;
+      k_xfft_fwd<true, T, true><<<nbx, ntx, smx, s>>>(a);
+    } else if (from_div) {
+      k_xfft_fwd<true, T><<<nbx, ntx, smx, s>>>(a);
+    } else {
+      k_xfft_fwd<false, T><<<nbx, ntx, smx, s>>>(a);
+    }
     C3D_LAUNCH_CHECK(h);
     if (f32) {
       k_mode00<<<1, 256, sizeof(double) * d.Ny, s>>>(d, S.linesum, S.mult, S.rdp, S.du, S.phi00);
@@ -1144,7 +1211,8 @@ __global__ void __launch_bounds__(256, 4) k_grad_sub2(Dims d, Metric m, const do
                                                    const double* __restrict__ Wi,
                                                    const double* __restrict__ phi,
                                                    double* __restrict__ Uo, double* __restrict__ Vo,
-                                                   double* __restrict__ Wo, int ghosts) {
+                                                   double* __restrict__ Wo, int ghosts,
+                                                   const double* __restrict__ ushift) {
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 2 + 2 * (int)blockIdx.z;
@@ -1172,8 +1240,17 @@ __global__ void __launch_bounds__(256, 4) k_grad_sub2(Dims d, Metric m, const do
     }
   }
   const double rx = m.rdxg[i], ry = m.rdyg[j];
-  const double un0 = u0 - (px - p0) * rx, wn0 = w0 - (p1 - p0) * m.rdzg[k], vn0 = v0 - (py - p0) * ry;
-  const double un1 = u1 - (p1x - p1) * rx, wn1 = w1 - (p2 - p1) * m.rdzg[k + 1], vn1 = v1 - (p1y - p1) * ry;
+  double un0 = u0 - (px - p0) * rx;
+  const double wn0 = w0 - (p1 - p0) * m.rdzg[k], vn0 = v0 - (py - p0) * ry;
+  double un1 = u1 - (p1x - p1) * rx;
+  const double wn1 = w1 - (p2 - p1) * m.rdzg[k + 1], vn1 = v1 - (p1y - p1) * ry;
+  if (ushift) {
+    // constant-mass-flow correction of u after the projection
+    // (src/time_integration.f90:187-193), ghosts included
+    const double sh = *ushift;
+    un0 += sh;
+    un1 += sh;
+  }
   if (!ghosts) {
     Uo[iu] = un0;
     Wo[iw] = wn0;
@@ -1211,16 +1288,20 @@ __global__ void __launch_bounds__(256, 4) k_grad_sub2(Dims d, Metric m, const do
 
 int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, const double* Wi,
                              const double* phi, double dt, double* Uo, double* Vo, double* Wo,
-                             bool dup_plane, bool with_ghosts) {
+                             bool dup_plane, bool with_ghosts, const double* ushift) {
   const Dims& d = h->d;
   dim3 b(32, 4, 2);
   dim3 g((d.Nx + 31) / 32, (d.Ny + 3) / 4, (d.Nz + 1) / 2);
   double* Pint = (h->ib != nullptr || h->write_pinterim) ? h->P_interim : nullptr;
   if (!dup_plane && !Pint) {
     const dim3 b2(32, 8, 1), g2((d.Nx + 31) / 32, (d.Ny + 7) / 8, (d.Nz + 1) / 2);
-    k_grad_sub2<<<g2, b2, 0, h->stream>>>(d, h->m, Ui, Vi, Wi, phi, Uo, Vo, Wo, with_ghosts ? 1 : 0);
+    k_grad_sub2<<<g2, b2, 0, h->stream>>>(d, h->m, Ui, Vi, Wi, phi, Uo, Vo, Wo, with_ghosts ? 1 : 0, ushift);
     C3D_LAUNCH_CHECK(h);
     return 0;
+  }
+  if (ushift) {
+    h->last_error = "mass-flow correction inside the projection needs the time step's update kernel";
+    return C3D_ERR_UNSUPPORTED;
   }
   k_grad_sub<<<g, b, 0, h->stream>>>(d, h->m, Ui, Vi, Wi, phi, Uo, Vo, Wo, Pint, 1.0 / dt, dup_plane ? 1 : 0);
   C3D_LAUNCH_CHECK(h);
@@ -1231,7 +1312,7 @@ int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, cons
 // ghosts filled.  FP64: one solve.  Mixed: an FP32 solve, then refinement
 // sweeps that solve again for the FP64 residual div(U) and re-project U* with
 // the accumulated potential.
-int launch_projection_step(Handle* h, int rk_step, double dt) {
+int launch_projection_step(Handle* h, int rk_step, double dt, const double* ushift) {
   const bool stage1 = (rk_step == 1 && h->ib == nullptr);
   int rc;
   if (h->poisson_mode == C3D_POISSON_MIXED) {
@@ -1248,13 +1329,17 @@ int launch_projection_step(Handle* h, int rk_step, double dt) {
     }
     h->stats.refinement_sweeps = sweeps;
   } else {
+    // with ushift, the forward x FFT also yields the x mass-flow correction
+    // (the bulk flux of d(phi)/dx over the periodic uniform x grid is zero,
+    // so the flux of the projected u is that of U*)
     rc = run_spectral_t<double>(h, true, h->Us, h->Vs, h->Ws, nullptr, h->rhs_p,
-                                stage1 ? h->phi1 : nullptr, 0, 7);
+                                stage1 ? h->phi1 : nullptr, 0, 7, 0, -1, ushift ? dt : 0.0);
     if (rc) return rc;
   }
   if (stage1) { h->P_pending = true; h->P_pending_dt = dt; }
-  // the projected fields with all their ghost entries
-  return launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W, false, true);
+  // the projected fields with all their ghost entries (and the x mass-flow
+  // correction when ushift is given)
+  return launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W, false, true, ushift);
 }
 
 // P = phi1/(dt*rk_coef(1,1)) with the copies of src/poisson.f90:92-98
@@ -1320,6 +1405,9 @@ int poisson_setup(Handle* h) {
     const int64_t ns = (int64_t)d.Ny * S.pz64 * d.nkx;
     if ((rc = dev_alloc(h, &S.spec, ns))) return rc;
     if ((rc = set_limits<double>(h, S.smem64, S.cs64))) return rc;
+    const int64_t nbx = (((int64_t)d.Ny * d.Nz + 1) / 2 + kLinesX - 1) / kLinesX;
+    if ((rc = dev_alloc(h, &h->flux_part, nbx))) return rc;
+    h->flux_part_len = nbx;
   }
   return build_tri_table(h);
 }
