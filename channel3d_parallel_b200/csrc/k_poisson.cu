@@ -253,6 +253,8 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
     s_ry[tid] = ry; s_rz[tid] = rz;
     if (FLUX && r >= nreal) s_cq[tid] = 0.0;
   }
+  pdl_wait();
+  pdl_trigger();
   __syncthreads();
   double facc = 0.0;
   // nt is a multiple of N: thread -> x index ii, real lines rl0, rl0 + nt/N, ...
@@ -437,6 +439,8 @@ __global__ void __launch_bounds__(yz_threads<NARROW>(), yz_min_blocks<NARROW>())
     mbar_init(&bar, 1);
     fence_mbar_init();
   }
+  pdl_wait();
+  pdl_trigger();
   __syncthreads();
   // this CTA's rows of the band: [blo, bhi)
   const int blo = min(max(a.rlo - j0, 0), jn), bhi = max(min(a.rhi + 1 - j0, jn), blo);
@@ -755,6 +759,8 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
     s_bo[tid] = bo;
     s_bo2[tid] = bo2;
   }
+  pdl_wait();
+  pdl_trigger();
   __syncthreads();
   // Z = A + iB on the full circle from the two half spectra, placed at the
   // digit-reversed positions the inverse transform expects
@@ -947,13 +953,15 @@ static int launch_yz(Handle* h, typename cplx<T>::t* spec, const typename cplx<T
   cfg.blockDim = dim3((unsigned)nt, 1, 1);
   cfg.dynamicSmemBytes = (size_t)smem;
   cfg.stream = h->stream;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = cs;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = h->use_pdl ? 2 : 1;
   if (narrow) C3D_CUDA_TRY(h, cudaLaunchKernelEx(&cfg, k_spectral_yz<T, true>, a));
   else C3D_CUDA_TRY(h, cudaLaunchKernelEx(&cfg, k_spectral_yz<T, false>, a));
   C3D_LAUNCH_CHECK(h);
@@ -1022,11 +1030,11 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
       }
       a.flux_part = h->flux_part; a.scw = h->sc;
       a.q0 = h->Qflow_x_0; a.norm = h->norm_u; a.dt = flux_dt;
-      k_xfft_fwd<true, T, true><<<nbx, ntx, smx, s>>>(a);
+      C3D_CUDA_TRY(h, launch_pdl(h->use_pdl, k_xfft_fwd<true, T, true>, nbx, ntx, smx, s, a));
     } else if (from_div) {
-      k_xfft_fwd<true, T><<<nbx, ntx, smx, s>>>(a);
+      C3D_CUDA_TRY(h, launch_pdl(h->use_pdl, k_xfft_fwd<true, T>, nbx, ntx, smx, s, a));
     } else {
-      k_xfft_fwd<false, T><<<nbx, ntx, smx, s>>>(a);
+      C3D_CUDA_TRY(h, launch_pdl(h->use_pdl, k_xfft_fwd<false, T>, nbx, ntx, smx, s, a));
     }
     C3D_LAUNCH_CHECK(h);
     if (f32) {
@@ -1045,7 +1053,7 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     a.pos = S.posx;
     a.P = Px; a.pz = pz; a.rs = rsx; a.rbase = rbase; a.nlines = nlines;
     a.inv_scale = 1.0 / ((double)d.Nx * (double)d.Nz);
-    k_xfft_inv<T><<<nbx, ntx, smx, s>>>(a);
+    C3D_CUDA_TRY(h, launch_pdl(h->use_pdl, k_xfft_inv<T>, nbx, ntx, smx, s, a));
     C3D_LAUNCH_CHECK(h);
   }
   if (parts == 7) h->stats.poisson_solves++;
@@ -1216,6 +1224,8 @@ __global__ void __launch_bounds__(256, 4) k_grad_sub2(Dims d, Metric m, const do
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 2 + 2 * (int)blockIdx.z;
+  pdl_wait();
+  pdl_trigger();
   if (i > d.Nx + 1 || j > d.Ny + 1) return;
   const bool two = k + 1 <= d.Nz + 1;
   const bool hv = j <= d.Ny;
@@ -1295,7 +1305,8 @@ int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, cons
   double* Pint = (h->ib != nullptr || h->write_pinterim) ? h->P_interim : nullptr;
   if (!dup_plane && !Pint) {
     const dim3 b2(32, 8, 1), g2((d.Nx + 31) / 32, (d.Ny + 7) / 8, (d.Nz + 1) / 2);
-    k_grad_sub2<<<g2, b2, 0, h->stream>>>(d, h->m, Ui, Vi, Wi, phi, Uo, Vo, Wo, with_ghosts ? 1 : 0, ushift);
+    C3D_CUDA_TRY(h, launch_pdl(h->use_pdl, k_grad_sub2, g2, b2, 0, h->stream, d, h->m, Ui, Vi, Wi, phi, Uo, Vo, Wo,
+                               with_ghosts ? 1 : 0, ushift));
     C3D_LAUNCH_CHECK(h);
     return 0;
   }

@@ -211,7 +211,6 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
   const int i = i0 + tx, j = j0 + ty;
   const bool active = (i <= d.Nx + 1) && (j <= d.Ny + 1);
   const bool hasv = active && (j <= d.Ny);
-  const double dPdx = a.sc->dPdx, dPdy = a.sc->dPdy, dPdz = a.sc->dPdz;
 
   // halo-tile positions of this thread (at most two: PN <= 2 * TX * TY): the
   // offset of plane 1 and the x/y validity are fixed, plane k adds k-1 planes
@@ -232,6 +231,8 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
     offW[q] = okW[q] ? idxW(d, gi, gj, 1) : 0;
   }
   const int64_t plU = (int64_t)d.nx * d.nyg, plV = (int64_t)d.nxg * d.ny, plW = (int64_t)d.nxg * d.nyg;
+  pdl_wait();
+  pdl_trigger();
   // asynchronous copy of plane k (tile + halo) of U, V, W into a slot
   auto issue_plane = [&](int k) {
     const int slot = k & (NSLOT - 1);
@@ -248,6 +249,7 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
     }
     cp_async_commit();
   };
+  const double dPdx = a.sc->dPdx, dPdy = a.sc->dPdy, dPdz = a.sc->dPdz;
   issue_plane(k0 - 1);
   issue_plane(k0);
   for (int q = 1; q <= AHEAD; ++q) {
@@ -394,12 +396,12 @@ int launch_rhs_stage(Handle* h, int stage, double dt) {
     a.Gu_out = h->Gu; a.Gv_out = h->Gv; a.Gw_out = h->Gw;
     a.cs = dt * (8.0 / 15.0);
     a.cg = dt * (1.0 / 4.0);
-    if (h->rhs_kernel == 0) k_rhs_tiled<1><<<tg, tb, kRhsSmem, h->stream>>>(a);
+    if (h->rhs_kernel == 0) C3D_CUDA_TRY(h, launch_pdl(h->use_pdl, k_rhs_tiled<1>, tg, tb, kRhsSmem, h->stream, a));
     else k_rhs<1><<<rhs_grid(d), rhs_block(), 0, h->stream>>>(a);
   } else {
     a.Gu = h->Gu; a.Gv = h->Gv; a.Gw = h->Gw;
     a.cs = (stage == 2) ? dt * (5.0 / 12.0) : dt * (3.0 / 4.0);
-    if (h->rhs_kernel == 0) k_rhs_tiled<2><<<tg, tb, kRhsSmem, h->stream>>>(a);
+    if (h->rhs_kernel == 0) C3D_CUDA_TRY(h, launch_pdl(h->use_pdl, k_rhs_tiled<2>, tg, tb, kRhsSmem, h->stream, a));
     else k_rhs<2><<<rhs_grid(d), rhs_block(), 0, h->stream>>>(a);
   }
   C3D_LAUNCH_CHECK(h);
