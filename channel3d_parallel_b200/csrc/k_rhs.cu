@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(256) k_rhs(RhsArgs a) {
 // field value is read from HBM once per CTA (halo overhead (TX+2)(TY+2)/(TX*TY));
 // the arithmetic is that of k_rhs.
 // ---------------------------------------------------------------------------
-constexpr int TX = 32, TY = 8, KC = 32;
+constexpr int TX = 32, TY = 8, KC = 64;
 constexpr int PX = TX + 2, PY = TY + 2, PN = PX * PY;
 constexpr int NSLOT = 8;   // planes k-1, k, k+1 in use, k+2..k+4 in flight
 constexpr int AHEAD = 3;   // planes issued beyond k+1
