@@ -585,6 +585,74 @@ __global__ void __launch_bounds__(128) k_ib_gather(GatherArgs a) {
   a.out[i] = r;
 }
 
+// The same gather with eight threads per (marker, component): thread r of
+// the group walks the stencil rows (qj, qk) with qj + 5 qk = r, r+8, r+16,
+// r+24 (at most four rounds of five loads instead of 25), and the group adds
+// its partial sums by a fixed shuffle tree.  Used for the one-component
+// gathers, whose 36,864 threads are too few to hide 25 rounds of latency.
+constexpr int kGatherLanes = 8;
+__global__ void __launch_bounds__(128) k_ib_gather8(GatherArgs a) {
+  const int nb = a.T.nb;
+  const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int sub = (int)(gt & (kGatherLanes - 1));
+  const int64_t gid = gt / kGatherLanes;
+  const bool valid = gid < (int64_t)nb * a.ncomp;   // every lane joins the shuffles
+  const int c = valid ? (int)(gid / nb) : 0;
+  const int l = valid ? (int)(gid - (int64_t)c * nb) : 0;
+  const int t = a.type[c];
+  const OpTables& T = a.T;
+  const Dims& d = a.d;
+  const GField& g = a.f[c];
+  const bool e1n = a.mode == G_E1N;
+  double acc = 0.0;
+  if (valid) {
+    int ix[5];
+    double wx[5], ox[5];
+    double nx_ = 0.0, ny_ = 0.0, nz_ = 0.0;
+    if (e1n) { nx_ = T.nrm[l]; ny_ = T.nrm[nb + l]; nz_ = T.nrm[2 * nb + l]; }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      ix[q] = T.idx[tslot(nb, t, 0, q, l)];
+      wx[q] = T.w1[tslot(nb, t, 0, q, l)];
+      ox[q] = e1n ? nx_ * T.off[tslot(nb, t, 0, q, l)] : 0.0;
+    }
+    for (int rr = sub; rr < 25; rr += kGatherLanes) {
+      const int qj = rr % 5, qk = rr / 5;
+      const int iy = T.idx[tslot(nb, t, 1, qj, l)], iz = T.idx[tslot(nb, t, 2, qk, l)];
+      const double wjk = T.scale * T.w1[tslot(nb, t, 1, qj, l)] * T.w1[tslot(nb, t, 2, qk, l)];
+      const double oyz = e1n ? ny_ * T.off[tslot(nb, t, 1, qj, l)] + nz_ * T.off[tslot(nb, t, 2, qk, l)] : 0.0;
+#pragma unroll
+      for (int qi = 0; qi < 5; ++qi) {
+        double v;
+        if (a.mode == G_GRAD) {
+          const double* P = a.phi;
+          const double p0 = P[idxR(d, ix[qi], iy, iz)];
+          double gv;
+          if (t == 0) gv = (P[idxR(d, ix[qi] + 1, iy, iz)] - p0) * a.m.rdxg[ix[qi]];
+          else if (t == 1)
+            gv = (iy >= 2 && iy <= d.ny - 1) ? (P[idxR(d, ix[qi], iy + 1, iz)] - p0) * a.m.rdyg[iy] : 0.0;
+          else gv = (P[idxR(d, ix[qi], iy, iz + 1)] - p0) * a.m.rdzg[iz];
+          v = gv * a.phimul - a.reg[c][lin(g.n1, g.n2, ix[qi], iy, iz, 0)];
+        } else {
+          v = g.F[lin(g.n1, g.n2, ix[qi], iy, iz, g.rhsp)] * g.mul;
+        }
+        double term = wjk * wx[qi] * v;
+        if (e1n) term *= ox[qi] + oyz;
+        acc += term;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = kGatherLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (valid && sub == 0) {
+    double r = a.sign * acc;
+    const int i = c * nb + l;
+    if (a.sub) r -= a.sub[i] * a.subv[i];
+    if (a.addv) r += a.addv[i];
+    a.out[i] = r;
+  }
+}
+
 enum SpreadMode { S_RAW = 0, S_JUMP = 1, S_NORMAL = 2 };
 
 struct SpreadArgs {
@@ -1177,7 +1245,7 @@ static int gather_c(Handle* h, const double* P, double mul, double* out, double 
   a.f[0] = GField{P, h->d.nxg - 2, h->d.nyg - 2, 1, mul};
   a.type[0] = 3;
   a.ncomp = 1; a.mode = G_E1N; a.out = out; a.sign = sign;
-  k_ib_gather<<<thread_blocks(h->ib->nb), 128, 0, h->stream>>>(a);
+  k_ib_gather8<<<thread_blocks(kGatherLanes * (int64_t)h->ib->nb), 128, 0, h->stream>>>(a);
   C3D_LAUNCH_CHECK(h);
   return 0;
 }
