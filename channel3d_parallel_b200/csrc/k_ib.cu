@@ -585,13 +585,15 @@ __global__ void __launch_bounds__(128) k_ib_gather(GatherArgs a) {
   a.out[i] = r;
 }
 
-// The same gather with eight threads per (marker, component): thread r of
-// the group walks the stencil rows (qj, qk) with qj + 5 qk = r, r+8, r+16,
-// r+24 (at most four rounds of five loads instead of 25), and the group adds
-// its partial sums by a fixed shuffle tree.  Used for the one-component
+// The same gather with LANES threads per (marker, component): thread r of
+// the group walks the stencil rows (qj, qk) with qj + 5 qk = r, r+LANES, ...
+// (25/LANES rounds of five loads instead of 25), and the group adds its
+// partial sums by a fixed shuffle tree.  Eight lanes for the one-component
 // gathers, whose 36,864 threads are too few to hide 25 rounds of latency.
 constexpr int kGatherLanes = 8;
+template <int LANES>
 __global__ void __launch_bounds__(128) k_ib_gather8(GatherArgs a) {
+  constexpr int kGatherLanes = LANES;
   const int nb = a.T.nb;
   const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int sub = (int)(gt & (kGatherLanes - 1));
@@ -1245,7 +1247,7 @@ static int gather_c(Handle* h, const double* P, double mul, double* out, double 
   a.f[0] = GField{P, h->d.nxg - 2, h->d.nyg - 2, 1, mul};
   a.type[0] = 3;
   a.ncomp = 1; a.mode = G_E1N; a.out = out; a.sign = sign;
-  k_ib_gather8<<<thread_blocks(kGatherLanes * (int64_t)h->ib->nb), 128, 0, h->stream>>>(a);
+  k_ib_gather8<kGatherLanes><<<thread_blocks(kGatherLanes * (int64_t)h->ib->nb), 128, 0, h->stream>>>(a);
   C3D_LAUNCH_CHECK(h);
   return 0;
 }
