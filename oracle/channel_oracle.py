@@ -862,7 +862,7 @@ def seeded_initial_state(g, dPdx, amplitude=0.1, seed=0, project=True, dt=1e-3):
 
 def channel_params(nx_global, ny_global, nz_global, Lxp, Lzp, nu, alpha=2.0,
                    dPdx=None, cfl=-1e-3, x_mass_cte=1, grid_type=1, **extra):
-    """Parameter dict for a BASELINE-style channel configuration."""
+    """Parameter dict for a channel configuration of the benchmark workloads."""
     from .namelist import DEFAULTS
     p = dict(DEFAULTS)
     p.update(dict(nx_global=nx_global, ny_global=ny_global, nz_global=nz_global,
