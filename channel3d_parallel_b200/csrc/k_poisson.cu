@@ -1326,6 +1326,7 @@ int launch_gradient_subtract(Handle* h, const double* Ui, const double* Vi, cons
 int launch_projection_step(Handle* h, int rk_step, double dt, const double* ushift) {
   const bool stage1 = (rk_step == 1 && h->ib == nullptr);
   int rc;
+  double* phi = h->rhs_p;
   if (h->poisson_mode == C3D_POISSON_MIXED) {
     const int sweeps = h->refine_sweeps;
     rc = run_spectral_t<float>(h, true, h->Us, h->Vs, h->Ws, nullptr, h->rhs_p,
@@ -1342,15 +1343,18 @@ int launch_projection_step(Handle* h, int rk_step, double dt, const double* ushi
   } else {
     // with ushift, the forward x FFT also yields the x mass-flow correction
     // (the bulk flux of d(phi)/dx over the periodic uniform x grid is zero,
-    // so the flux of the projected u is that of U*)
-    rc = run_spectral_t<double>(h, true, h->Us, h->Vs, h->Ws, nullptr, h->rhs_p,
-                                stage1 ? h->phi1 : nullptr, 0, 7, 0, -1, ushift ? dt : 0.0);
+    // so the flux of the projected u is that of U*).  The stage-1 potential,
+    // kept for the pressure (src/poisson.f90:91-99), is solved straight into
+    // its own array, which the update then reads: no second copy.
+    phi = stage1 ? h->phi1 : h->rhs_p;
+    rc = run_spectral_t<double>(h, true, h->Us, h->Vs, h->Ws, nullptr, phi, nullptr, 0, 7, 0, -1,
+                                ushift ? dt : 0.0);
     if (rc) return rc;
   }
   if (stage1) { h->P_pending = true; h->P_pending_dt = dt; }
   // the projected fields with all their ghost entries (and the x mass-flow
   // correction when ushift is given)
-  return launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W, false, true, ushift);
+  return launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, phi, dt, h->U, h->V, h->W, false, true, ushift);
 }
 
 // P = phi1/(dt*rk_coef(1,1)) with the copies of src/poisson.f90:92-98
