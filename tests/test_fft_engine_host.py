@@ -17,8 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 @pytest.mark.skipif(shutil.which("g++") is None, reason="g++ not available")
 def test_fft_engine_plans(tmp_path):
     exe = str(tmp_path / "fft_engine_check")
-    src = os.path.join(HERE, "fft_host", "fft_engine_check.cpp")
-    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(HERE, "fft_host"), src, "-o", exe],
+    src = os.path.join(HERE, "host_kernels", "fft_engine_check.cpp")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(HERE, "host_kernels"), src, "-o", exe],
                    check=True, capture_output=True, text=True)
     r = subprocess.run([exe], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
