@@ -16,7 +16,10 @@
 //   inverse DFT / (nxp*nzp), real     -> k_xfft_inv: complex-to-real x FFT of
 //   part, periodic copies (:78-88)       the Hermitian half spectrum.
 // gradient (src/differential_operators.f90:16-52) and the projection update
-// (src/projection.f90:22-46) are k_grad_sub.
+// (src/projection.f90:22-46) are k_grad_sub; in the time step k_grad_sub2,
+// which also writes every ghost entry of u, v, w (the boundary conditions)
+// and, in the last stage, adds the constant-x-mass-flow shift whose bulk
+// flux the forward x FFT reduced (k_xfft_fwd<.., FLUX>).
 //
 // Two precisions share the kernels (template T): FP64, and FP32 for the
 // mixed-precision solve, where the kx = kz = 0 wall-normal mode is computed
