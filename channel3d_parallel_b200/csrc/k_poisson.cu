@@ -768,24 +768,39 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
   __syncthreads();
   // Z = A + iB on the full circle from the two half spectra, placed at the
   // digit-reversed positions the inverse transform expects
-  for (int t = tid; t < kLinesX * nk; t += nt) {
-    const int pl = t % kLinesX;
-    const int mm = t / kLinesX;
-    const int64_t ra = r0 + 2 * pl;
-    const C* in = a.spec + (int64_t)mm * d.Ny * a.pz;
-    C A = C{(T)0, (T)0}, B = C{(T)0, (T)0};
-    if (ra < nreal) A = in[s_off[2 * pl]];
-    if (ra + 1 < nreal) B = in[s_off[2 * pl + 1]];
-    if (mm == 0 || 2 * mm == N) { A.y = (T)0; B.y = (T)0; }   // Hermitian projection
-    C Z;
-    Z.x = A.x - B.y;
-    Z.y = A.y + B.x;
-    sm.buf[pl * RS + sm.pos[mm]] = Z;
-    if (mm > 0 && 2 * mm < N) {
-      C Zc;
-      Zc.x = A.x + B.y;
-      Zc.y = -A.y + B.x;
-      sm.buf[pl * RS + sm.pos[N - mm]] = Zc;
+  // the spectrum values of kU items are loaded before any of them is placed
+  constexpr int kU = 4;
+  for (int t0 = tid; t0 < kLinesX * nk; t0 += kU * nt) {
+    C Ab[kU], Bb[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int t = t0 + u * nt;
+      Ab[u] = Bb[u] = C{(T)0, (T)0};
+      if (t < kLinesX * nk) {
+        const int pl = t % kLinesX, mm = t / kLinesX;
+        const int64_t ra = r0 + 2 * pl;
+        const C* in = a.spec + (int64_t)mm * d.Ny * a.pz;
+        if (ra < nreal) Ab[u] = in[s_off[2 * pl]];
+        if (ra + 1 < nreal) Bb[u] = in[s_off[2 * pl + 1]];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int t = t0 + u * nt;
+      if (t >= kLinesX * nk) break;
+      const int pl = t % kLinesX, mm = t / kLinesX;
+      C A = Ab[u], B = Bb[u];
+      if (mm == 0 || 2 * mm == N) { A.y = (T)0; B.y = (T)0; }   // Hermitian projection
+      C Z;
+      Z.x = A.x - B.y;
+      Z.y = A.y + B.x;
+      sm.buf[pl * RS + sm.pos[mm]] = Z;
+      if (mm > 0 && 2 * mm < N) {
+        C Zc;
+        Zc.x = A.x + B.y;
+        Zc.y = -A.y + B.x;
+        sm.buf[pl * RS + sm.pos[N - mm]] = Zc;
+      }
     }
   }
   __syncthreads();
