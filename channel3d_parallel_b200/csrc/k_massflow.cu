@@ -356,9 +356,10 @@ int compute_dt_cfl(Handle* h, double* dt) {
   double dtc = p.CFL * lu;
   dtc = p.CFL * lv < dtc ? p.CFL * lv : dtc;
   dtc = p.CFL * lw < dtc ? p.CFL * lw : dtc;
-  double dtv = p.CFL * h->dxmin * h->dxmin / p.nu;
-  double t2 = p.CFL * h->dymin * h->dymin / p.nu;
-  double t3 = p.CFL * h->dzmin * h->dzmin / p.nu;
+  // CFL*dxmin**2/nu in the reference's order (the square first)
+  double dtv = p.CFL * (h->dxmin * h->dxmin) / p.nu;
+  double t2 = p.CFL * (h->dymin * h->dymin) / p.nu;
+  double t3 = p.CFL * (h->dzmin * h->dzmin) / p.nu;
   dtv = t2 < dtv ? t2 : dtv;
   dtv = t3 < dtv ? t3 : dtv;
   double r = dtc < dtv ? dtc : dtv;

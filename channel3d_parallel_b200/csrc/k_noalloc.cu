@@ -13,7 +13,10 @@
 // loads the library until the process exits.  Host code cannot use the
 // array's name as a device address; the first call on each device resolves
 // the address with cudaGetSymbolAddress while that device is current (so
-// that first call must come before any stream capture).  All calls share the
+// that first call must come before any stream capture).  The address is kept
+// for the life of the process, so the entry must not be used across a
+// cudaDeviceReset of that device (the array then has a new address that the
+// cached one does not follow).  All calls share the
 // array: calls whose kernels overlap on a GPU race on it, so issue them on
 // one stream or serialise them.  Each call writes every partial it later
 // reads, so nothing needs clearing between calls.
@@ -120,6 +123,15 @@ extern "C" int c3d_mean_mass_flow_u_noalloc(const double* U, int nx, int nyg, in
                      std::to_string(kNoAllocMaxPlanes) + " planes");
     return C3D_ERR_PARAM;
   }
+  // an error left pending by the caller's own earlier work is reported as
+  // such and left in place (peek, not get), so it is not mistaken for a
+  // failure of this call's launches
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) {
+    set_global_error(std::string("c3d_mean_mass_flow_u_noalloc: CUDA error pending before the call: ") +
+                     cudaGetErrorString(e));
+    return C3D_ERR_CUDA;
+  }
   double2* part = nullptr;
   std::string err;
   int rc = resolve_scratch(&part, err);
@@ -127,7 +139,7 @@ extern "C" int c3d_mean_mass_flow_u_noalloc(const double* U, int nx, int nyg, in
   cudaStream_t s = (cudaStream_t)stream;
   k_flux_plane_noalloc<<<nplanes, 256, 0, s>>>(U, nx, nyg, yg, part);
   k_flux_final_noalloc<<<1, 256, 0, s>>>(part, nplanes, qflow);
-  cudaError_t e = cudaGetLastError();
+  e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_global_error(std::string("c3d_mean_mass_flow_u_noalloc launch: ") + cudaGetErrorString(e));
     return C3D_ERR_CUDA;

@@ -297,8 +297,11 @@ int c3d_precond_eval(int handle, const float* feats, const float* moments, int m
  * partial sums live in a static device array of 4096 z planes (64 KiB per
  * GPU that loads the library, held until exit); nzg-2 > 4096 is rejected
  * with C3D_ERR_PARAM.  The first call on a device looks up that array's
- * address, so make it before any stream capture.  Calls share the array:
- * calls that overlap on the GPU race, so serialise them (one stream).
+ * address, so make it before any stream capture; the address is kept until
+ * exit, so do not use this entry across a cudaDeviceReset of that device.
+ * A CUDA error already pending when the call is made is reported (and left
+ * pending) without launching anything.  Calls share the array: calls that
+ * overlap on the GPU race, so serialise them (one stream).
  *   U      device pointer, U(nx, nyg, nzg) in Fortran order
  *   yg     device pointer, yg(1:nyg)
  *   qflow  device pointer to one double: Int_U / norm
