@@ -171,28 +171,58 @@ def measure_mixed(steps=10):
     return out
 
 
-def make_ib_channel(maxit):
-    """cfg2: the 192x129x192 channel with an immersed plane at y = 0.2 above
-    the lower wall (y = -0.8 in wall-centred coordinates), 192x192 markers,
-    standing wave 0.02 sin(2 pi x/Lx) cos(2 pi t/5); uniform wall buffer
-    (grid_type 2) so the delta stencils of the plane lie in uniform y cells."""
+IB_CONFIGS = {
+    # cfg2: the 192x129x192 channel with an immersed plane at y = 0.2 above the
+    # lower wall (y = -0.8 in wall-centred coordinates), 192x192 markers,
+    # standing wave 0.02 sin(2 pi x/Lx) cos(2 pi t/5); uniform wall buffer
+    # (grid_type 2) so the delta stencils of the plane lie in uniform y cells
+    "cfg2": dict(grid=(194, 129, 194), Lxp=4.0 * math.pi, Lzp=4.0 * math.pi / 3.0, nu=1.0 / 5600.0,
+                 grid_type=2, alpha_stretch=2.0, min_buffer_width=0.3, body_type="wall_standing_wave",
+                 nxb=192, nzb=192, body_param_1=0.02, body_param_2=2 * math.pi / 5, body_param_3=1.0,
+                 body_param_4=0.2,
+                 desc="plane y=0.2, 192x192 markers, standing wave A=0.02 omega=2pi/5"),
+    # cfg3: 256x129x128 on a uniform grid (the cylinders' stencils need uniform
+    # cells); Lx = 4.5 holds the cylinders at x = 1.5 and 3.0, Lz = 2 gives
+    # nearly square x-z cells; 200 x 128 markers per cylinder of radius 0.15,
+    # surface speeds +-0.5
+    "cfg3": dict(grid=(258, 129, 130), Lxp=4.5, Lzp=2.0, nu=1.0 / 5600.0, grid_type=0, alpha_stretch=0.0,
+                 body_type="two_cylinders_z", nxb=200, nzb=128, body_param_1=0.15, body_param_2=0.5,
+                 body_param_3=1.5, body_param_4=0.3,
+                 desc="two counter-rotating z cylinders r=0.15 at (1.5,0), (3.0,0.3), 2x200x128 markers"),
+    # cfg4: Re_tau=550 channel 384x257x384 (Lx=2pi, Lz=pi, nu=1/20000), 16x8
+    # wall-mounted plates of height 0.1, 32x16 markers each, tip amplitude 0.01,
+    # seeded phases
+    "cfg4": dict(grid=(386, 257, 386), Lxp=2.0 * math.pi, Lzp=math.pi, nu=1.0 / 20000.0, grid_type=2,
+                 alpha_stretch=2.0, min_buffer_width=0.05, body_type="wall_plates", nxb=16, nzb=8,
+                 body_param_1=0.1, body_param_2=0.01, body_param_3=2 * math.pi, body_param_4=7,
+                 desc="16x8 wall plates h=0.1, 32x16 markers each, tip amplitude 0.01"),
+}
+
+
+def make_ib_channel(maxit, cfg="cfg2", tol=1e-10):
     import channel3d_parallel_b200 as c3d
-    ch = c3d.Channel(nx_global=NX, ny_global=NY, nz_global=NZ, Lxp=LX, Lzp=LZ, nu=NU, CFL=-DT,
-                     x_mass_cte=1, grid_type=2, alpha_stretch=2.0, min_buffer_width=0.3,
-                     dPdx=3.0 * NU, body_type="wall_standing_wave", nxb=NX - 2, nzb=NZ - 2,
-                     body_param_1=0.02, body_param_2=2 * math.pi / 5, body_param_3=1.0,
-                     body_param_4=0.2, cg_tol=1e-10, cg_max_iter=maxit)
+    c = dict(IB_CONFIGS[cfg])
+    nx, ny, nz = c.pop("grid")
+    c.pop("desc")
+    nu = c.pop("nu")
+    ch = c3d.Channel(nx_global=nx, ny_global=ny, nz_global=nz, CFL=-DT, x_mass_cte=1, nu=nu,
+                     dPdx=3.0 * nu, cg_tol=tol, cg_max_iter=maxit, **c)
     ch.compute_heaviside()
-    c3d.seeded_initial_state(ch, 3.0 * NU, NU)
+    c3d.seeded_initial_state(ch, 3.0 * nu, nu)
     return ch
 
 
-def measure_ib(maxit=50, steps=2, modes=("none", "jacobi", "spai", "learned")):
-    """Schur BiCGSTAB of the IB projection on cfg2 for each preconditioner:
-    iterations and device ms per solve (3 solves per step), ms per iteration
-    (2 Schur applications) and the residual reached."""
+def measure_ib(maxit=300, steps=2, modes=("none", "jacobi", "band", "learned"), cfgs=("cfg2",),
+               band_maxit=600):
+    """Schur BiCGSTAB of the IB projection at the 1e-10 tolerance for each
+    preconditioner: iterations and device ms per solve (3 solves per step),
+    ms per iteration (two Schur applications), the residual reached, and for
+    the band preconditioner its builds (probes of the Schur operator and the
+    banded factorisations) in device ms."""
     import channel3d_parallel_b200 as c3d
     L = c3d.lib
+    mode_id = {"none": L.PRECOND_NONE, "jacobi": L.PRECOND_JACOBI, "band": L.PRECOND_BAND,
+               "learned": L.PRECOND_LEARNED, "spai": L.PRECOND_SPAI}
 
     def run(ch, n):
         s0 = ch.stats()
@@ -201,25 +231,45 @@ def measure_ib(maxit=50, steps=2, modes=("none", "jacobi", "spai", "learned")):
         ns = s1["bicgstab_solves"] - s0["bicgstab_solves"]
         it = s1["bicgstab_iters"] - s0["bicgstab_iters"]
         ms = s1["bicgstab_ms"] - s0["bicgstab_ms"]
+        bms = s1["precond_build_ms"] - s0["precond_build_ms"]
         return {"iters_per_solve": it / ns, "ms_per_solve": ms / ns, "ms_per_iter": ms / max(it, 1),
-                "iters_per_step": it / n, "last_residual": s1["last_residual"],
-                "fallbacks": s1["precond_fallbacks"] - s0["precond_fallbacks"]}
+                "build_ms_per_solve": bms / ns, "builds": s1["precond_builds"] - s0["precond_builds"],
+                "total_ms_per_solve": (ms + bms) / ns, "iters_per_step": it / n,
+                "last_residual": s1["last_residual"], "converged": s1["last_residual"] < 1e-10,
+                "fallbacks": s1["precond_fallbacks"] - s0["precond_fallbacks"],
+                "max_div": ch.check_divergence()}
 
-    res = {"config": "cfg2 plane y=0.2, 192x192 markers, standing wave A=0.02 omega=2pi/5",
-           "markers": (NX - 2) * (NZ - 2), "cg_tol": 1e-10, "cg_max_iter": maxit, "modes": {}}
-    for name, mode in (("none", L.PRECOND_NONE), ("jacobi", L.PRECOND_JACOBI), ("spai", L.PRECOND_SPAI)):
-        if name not in modes:
-            continue
-        ch = make_ib_channel(maxit)
-        ch.set_mode(precond=mode)
-        res["modes"][name] = run(ch, steps)
-        ch.close()
-    if "learned" not in modes:
-        return res
-    ch = make_ib_channel(maxit)
-    ch.set_mode(precond=L.PRECOND_JACOBI)
+    out = {}
+    for cfg in cfgs:
+        c = IB_CONFIGS[cfg]
+        res = {"config": c["desc"], "grid": list(c["grid"]), "cg_tol": 1e-10, "modes": {}}
+        for name in modes:
+            cap = band_maxit if name in ("band", "learned") else maxit
+            ch = make_ib_channel(cap, cfg)
+            res["markers"] = ch.dims["nb"]
+            try:
+                if name == "learned":
+                    res["modes"][name] = learned_run(ch, run, steps)
+                else:
+                    ch.set_mode(precond=mode_id[name])
+                    res["modes"][name] = run(ch, steps)
+                    res["modes"][name]["cg_max_iter"] = cap
+            except c3d.C3DError as e:
+                res["modes"][name] = {"unavailable": str(e)}
+            finally:
+                ch.close()
+        out[cfg] = res
+    return out
+
+
+def learned_run(ch, run, steps):
+    """Learned preconditioner: trained on probe pairs at three geometries
+    (RK stages of band-preconditioned steps), then used."""
+    import channel3d_parallel_b200 as c3d
+    L = c3d.lib
+    ch.set_mode(precond=L.PRECOND_BAND)
     t0 = time.perf_counter()
-    for _ in range(3):                 # probe pairs at three geometries (stages of Jacobi steps)
+    for _ in range(3):
         ch.precond_probe()
         ch.compute_time_step_RK3(1)
     t_probe = time.perf_counter() - t0
@@ -230,9 +280,7 @@ def measure_ib(maxit=50, steps=2, modes=("none", "jacobi", "spai", "learned")):
     r = run(ch, steps)
     r.update({"train_loss": loss, "train_s": t_train, "probe_and_step_s": t_probe,
               "pairs": ch.precond_info()["pairs"]})
-    res["modes"]["learned"] = r
-    ch.close()
-    return res
+    return r
 
 
 def run_reference(args):
@@ -384,7 +432,7 @@ def run_ours(args):
     extras = {}
     if ws == 1 and not args.no_extras:
         extras["mixed_vs_fp64"] = measure_mixed()
-        extras["ib_schur"] = measure_ib(maxit=args.ib_maxit)
+        extras["ib_schur"] = measure_ib(maxit=args.ib_maxit, cfgs=tuple(args.ib_cfgs.split(",")))
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         sec, nst, threads = cpu_baseline_sample()
@@ -433,11 +481,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the mixed-precision and IB Schur-solve measurements")
-    ap.add_argument("--ib-maxit", type=int, default=50,
-                    help="BiCGSTAB iteration cap of the IB measurement (reference default 50)")
+    ap.add_argument("--ib-maxit", type=int, default=300,
+                    help="BiCGSTAB iteration cap of the IB measurement without the band preconditioner")
+    ap.add_argument("--ib-cfgs", default="cfg2",
+                    help="IB configurations to measure (cfg2, cfg3, cfg4)")
     ap.add_argument("--only-ib", action="store_true",
                     help="only the IB Schur-solve measurement (--steps steps per preconditioner)")
-    ap.add_argument("--ib-modes", default="none,jacobi,spai,learned")
+    ap.add_argument("--ib-modes", default="none,jacobi,band,learned")
     ap.add_argument("--device-only", action="store_true",
                     help="only the device-timed step loop (used for profiler captures)")
     args = ap.parse_args()
@@ -445,7 +495,8 @@ def main():
         args.warmup = 3
     if args.only_ib:
         print(json.dumps(measure_ib(maxit=args.ib_maxit, steps=args.steps,
-                                    modes=tuple(args.ib_modes.split(",")))), flush=True)
+                                    modes=tuple(args.ib_modes.split(",")),
+                                    cfgs=tuple(args.ib_cfgs.split(",")))), flush=True)
         return
     if args.impl == "reference":
         if args.steps > 20:

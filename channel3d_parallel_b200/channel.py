@@ -211,6 +211,13 @@ class Channel:
         self._check(self._lib.c3d_schur(self.handle, L.dptr(f), L.dptr(out)))
         return out
 
+    def precond_apply(self, v):
+        """M v for the preconditioner selected by set_mode (built if needed)."""
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        out = np.zeros_like(v)
+        self._check(self._lib.c3d_precond_apply(self.handle, L.dptr(v), L.dptr(out)))
+        return out
+
     def bicgstab(self, rhs):
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)
         return self._check(self._lib.c3d_bicgstab(self.handle, L.dptr(rhs)))

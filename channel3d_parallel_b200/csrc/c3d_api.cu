@@ -907,7 +907,12 @@ int c3d_set_mode(int id, int poisson_mode, int precond_mode) {
   GET_HANDLE(id);
   if (poisson_mode != C3D_POISSON_FP64 && poisson_mode != C3D_POISSON_MIXED &&
       poisson_mode != C3D_POISSON_MIXED_UNREFINED) RET(h, C3D_ERR_PARAM);
-  if (precond_mode < C3D_PRECOND_NONE || precond_mode > C3D_PRECOND_SPAI) RET(h, C3D_ERR_PARAM);
+  if (precond_mode < C3D_PRECOND_NONE || precond_mode > C3D_PRECOND_BAND) RET(h, C3D_ERR_PARAM);
+  if (precond_mode == C3D_PRECOND_BAND && h->ib && !band_supported(h)) {
+    h->last_error = "C3D_PRECOND_BAND needs a marker lattice whose geometry repeats along z "
+                    "(every body type except wall_plates)";
+    RET(h, C3D_ERR_UNSUPPORTED);
+  }
   if (poisson_mode != C3D_POISSON_FP64) {
     int rc = mixed_setup(h);
     if (rc) RET(h, rc);
@@ -1080,6 +1085,17 @@ int c3d_bicgstab(int id, const double* rhs) {
   double* dr = ib_scratch(h, 2);
   C3D_CUDA_TRY(h, cudaMemcpyAsync(dr, rhs, n * 8, cudaMemcpyHostToDevice, h->stream));
   RET(h, ib_bicgstab(h, dr, h->dt));
+}
+int c3d_precond_apply(int id, const double* in, double* out) {
+  GET_HANDLE(id);
+  int rc = need_ib(h); if (rc) RET(h, rc);
+  const int64_t n = 4 * (int64_t)ib_nb(h);
+  double* din = ib_scratch(h, 1);
+  double* dout = ib_scratch(h, 0);
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(din, in, n * 8, cudaMemcpyHostToDevice, h->stream));
+  rc = ib_precond_apply(h, din, dout, h->dt);
+  if (rc) RET(h, rc);
+  RET(h, marker_out(h, dout, out, n));
 }
 int c3d_compute_IB_projection(int id) {
   GET_HANDLE(id);

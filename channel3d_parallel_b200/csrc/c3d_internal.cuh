@@ -316,10 +316,12 @@ int ib_regT_1n(Handle* h, const double* U, const double* V, const double* W, dou
 int ib_reg(Handle* h, int comp, const double* f_dev, double* F);
 int ib_schur(Handle* h, const double* f_dev, double* Sf_dev, double dt);
 int ib_bicgstab(Handle* h, const double* rhs_dev, double dt);
+int ib_precond_apply(Handle* h, const double* in_dev, double* out_dev, double dt);
 double* ib_marker_ptr(Handle* h, int id, int64_t* len);
 double* ib_field_ptr(Handle* h, int id);
 double* ib_scratch(Handle* h, int which);
 int ib_nb(Handle* h);
+bool band_supported(Handle* h);   // banded Schur preconditioner available (k_ib_band.cu)
 
 // allocation helper
 template <typename T>

@@ -8,6 +8,8 @@
 
 namespace c3d {
 
+struct BandState;   // banded z-Fourier preconditioner (k_ib_band.cu)
+
 struct IbState {
   std::string kind;
   bool moving = false;
@@ -28,6 +30,13 @@ struct IbState {
   double* w1_d = nullptr;
   double* off_d = nullptr;
   int* flag_d = nullptr;
+  // inverse maps of the u, v, w stencils for the spreading gather
+  int* sp_cnt[3] = {nullptr, nullptr, nullptr};
+  int* sp_off[3] = {nullptr, nullptr, nullptr};
+  uint32_t* sp_ent[3] = {nullptr, nullptr, nullptr};
+  double* sp_w[3] = {nullptr, nullptr, nullptr};
+  int* sp_sums = nullptr;            // prefix-sum chunk totals
+  double* amp = nullptr;             // [3][nb] spread amplitudes
   // fields
   double *Ureg = nullptr, *Vreg = nullptr, *Wreg = nullptr;
   double *Hu = nullptr, *Hv = nullptr, *Hw = nullptr;     // interior Heaviside
@@ -55,6 +64,7 @@ struct IbState {
   std::vector<double> yb_at_jac;     // marker y when the Jacobi diagonal was probed
   int jac_clipped[4] = {0, 0, 0, 0}; // safeguarded diagonal entries per component
   double dt_at_jac = 0;
+  BandState* band = nullptr;         // banded z-Fourier preconditioner
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;   // Schur-solve timing
   ~IbState() {
     if (ev_a) cudaEventDestroy(ev_a);
@@ -71,5 +81,16 @@ int mlp_collect_solve(Handle* h, int iters_stored);       // moments from the st
 // probe pass of the Schur operator (k_ib.cu): Jacobi and SPAI blocks, and,
 // when mom is not null, per-marker SPAI moments [nb][36]
 int ib_probe(Handle* h, double dt, float* mom);
+// banded z-Fourier preconditioner (k_ib_band.cu): supported lattices, build
+// by probing, staleness after the geometry moved, application out = B^-1 in
+bool band_supported(Handle* h);
+int band_build(Handle* h, double dt);
+bool band_stale(Handle* h, double dt);
+void band_invalidate(Handle* h);
+int band_apply(Handle* h, const double* in, double* out);
+double* band_T(Handle* h);
+int band_factor_T(Handle* h, double dt);
+int band_probe_count(Handle* h);
+void band_free(IbState* s);
 
 }  // namespace c3d

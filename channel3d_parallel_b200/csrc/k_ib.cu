@@ -657,53 +657,208 @@ __global__ void __launch_bounds__(128) k_ib_gather8(GatherArgs a) {
 
 enum SpreadMode { S_RAW = 0, S_JUMP = 1, S_NORMAL = 2 };
 
-struct SpreadArgs {
-  OpTables T;
-  Dims d;
-  double* F[3];
-  int n1[3], n2[3];
-  int comp0, ncomp;
-  int mode;
-  const double* f;    // S_RAW: f[l] for component comp0; S_JUMP: fb (4nb)
-  double dtnu, dt;
+// ---- spreading R f as a gather over an inverse map of the stencils ------
+// The reference adds each marker's 125 stencil contributions to the field
+// (local_reg, src/immersed_boundary_operators.f90:544-603).  Here every grid
+// point sums the contributions that reach it, in increasing (marker, stencil
+// point) order -- the order in which the markers are visited -- so R f is
+// bitwise reproducible (no atomics, no order that depends on scheduling).
+// Per component the map is CSR over the field's points: cnt[p] entries from
+// off[p] in ent (marker << 7 | stencil point q = qi + 5 qj + 25 qk) with the
+// tensor weight w = wx (wy wz) beside each entry.  It is rebuilt whenever the
+// operators are (every RK stage for moving bodies).
+
+// count the entries of each grid point: one thread per (marker, qj, qk)
+__global__ void k_sp_count(OpTables T, int c, int n1, int n2, int* __restrict__ cnt) {
+  const int nb = T.nb;
+  const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (gid >= 25 * (int64_t)nb) return;
+  const int l = (int)(gid % nb);
+  const int r = (int)(gid / nb);
+  const int qj = r % 5, qk = r / 5;
+  const int iy = T.idx[tslot(nb, c, 1, qj, l)], iz = T.idx[tslot(nb, c, 2, qk, l)];
+#pragma unroll
+  for (int qi = 0; qi < 5; ++qi) atomicAdd(cnt + lin(n1, n2, T.idx[tslot(nb, c, 0, qi, l)], iy, iz, 0), 1);
+}
+
+// place the entries (arbitrary order within a point; sorted next)
+__global__ void k_sp_fill(OpTables T, int c, int n1, int n2, const int* __restrict__ off, int* __restrict__ cur,
+                          uint32_t* __restrict__ ent) {
+  const int nb = T.nb;
+  const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (gid >= 25 * (int64_t)nb) return;
+  const int l = (int)(gid % nb);
+  const int r = (int)(gid / nb);
+  const int qj = r % 5, qk = r / 5;
+  const int iy = T.idx[tslot(nb, c, 1, qj, l)], iz = T.idx[tslot(nb, c, 2, qk, l)];
+#pragma unroll
+  for (int qi = 0; qi < 5; ++qi) {
+    const int64_t p = lin(n1, n2, T.idx[tslot(nb, c, 0, qi, l)], iy, iz, 0);
+    const int slot = off[p] + atomicAdd(cur + p, 1);
+    ent[slot] = ((uint32_t)l << 7) | (uint32_t)(qi + 5 * qj + 25 * qk);
+  }
+}
+
+// sort each point's entries (insertion sort: a point has at most a few
+// dozen) and attach the tensor weights
+__global__ void k_sp_sort(OpTables T, int c, int64_t npts, const int* __restrict__ cnt, const int* __restrict__ off,
+                          uint32_t* __restrict__ ent, double* __restrict__ w) {
+  const int nb = T.nb;
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const int n = cnt[p];
+  if (n == 0) return;
+  uint32_t* e = ent + off[p];
+  for (int a = 1; a < n; ++a) {
+    const uint32_t v = e[a];
+    int b = a - 1;
+    while (b >= 0 && e[b] > v) { e[b + 1] = e[b]; --b; }
+    e[b + 1] = v;
+  }
+  double* wp = w + off[p];
+  for (int a = 0; a < n; ++a) {
+    const int l = (int)(e[a] >> 7), q = (int)(e[a] & 127u);
+    const int qi = q % 5, qj = (q / 5) % 5, qk = q / 25;
+    wp[a] = T.w1[tslot(nb, c, 0, qi, l)] * (T.w1[tslot(nb, c, 1, qj, l)] * T.w1[tslot(nb, c, 2, qk, l)]);
+  }
+}
+
+// per (component, marker) amplitude scale*factor*sb*f_c of the spread
+__global__ void k_sp_amp(OpTables T, int comp0, int ncomp, int mode, const double* __restrict__ f, double dtnu,
+                         double dt, double* __restrict__ amp) {
+  const int nb = T.nb;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nb * ncomp) return;
+  const int cc = gid / nb, l = gid - cc * nb;
+  const int c = comp0 + cc;
+  double fl;
+  if (mode == S_RAW) fl = f[l];
+  else if (mode == S_NORMAL) fl = T.nrm[c * nb + l];
+  else fl = dtnu * f[c * nb + l] - dt * f[3 * nb + l] * T.nrm[c * nb + l];
+  amp[c * nb + l] = T.scale * T.factor * T.sb[l] * fl;
+}
+
+struct SpGather {
+  const int* cnt;
+  const int* off;
+  const uint32_t* ent;
+  const double* w;
+  double* F;
+  int n1, n2, n3;
+  int jlo, jhi;       // Fortran rows written (every point of them)
 };
 
-// one thread per (marker, component), as the gather; within one atomic
-// instruction the threads of a warp (consecutive markers) add to distinct
-// grid points
-__global__ void __launch_bounds__(128) k_ib_spread(SpreadArgs a) {
-  const int nb = a.T.nb;
-  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= nb * a.ncomp) return;
-  const int cc = gid / nb;
-  const int c = a.comp0 + cc;
-  const int l = gid - cc * nb;
-  const OpTables& T = a.T;
-  double fl;
-  if (a.mode == S_RAW) fl = a.f[l];
-  else if (a.mode == S_NORMAL) fl = T.nrm[c * nb + l];
-  else fl = a.dtnu * a.f[c * nb + l] - a.dt * a.f[3 * nb + l] * T.nrm[c * nb + l];
-  const double amp = T.scale * T.factor * T.sb[l] * fl;
-  int ix[5], iy[5], iz[5];
-  double wx[5], wy[5], wz[5];
-#pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    ix[q] = T.idx[tslot(nb, c, 0, q, l)];
-    iy[q] = T.idx[tslot(nb, c, 1, q, l)];
-    iz[q] = T.idx[tslot(nb, c, 2, q, l)];
-    wx[q] = T.w1[tslot(nb, c, 0, q, l)];
-    wy[q] = T.w1[tslot(nb, c, 1, q, l)];
-    wz[q] = T.w1[tslot(nb, c, 2, q, l)];
-  }
-  double* F = a.F[cc];
-  const int n1 = a.n1[cc], n2 = a.n2[cc];
-  for (int qk = 0; qk < 5; ++qk)
-    for (int qj = 0; qj < 5; ++qj) {
-      const double wjk = wy[qj] * wz[qk];
-#pragma unroll
-      for (int qi = 0; qi < 5; ++qi)
-        atomicAdd(F + lin(n1, n2, ix[qi], iy[qj], iz[qk], 0), wx[qi] * wjk * amp);
+// F(i, j, k) = sum over the point's entries of w * amp(marker), for the
+// rows jlo..jhi of up to three fields; points without entries get 0
+__global__ void __launch_bounds__(256) k_sp_gather(SpGather g0, SpGather g1, SpGather g2, int ncomp,
+                                                   const double* __restrict__ amp, int nb) {
+  if ((int)blockIdx.y >= ncomp) return;
+  // field description of this component, picked member by member (a
+  // reference to one of the parameters would copy them to local memory)
+  const int by = blockIdx.y;
+#define SP_PICK(m) (by == 0 ? g0.m : (by == 1 ? g1.m : g2.m))
+  SpGather g;
+  g.cnt = SP_PICK(cnt); g.off = SP_PICK(off); g.ent = SP_PICK(ent); g.w = SP_PICK(w); g.F = SP_PICK(F);
+  g.n1 = SP_PICK(n1); g.n2 = SP_PICK(n2); g.n3 = SP_PICK(n3); g.jlo = SP_PICK(jlo); g.jhi = SP_PICK(jhi);
+#undef SP_PICK
+  const int nrow = g.jhi - g.jlo + 1;
+  const int64_t tot = (int64_t)g.n1 * nrow * g.n3;
+  const double* a = amp + (int64_t)blockIdx.y * nb;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.n1);
+    const int64_t r = t / g.n1;
+    const int j = g.jlo + (int)(r % nrow);
+    const int k = (int)(r / nrow);
+    const int64_t p = (int64_t)i + (int64_t)g.n1 * ((j - 1) + (int64_t)g.n2 * k);
+    const int n = g.cnt[p];
+    double acc = 0.0;
+    if (n) {
+      const int o = g.off[p];
+      for (int e = 0; e < n; ++e) acc += g.w[o + e] * a[g.ent[o + e] >> 7];
     }
+    g.F[p] = acc;
+  }
+}
+
+// exclusive prefix sum of n ints (three passes: chunk sums, their scan,
+// chunk scans)
+constexpr int kScanChunk = 4096;
+__global__ void __launch_bounds__(1024) k_scan_sums(const int* __restrict__ in, int64_t n, int* __restrict__ sums) {
+  __shared__ int ws[32];
+  const int64_t base = (int64_t)blockIdx.x * kScanChunk;
+  int v = 0;
+  for (int k = threadIdx.x; k < kScanChunk; k += blockDim.x)
+    if (base + k < n) v += in[base + k];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int u = ws[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) u += __shfl_xor_sync(0xffffffffu, u, o);
+    if (threadIdx.x == 0) sums[blockIdx.x] = u;
+  }
+}
+
+// block-wide exclusive scan of one value per thread (1024 threads); returns
+// the thread's prefix and the block total in *total
+__device__ int block_excl_scan(int v, int* ws, int* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int t = ws[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    ws[lane] = t;   // inclusive warp totals
+  }
+  __syncthreads();
+  const int before = (wid > 0 ? ws[wid - 1] : 0) + x - v;
+  *total = ws[31];
+  __syncthreads();
+  return before;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_top(int* __restrict__ sums, int nsums) {
+  __shared__ int ws[32];
+  int carry = 0;
+  for (int base = 0; base < nsums; base += 1024) {
+    const int k = base + threadIdx.x;
+    const int v = k < nsums ? sums[k] : 0;
+    int tot;
+    const int ex = block_excl_scan(v, ws, &tot);
+    if (k < nsums) sums[k] = carry + ex;
+    carry += tot;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_scan_chunks(const int* __restrict__ in, int64_t n,
+                                                      const int* __restrict__ sums, int* __restrict__ out) {
+  __shared__ int ws[32];
+  const int64_t base = (int64_t)blockIdx.x * kScanChunk;
+  constexpr int kPer = kScanChunk / 1024;
+  int v[kPer];
+  int loc = 0;
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    const int64_t k = base + (int64_t)threadIdx.x * kPer + u;
+    v[u] = k < n ? in[k] : 0;
+    loc += v[u];
+  }
+  int tot;
+  int run = sums[blockIdx.x] + block_excl_scan(loc, ws, &tot);
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    const int64_t k = base + (int64_t)threadIdx.x * kPer + u;
+    if (k < n) out[k] = run;
+    run += v[u];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1161,6 +1316,7 @@ int ib_create(Handle* h) {
 }
 
 void ib_free(Handle* h) {
+  if (h->ib) band_free(h->ib);
   delete h->ib;
   h->ib = nullptr;
 }
@@ -1189,6 +1345,8 @@ __global__ void k_iy_range(const int* __restrict__ idx, int nb, int* __restrict_
   atomicMin(range, lo);
   atomicMax(range + 1, hi);
 }
+
+static int build_spread_maps(Handle* h);
 
 int ib_setup_operators(Handle* h) {
   IbState* s = h->ib;
@@ -1220,7 +1378,7 @@ int ib_setup_operators(Handle* h) {
   s->iy_lo = range[0];
   s->iy_hi = range[1];
   s->have_lrn = false;
-  return 0;
+  return build_spread_maps(h);
 }
 
 // gather helpers
@@ -1252,21 +1410,77 @@ static int gather_c(Handle* h, const double* P, double mul, double* out, double 
   return 0;
 }
 
-static int spread(Handle* h, int mode, int comp0, int ncomp, const double* f, double dt,
-                  double* F0, double* F1, double* F2) {
+// build the inverse maps of the u, v, w stencils (after the weights)
+static int build_spread_maps(Handle* h) {
   IbState* s = h->ib;
   const Dims& d = h->d;
-  SpreadArgs a{};
-  a.T = tables(h); a.d = d; a.mode = mode; a.f = f; a.comp0 = comp0; a.ncomp = ncomp;
-  a.dtnu = dt * h->p.nu; a.dt = dt;
-  double* Fs[3] = {F0, F1, F2};
+  const OpTables T = tables(h);
+  const int64_t ne = 125 * (int64_t)s->nb;
   const int n1s[3] = {d.nx, d.nxg, d.nxg}, n2s[3] = {d.nyg, d.ny, d.nyg};
-  for (int c = 0; c < ncomp; ++c) {
-    a.F[c] = Fs[c];
-    a.n1[c] = n1s[comp0 + c];
-    a.n2[c] = n2s[comp0 + c];
+  const int64_t npts[3] = {sizeU(d), sizeV(d), sizeW(d)};
+  int rc;
+  for (int c = 0; c < 3; ++c) {
+    if (!s->sp_cnt[c]) {
+      if ((rc = dev_alloc(h, &s->sp_cnt[c], npts[c]))) return rc;
+      if ((rc = dev_alloc(h, &s->sp_off[c], npts[c]))) return rc;
+      if ((rc = dev_alloc(h, &s->sp_ent[c], ne))) return rc;
+      if ((rc = dev_alloc(h, &s->sp_w[c], ne))) return rc;
+    }
   }
-  k_ib_spread<<<thread_blocks((int64_t)ncomp * s->nb), 128, 0, h->stream>>>(a);
+  const int64_t maxpts = std::max(npts[0], std::max(npts[1], npts[2]));
+  const int nchunks = (int)((maxpts + kScanChunk - 1) / kScanChunk);
+  if (!s->sp_sums && (rc = dev_alloc(h, &s->sp_sums, nchunks))) return rc;
+  if (!s->amp && (rc = dev_alloc(h, &s->amp, 3 * (int64_t)s->nb))) return rc;
+  const unsigned gq = (unsigned)((25 * (int64_t)s->nb + 255) / 256);
+  for (int c = 0; c < 3; ++c) {
+    const int64_t n = npts[c];
+    const int nch = (int)((n + kScanChunk - 1) / kScanChunk);
+    C3D_CUDA_TRY(h, cudaMemsetAsync(s->sp_cnt[c], 0, 4 * (size_t)n, h->stream));
+    k_sp_count<<<gq, 256, 0, h->stream>>>(T, c, n1s[c], n2s[c], s->sp_cnt[c]);
+    C3D_LAUNCH_CHECK(h);
+    k_scan_sums<<<nch, 1024, 0, h->stream>>>(s->sp_cnt[c], n, s->sp_sums);
+    C3D_LAUNCH_CHECK(h);
+    k_scan_top<<<1, 1024, 0, h->stream>>>(s->sp_sums, nch);
+    C3D_LAUNCH_CHECK(h);
+    k_scan_chunks<<<nch, 1024, 0, h->stream>>>(s->sp_cnt[c], n, s->sp_sums, s->sp_off[c]);
+    C3D_LAUNCH_CHECK(h);
+    // the counts become the fill cursors and are counts again afterwards
+    C3D_CUDA_TRY(h, cudaMemsetAsync(s->sp_cnt[c], 0, 4 * (size_t)n, h->stream));
+    k_sp_fill<<<gq, 256, 0, h->stream>>>(T, c, n1s[c], n2s[c], s->sp_off[c], s->sp_cnt[c], s->sp_ent[c]);
+    C3D_LAUNCH_CHECK(h);
+    k_sp_sort<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(T, c, n, s->sp_cnt[c], s->sp_off[c], s->sp_ent[c],
+                                                                  s->sp_w[c]);
+    C3D_LAUNCH_CHECK(h);
+  }
+  return 0;
+}
+
+// R f of components comp0 .. comp0+ncomp-1 into F0.. over the Fortran rows
+// jlo..jhi of each field (every point of those rows is written)
+static int spread(Handle* h, int mode, int comp0, int ncomp, const double* f, double dt,
+                  double* F0, double* F1, double* F2, int jlo = 1, int jhi = 1 << 30) {
+  IbState* s = h->ib;
+  const Dims& d = h->d;
+  const OpTables T = tables(h);
+  k_sp_amp<<<thread_blocks((int64_t)ncomp * s->nb), 128, 0, h->stream>>>(T, comp0, ncomp, mode, f, dt * h->p.nu, dt,
+                                                                         s->amp);
+  C3D_LAUNCH_CHECK(h);
+  double* Fs[3] = {F0, F1, F2};
+  const int n1s[3] = {d.nx, d.nxg, d.nxg}, n2s[3] = {d.nyg, d.ny, d.nyg}, n3s[3] = {d.nzg, d.nzg, d.nz};
+  SpGather g[3]{};
+  int64_t most = 0;
+  for (int cc = 0; cc < ncomp; ++cc) {
+    const int c = comp0 + cc;
+    g[cc].cnt = s->sp_cnt[c]; g[cc].off = s->sp_off[c]; g[cc].ent = s->sp_ent[c]; g[cc].w = s->sp_w[c];
+    g[cc].F = Fs[cc]; g[cc].n1 = n1s[c]; g[cc].n2 = n2s[c]; g[cc].n3 = n3s[c];
+    g[cc].jlo = std::max(jlo, 1);
+    g[cc].jhi = std::min(jhi, n2s[c]);
+    if (g[cc].jhi < g[cc].jlo) { g[cc].jlo = 1; g[cc].jhi = 0; }
+    most = std::max(most, (int64_t)g[cc].n1 * (g[cc].jhi - g[cc].jlo + 1) * g[cc].n3);
+  }
+  if (most == 0) return 0;
+  dim3 grid((unsigned)std::min<int64_t>((most + 255) / 256, 148 * 8), (unsigned)ncomp);
+  k_sp_gather<<<grid, 256, 0, h->stream>>>(g[0], g[1], g[2], ncomp, s->amp + (int64_t)comp0 * s->nb, s->nb);
   C3D_LAUNCH_CHECK(h);
   return 0;
 }
@@ -1277,17 +1491,7 @@ static int spread(Handle* h, int mode, int comp0, int ncomp, const double* f, do
 // zeros or values of earlier geometries that no banded reader touches)
 static int reg_all_band(Handle* h, int mode, const double* f, double dt, int jlo, int jhi) {
   IbState* s = h->ib;
-  const Dims& d = h->d;
-  double* F[3] = {s->Ureg, s->Vreg, s->Wreg};
-  const int n1[3] = {d.nx, d.nxg, d.nxg}, n2[3] = {d.nyg, d.ny, d.nyg}, n3[3] = {d.nzg, d.nzg, d.nz};
-  for (int c = 0; c < 3; ++c) {
-    const int a = std::max(jlo, 1), b = std::min(jhi, n2[c]);
-    if (b < a) continue;
-    const size_t plane = 8 * (size_t)n1[c] * n2[c];
-    C3D_CUDA_TRY(h, cudaMemset2DAsync(F[c] + (size_t)(a - 1) * n1[c], plane, 0, 8 * (size_t)n1[c] * (b - a + 1),
-                                      n3[c], h->stream));
-  }
-  int rc = spread(h, mode, 0, 3, f, dt, s->Ureg, s->Vreg, s->Wreg);
+  int rc = spread(h, mode, 0, 3, f, dt, s->Ureg, s->Vreg, s->Wreg, jlo, jhi);
   if (rc) return rc;
   return launch_fill_ghosts3(h, s->Ureg, s->Vreg, s->Wreg);
 }
@@ -1298,7 +1502,7 @@ static int reg_all(Handle* h, int mode, const double* f, double dt) {
   C3D_CUDA_TRY(h, cudaMemsetAsync(s->Ureg, 0, 8 * sizeU(d), h->stream));
   C3D_CUDA_TRY(h, cudaMemsetAsync(s->Vreg, 0, 8 * sizeV(d), h->stream));
   C3D_CUDA_TRY(h, cudaMemsetAsync(s->Wreg, 0, 8 * sizeW(d), h->stream));
-  int rc = spread(h, mode, 0, 3, f, dt, s->Ureg, s->Vreg, s->Wreg);
+  int rc = spread(h, mode, 0, 3, f, dt, s->Ureg, s->Vreg, s->Wreg, s->iy_lo, s->iy_hi);
   if (rc) return rc;
   return launch_fill_ghosts3(h, s->Ureg, s->Vreg, s->Wreg);
 }
@@ -1333,7 +1537,7 @@ int ib_reg(Handle* h, int comp, const double* f, double* F) {
   const int64_t n = comp == 1 ? sizeU(d) : (comp == 2 ? sizeV(d) : sizeW(d));
   C3D_CUDA_TRY(h, cudaMemsetAsync(F, 0, 8 * n, h->stream));
   (void)s;
-  return spread(h, S_RAW, comp - 1, 1, f, 0.0, F, nullptr, nullptr);
+  return spread(h, S_RAW, comp - 1, 1, f, 0.0, F, nullptr, nullptr, s->iy_lo, s->iy_hi);
 }
 
 // schur(Sf, f), src/projection.f90:98-144
@@ -1415,16 +1619,26 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
   if (mode == C3D_PRECOND_LEARNED && !s->have_lrn) {
     if ((rc = mlp_build_blocks(h, dt))) return rc;
   }
-  if (mode != C3D_PRECOND_NONE && jacobi_stale(h, dt)) {
+  if (mode != C3D_PRECOND_NONE && mode != C3D_PRECOND_BAND && jacobi_stale(h, dt)) {
     if ((rc = build_jacobi(h, dt))) return rc;
   }
   const double* blk = mode == C3D_PRECOND_LEARNED ? s->lrn_blk
                       : mode == C3D_PRECOND_JACOBI ? s->jac_blk
                       : mode == C3D_PRECOND_SPAI   ? s->spai_blk : nullptr;
+  bool band = mode == C3D_PRECOND_BAND;
   double* x = s->fb;
   if (!s->ev_a) {
     C3D_CUDA_TRY(h, cudaEventCreate(&s->ev_a));
     C3D_CUDA_TRY(h, cudaEventCreate(&s->ev_b));
+  }
+  if (band && band_stale(h, dt)) {
+    C3D_CUDA_TRY(h, cudaEventRecord(s->ev_a, h->stream));
+    if ((rc = band_build(h, dt))) return rc;
+    C3D_CUDA_TRY(h, cudaEventRecord(s->ev_b, h->stream));
+    C3D_CUDA_TRY(h, cudaEventSynchronize(s->ev_b));
+    float bms = 0.f;
+    C3D_CUDA_TRY(h, cudaEventElapsedTime(&bms, s->ev_a, s->ev_b));
+    h->stats.precond_build_ms += bms;
   }
   C3D_CUDA_TRY(h, cudaEventRecord(s->ev_a, h->stream));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(s->scr1, x, 8 * n, cudaMemcpyDeviceToDevice, h->stream));
@@ -1448,7 +1662,9 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
     if ((rc = dot(h, s->rhat, s->r, nullptr, nullptr, 0))) return rc;           // rho_n, bta
     k_bcg_p<<<gb, 256, 0, h->stream>>>(n, s->r, s->p, s->nu, s->ph, nullptr, s->sc);
     C3D_LAUNCH_CHECK(h);
-    if (blk) {
+    if (band) {
+      if ((rc = band_apply(h, s->p, s->ph))) return rc;
+    } else if (blk) {
       k_apply_blocks<<<gm, 256, 0, h->stream>>>(nb, blk, s->p, s->ph);
       C3D_LAUNCH_CHECK(h);
     }
@@ -1456,7 +1672,9 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
     if ((rc = dot(h, s->rhat, s->nu, nullptr, nullptr, 1))) return rc;          // alpha
     k_bcg_s<<<gb, 256, 0, h->stream>>>(n, s->r, s->nu, s->s, s->sh, x, s->ph, nullptr, s->sc);
     C3D_LAUNCH_CHECK(h);
-    if (blk) {
+    if (band) {
+      if ((rc = band_apply(h, s->s, s->sh))) return rc;
+    } else if (blk) {
       k_apply_blocks<<<gm, 256, 0, h->stream>>>(nb, blk, s->s, s->sh);
       C3D_LAUNCH_CHECK(h);
     }
@@ -1507,6 +1725,31 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
   h->stats.last_residual = std::sqrt(err);
   if (!(err == err)) { h->last_error = "BiCGSTAB produced a non-finite residual"; return C3D_ERR_NAN; }
   if (it == h->p.cg_max_iter && err >= eps) return C3D_WARN_NOT_CONVERGED;
+  return 0;
+}
+
+// out = M in for the preconditioner of the current mode (built when missing
+// or stale); the identity without one
+int ib_precond_apply(Handle* h, const double* in, double* out, double dt) {
+  IbState* s = h->ib;
+  const int nb = s->nb;
+  const int64_t n = 4 * (int64_t)nb;
+  const int mode = h->precond_mode;
+  int rc;
+  if (mode == C3D_PRECOND_BAND) {
+    if (band_stale(h, dt) && (rc = band_build(h, dt))) return rc;
+    return band_apply(h, in, out);
+  }
+  if (mode == C3D_PRECOND_NONE) {
+    C3D_CUDA_TRY(h, cudaMemcpyAsync(out, in, 8 * n, cudaMemcpyDeviceToDevice, h->stream));
+    return 0;
+  }
+  if (mode == C3D_PRECOND_LEARNED && !s->have_lrn && (rc = mlp_build_blocks(h, dt))) return rc;
+  if (jacobi_stale(h, dt) && (rc = build_jacobi(h, dt))) return rc;
+  const double* blk = mode == C3D_PRECOND_LEARNED ? s->lrn_blk
+                      : mode == C3D_PRECOND_JACOBI ? s->jac_blk : s->spai_blk;
+  k_apply_blocks<<<(unsigned)((nb + 255) / 256), 256, 0, h->stream>>>(nb, blk, in, out);
+  C3D_LAUNCH_CHECK(h);
   return 0;
 }
 

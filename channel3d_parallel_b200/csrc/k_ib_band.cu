@@ -1,0 +1,646 @@
+// Banded z-Fourier preconditioner of the Schur-complement BiCGSTAB.
+//
+// No counterpart in the reference: its BiCGSTAB (src/projection.f90:146-186)
+// is unpreconditioned.  On a moving wall the Schur operator S of
+// src/projection.f90:98-144 is indefinite and nearly singular: the diagonal
+// terms -E1nH_ext*dudn and -E1nHc_ext*p_jump change sign with the offset of
+// a marker inside its y cell, so a wavy plane (which visits every offset)
+// has rows whose diagonal nearly cancels the spreading term.  That structure
+// is local along the marker lattice; what couples markers over long
+// distances is smooth.  The preconditioner therefore solves exactly with
+//     B = S restricted to lattice neighbours |d| <= 2 along the first lattice
+//         direction (all four components, every z distance),
+// which, for bodies whose geometry does not vary along z (every body type
+// here except the wall plates), is block-circulant in z: a DFT along z turns
+// B into independent banded systems per z wavenumber q and lattice segment
+// (a wall row, a cylinder ring), each solved by a banded LU with partial
+// pivoting.
+//
+// B is measured, not modelled: unit probes at z row 0 of one colour class
+// of markers (markers of a class are 8 lattice columns apart for the dudn
+// components, 32 for the pressure jump, whose Schur response reaches far
+// enough that closer probes would alias), one Schur application per class
+// and component, give S's columns at every z; the band entries are read
+// from them.
+//
+// Layout:
+//   T      [iz][L], L = ((cp*lat + i1)*5 + d)*4 + c: the response in component
+//          cp at lattice column nbr(i1, d), z row iz, to a unit in component c
+//          at (i1, z row 0);
+//   That   [q][L] its DFT over iz (q = 0 .. nzl/2);
+//   AB     per system (q, segment): LAPACK band storage (ldab = 2 kl + ku + 1,
+//          column-major) of the 4*len x 4*len system, rows and columns ordered
+//          by folded lattice position (0, len-1, 1, len-2, ... so that a cyclic
+//          band of width 2 has width 4 without wrap) times 4 plus component;
+//          after factorisation the diagonal holds the reciprocal pivot.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "c3d_internal.cuh"
+#include "ib_state.cuh"
+
+namespace c3d {
+
+namespace {
+
+constexpr int kKb = 2;                       // lattice neighbours along dim 1
+constexpr int kNd = 2 * kKb + 1;
+constexpr int kKl = 4 * (2 * kKb) + 3;       // scalar half bandwidth in folded order (19)
+constexpr int kKu = kKl;
+constexpr int kKv = kKl + kKu;               // 38
+constexpr int kLdab = 2 * kKl + kKu + 1;     // 58
+constexpr int kSolveChunk = 16;              // band columns staged per copy in the solve
+constexpr int kFactorWin = 64;               // band columns resident in the factor kernel
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 crcp(double2 a) {
+  // 1/a with scaling against overflow (Smith's method)
+  if (fabs(a.x) >= fabs(a.y)) {
+    const double r = a.y / a.x, den = a.x + a.y * r;
+    return make_double2(1.0 / den, -r / den);
+  }
+  const double r = a.x / a.y, den = a.y + a.x * r;
+  return make_double2(r / den, -1.0 / den);
+}
+
+}  // namespace
+
+struct BandState {
+  bool ok = false;                 // lattice supports the band form
+  int lat = 0, nzl = 0, nq = 0, nseg = 0;
+  std::vector<int> seg_start, seg_len;
+  int spacing[4] = {8, 8, 8, 32};
+  std::vector<std::vector<int>> colours;   // per component: used colour ids
+  int* nbr_d = nullptr;            // [lat][5]
+  int* pos_d = nullptr;            // [lat] system row block (segment start + folded position)
+  int* seg_d = nullptr;            // [lat] segment of the column
+  int* segstart_d = nullptr;       // [nseg]
+  int* seglen_d = nullptr;         // [nseg]
+  int* colour_d = nullptr;         // [4][lat]
+  double* T_d = nullptr;           // [nzl][80 lat]
+  double2* That_d = nullptr;       // [nq][80 lat]
+  double2* AB_d = nullptr;         // [nq][ldab * 4 lat]
+  int* ipiv_d = nullptr;           // [nq][4 lat]
+  double2* rhs_d = nullptr;        // [nq][4 lat]
+  double* tw_d = nullptr;          // [2][nzl] cos, sin of 2 pi k / nzl
+  int* flag_d = nullptr;           // [0] zero pivot seen
+  bool built = false;
+  std::vector<double> yb_at, xb_at;
+  double dt_at = 0;
+  int builds = 0;
+  int64_t probes = 0;
+};
+
+void band_free(IbState* s) {
+  delete s->band;
+  s->band = nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+// unit probes of one colour class in component c at z row 0
+__global__ void k_band_probe(int nb, int lat, int c, int colour, const int* __restrict__ col_of,
+                             double* __restrict__ out) {
+  const int64_t n = 4 * (int64_t)nb;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    if (t >= (int64_t)c * nb && t < (int64_t)c * nb + lat) {
+      const int i1 = (int)(t - (int64_t)c * nb);
+      v = col_of[c * lat + i1] == colour ? 1.0 : 0.0;
+    }
+    out[t] = v;
+  }
+}
+
+// band entries of the probed columns from the response R = S e
+__global__ void k_band_extract(int nb, int lat, int nzl, int c, int colour, const int* __restrict__ col_of,
+                               const int* __restrict__ nbr, const double* __restrict__ R,
+                               double* __restrict__ T) {
+  const int64_t tot = (int64_t)lat * 4 * kNd * nzl;
+  const int64_t nl = 80 * (int64_t)lat;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+    const int i1 = (int)(t % lat);
+    int64_t r = t / lat;
+    const int d = (int)(r % kNd); r /= kNd;
+    const int cp = (int)(r % 4);
+    const int iz = (int)(r / 4);
+    if (col_of[c * lat + i1] != colour) continue;
+    const int j1 = nbr[i1 * kNd + d];
+    const int64_t L = (((int64_t)cp * lat + i1) * kNd + d) * 4 + c;
+    T[(int64_t)iz * nl + L] = R[(int64_t)cp * nb + j1 + (int64_t)lat * iz];
+  }
+}
+
+// That[q][L] = sum_iz T[iz][L] exp(-2 pi i q iz / nzl)
+__global__ void k_band_dft_T(int nl, int nzl, int nq, const double* __restrict__ tw,
+                             const double* __restrict__ T, double2* __restrict__ That) {
+  const int64_t tot = (int64_t)nq * nl;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+    const int L = (int)(t % nl);
+    const int q = (int)(t / nl);
+    double re = 0.0, im = 0.0;
+    int k = 0;
+    for (int iz = 0; iz < nzl; ++iz) {
+      const double v = T[(int64_t)iz * nl + L];
+      re += v * tw[k];
+      im -= v * tw[nzl + k];
+      k += q;
+      if (k >= nzl) k -= nzl;
+    }
+    That[t] = make_double2(re, im);
+  }
+}
+
+// scatter the band entries of every system into LAPACK band storage
+__global__ void k_band_assemble(int lat, int nq, const int* __restrict__ nbr, const int* __restrict__ pos,
+                                const int* __restrict__ seg, const int* __restrict__ segstart,
+                                const double2* __restrict__ That, double2* __restrict__ AB) {
+  const int nl = 80 * lat;
+  const int64_t tot = (int64_t)nq * nl;
+  const int64_t abq = (int64_t)kLdab * 4 * lat;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+    const int L = (int)(t % nl);
+    const int q = (int)(t / nl);
+    const int c = L % 4;
+    int r = L / 4;
+    const int d = r % kNd; r /= kNd;
+    const int i1 = r % lat;
+    const int cp = r / lat;
+    const int s = seg[i1];
+    const int base = 4 * segstart[s];
+    const int col = 4 * pos[i1] + c - base;
+    const int row = 4 * pos[nbr[i1 * kNd + d]] + cp - base;
+    AB[q * abq + (int64_t)kLdab * base + (int64_t)col * kLdab + kKv + row - col] = That[t];
+  }
+}
+
+// Banded LU with partial pivoting of one system (LAPACK zgbtf2, 0-based),
+// band columns j .. j+63 resident in shared memory; the diagonal of U is
+// replaced by its reciprocal.  One CTA per system.
+__global__ void __launch_bounds__(256) k_band_factor(int lat, int nseg, const int* __restrict__ segstart,
+                                                     const int* __restrict__ seglen, double2* __restrict__ AB,
+                                                     int* __restrict__ ipiv, int* __restrict__ flag) {
+  extern __shared__ double2 win[];    // [kFactorWin][kLdab]
+  __shared__ int s_jp, s_ju;
+  const int q = blockIdx.x / nseg, s = blockIdx.x % nseg;
+  const int m = 4 * seglen[s];
+  const int base = 4 * segstart[s];
+  double2* A = AB + (int64_t)q * kLdab * 4 * lat + (int64_t)kLdab * base;
+  int* piv = ipiv + (int64_t)q * 4 * lat + base;
+  const int tid = threadIdx.x;
+  const int ncol0 = min(m, kFactorWin);
+  for (int e = tid; e < ncol0 * kLdab; e += blockDim.x) win[e] = A[e];
+  if (tid == 0) s_ju = 0;
+  __syncthreads();
+  for (int j = 0; j < m; ++j) {
+    const int km = min(kKl, m - 1 - j);
+    double2* cj = win + (j % kFactorWin) * kLdab;
+    if (tid < 32) {
+      // pivot: largest |re| + |im| among rows j .. j+km (the first on ties)
+      double best = -1.0;
+      int bi = 0;
+      for (int t = tid; t <= km; t += 32) {
+        const double2 v = cj[kKv + t];
+        const double a = fabs(v.x) + fabs(v.y);
+        if (a > best) { best = a; bi = t; }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, best, o);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (tid == 0) {
+        s_jp = bi;
+        piv[j] = j + bi;
+        if (!(best > 0.0)) atomicExch(flag, 1);
+        s_ju = max(s_ju, min(j + kKu + bi, m - 1));
+      }
+    }
+    __syncthreads();
+    const int jp = s_jp, ju = s_ju;
+    if (jp != 0) {
+      for (int col = j + tid; col <= ju; col += blockDim.x) {
+        double2* cc = win + (col % kFactorWin) * kLdab;
+        const int a = kKv + j - col, b = a + jp;
+        const double2 tmp = cc[a];
+        cc[a] = cc[b];
+        cc[b] = tmp;
+      }
+      __syncthreads();
+    }
+    const double2 piv_v = cj[kKv];
+    const bool nz = (fabs(piv_v.x) + fabs(piv_v.y)) > 0.0;
+    const double2 r = nz ? crcp(piv_v) : make_double2(0.0, 0.0);
+    if (km > 0 && nz) {
+      for (int t = 1 + tid; t <= km; t += blockDim.x) cj[kKv + t] = cmul(cj[kKv + t], r);
+      __syncthreads();
+      const int ncols = ju - j;
+      for (int e = tid; e < ncols * km; e += blockDim.x) {
+        const int col = j + 1 + e / km;
+        const int t = 1 + e % km;
+        double2* cc = win + (col % kFactorWin) * kLdab;
+        const double2 a = cc[kKv + j - col];
+        cc[kKv + j + t - col] = csub(cc[kKv + j + t - col], cmul(cj[kKv + t], a));
+      }
+    }
+    __syncthreads();
+    // column j is final: store it (diagonal as reciprocal) and bring in column j + win
+    const int jn = j + kFactorWin;
+    for (int e = tid; e < kLdab; e += blockDim.x) {
+      double2 v = cj[e];
+      if (e == kKv) v = r;
+      A[(int64_t)j * kLdab + e] = v;
+      if (jn < m) cj[e] = A[(int64_t)jn * kLdab + e];
+    }
+    __syncthreads();
+  }
+}
+
+// rhs[q][4 pos(i1) + c] = sum_iz v[c nb + i1 + lat iz] exp(-2 pi i q iz / nzl)
+__global__ void k_band_fwd(int nb, int lat, int nzl, int nq, const double* __restrict__ tw,
+                           const int* __restrict__ pos, const double* __restrict__ v, double2* __restrict__ rhs) {
+  const int64_t tot = (int64_t)nq * 4 * lat;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+    const int i1 = (int)(t % lat);
+    int64_t r = t / lat;
+    const int c = (int)(r % 4);
+    const int q = (int)(r / 4);
+    const double* vp = v + (int64_t)c * nb + i1;
+    double re = 0.0, im = 0.0;
+    int k = 0;
+    for (int iz = 0; iz < nzl; ++iz) {
+      const double x = vp[(int64_t)lat * iz];
+      re += x * tw[k];
+      im -= x * tw[nzl + k];
+      k += q;
+      if (k >= nzl) k -= nzl;
+    }
+    rhs[(int64_t)q * 4 * lat + 4 * pos[i1] + c] = make_double2(re, im);
+  }
+}
+
+// v[c nb + i1 + lat iz] = (1/nzl) sum_q w_q Re(rhs[q][..] exp(+2 pi i q iz / nzl)),
+// w_q = 2 except q = 0 and q = nzl/2 (even nzl): the real inverse transform
+// of a Hermitian spectrum
+__global__ void k_band_inv(int nb, int lat, int nzl, int nq, const double* __restrict__ tw,
+                           const int* __restrict__ pos, const double2* __restrict__ rhs, double* __restrict__ v) {
+  const int64_t tot = (int64_t)4 * nb;
+  const double inv = 1.0 / nzl;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t / nb);
+    const int l = (int)(t - (int64_t)c * nb);
+    const int i1 = l % lat, iz = l / lat;
+    const double2* rp = rhs + 4 * pos[i1] + c;
+    double acc = 0.0;
+    int k = 0;
+    for (int q = 0; q < nq; ++q) {
+      const double2 x = rp[(int64_t)q * 4 * lat];
+      const double w = (q == 0 || 2 * q == nzl) ? 1.0 : 2.0;
+      acc += w * (x.x * tw[k] - x.y * tw[nzl + k]);
+      k += iz;
+      if (k >= nzl) k -= nzl;
+    }
+    v[t] = acc * inv;
+  }
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Forward and back substitution of one system (LAPACK zgbtrs, no transpose)
+// by one warp, the band columns streamed through shared memory in chunks of
+// kSolveChunk (double-buffered cp.async), the right-hand side resident.
+__global__ void __launch_bounds__(32) k_band_solve(int lat, int nseg, const int* __restrict__ segstart,
+                                                   const int* __restrict__ seglen, const double2* __restrict__ AB,
+                                                   const int* __restrict__ ipiv, double2* __restrict__ rhs) {
+  extern __shared__ double2 sm[];
+  double2* buf = sm;                                   // [2][kSolveChunk][kLdab]
+  double2* b = sm + 2 * kSolveChunk * kLdab;           // [m]
+  const int q = blockIdx.x / nseg, s = blockIdx.x % nseg;
+  const int m = 4 * seglen[s];
+  const int base = 4 * segstart[s];
+  const double2* A = AB + (int64_t)q * kLdab * 4 * lat + (int64_t)kLdab * base;
+  const int* piv = ipiv + (int64_t)q * 4 * lat + base;
+  double2* x = rhs + (int64_t)q * 4 * lat + base;
+  const int lane = threadIdx.x;
+  for (int e = lane; e < m; e += 32) b[e] = x[e];
+  const int nch = (m + kSolveChunk - 1) / kSolveChunk;
+  auto load_chunk = [&](int ch, int slot) {
+    const int c0 = ch * kSolveChunk;
+    const int nc = min(kSolveChunk, m - c0);
+    const double2* src = A + (int64_t)c0 * kLdab;
+    double2* dst = buf + slot * kSolveChunk * kLdab;
+    for (int e = lane; e < nc * kLdab; e += 32) cp_async16(dst + e, src + e);
+    cp_async_commit();
+  };
+  // forward: b := L^-1 P b
+  load_chunk(0, 0);
+  for (int ch = 0; ch < nch; ++ch) {
+    if (ch + 1 < nch) load_chunk(ch + 1, (ch + 1) & 1); else cp_async_commit();
+    cp_async_wait<1>();
+    __syncwarp();
+    const double2* cb = buf + (ch & 1) * kSolveChunk * kLdab;
+    const int c0 = ch * kSolveChunk;
+    const int nc = min(kSolveChunk, m - c0);
+    for (int jj = 0; jj < nc; ++jj) {
+      const int j = c0 + jj;
+      if (j >= m - 1) break;
+      const int l = piv[j];
+      if (lane == 0 && l != j) { const double2 tmp = b[l]; b[l] = b[j]; b[j] = tmp; }
+      __syncwarp();
+      const double2 bj = b[j];
+      const int lm = min(kKl, m - 1 - j);
+      if (lane < lm) b[j + 1 + lane] = csub(b[j + 1 + lane], cmul(cb[jj * kLdab + kKv + 1 + lane], bj));
+      __syncwarp();
+    }
+    __syncwarp();
+  }
+  cp_async_wait<0>();
+  __syncwarp();
+  // backward: b := U^-1 b (the stored diagonal is the reciprocal)
+  load_chunk(nch - 1, 0);
+  for (int k = 0; k < nch; ++k) {
+    const int ch = nch - 1 - k;
+    if (ch - 1 >= 0) load_chunk(ch - 1, (k + 1) & 1); else cp_async_commit();
+    cp_async_wait<1>();
+    __syncwarp();
+    const double2* cb = buf + (k & 1) * kSolveChunk * kLdab;
+    const int c0 = ch * kSolveChunk;
+    const int nc = min(kSolveChunk, m - c0);
+    for (int jj = nc - 1; jj >= 0; --jj) {
+      const int j = c0 + jj;
+      const double2* col = cb + jj * kLdab;
+      if (lane == 0) b[j] = cmul(b[j], col[kKv]);
+      __syncwarp();
+      const double2 bj = b[j];
+      for (int t = lane + 1; t <= kKv; t += 32) {
+        const int i = j - t;
+        if (i >= 0) b[i] = csub(b[i], cmul(col[kKv - t], bj));
+      }
+      __syncwarp();
+    }
+    __syncwarp();
+  }
+  cp_async_wait<0>();
+  __syncwarp();
+  for (int e = lane; e < m; e += 32) x[e] = b[e];
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+// Segments of the marker lattice along its first direction, by body type:
+// each is a closed ring (a periodic wall row, a cylinder's circumference).
+// The band form needs geometry that repeats along z; the wall plates do not.
+static bool lattice_segments(const IbState* s, const Params& p, std::vector<int>& start, std::vector<int>& len) {
+  start.clear();
+  len.clear();
+  const std::string& k = s->kind;
+  const int lat = s->lat_nx;
+  if (k == "center_wall" || k == "wall_standing_wave") {
+    start = {0};
+    len = {lat};
+  } else if (k == "standing_wave" || k == "traveling_wave_x" || k == "two_cylinders_z") {
+    if (lat % 2) return false;
+    start = {0, lat / 2};
+    len = {lat / 2, lat / 2};
+  } else if (k == "double_cylinders_z") {
+    // each row holds the inner ring's nxb1 markers (body 0), then the outer
+    // ring's (src/immersed_boundary_geometry.f90:117-174)
+    int n1 = 0;
+    for (int i = 0; i < lat; ++i)
+      if (s->body[i] == 0) ++n1;
+    if (n1 <= 0 || n1 >= lat) return false;
+    start = {0, n1};
+    len = {n1, lat - n1};
+  } else {
+    return false;
+  }
+  (void)p;
+  for (int l : len)
+    if (l < 5) return false;
+  return true;
+}
+
+static int band_setup(Handle* h) {
+  IbState* s = h->ib;
+  if (s->band) return 0;
+  BandState* B = new BandState();
+  s->band = B;
+  B->ok = lattice_segments(s, h->p, B->seg_start, B->seg_len);
+  if (!B->ok) return 0;
+  const int lat = s->lat_nx;
+  B->lat = lat;
+  B->nzl = s->nb / lat;
+  B->nq = B->nzl / 2 + 1;
+  B->nseg = (int)B->seg_start.size();
+  if (B->nzl * lat != s->nb) { B->ok = false; return 0; }
+  // folded positions, neighbours, colours
+  std::vector<int> pos(lat), seg(lat), nbr((size_t)lat * kNd), col((size_t)4 * lat);
+  for (int sgi = 0; sgi < B->nseg; ++sgi) {
+    const int st = B->seg_start[sgi], n = B->seg_len[sgi];
+    const int half = (n + 1) / 2;
+    for (int i = 0; i < n; ++i) {
+      const int fp = i < half ? 2 * i : 2 * (n - 1 - i) + 1;
+      pos[st + i] = st + fp;
+      seg[st + i] = sgi;
+      for (int d = -kKb; d <= kKb; ++d) nbr[(size_t)(st + i) * kNd + d + kKb] = st + ((i + d) % n + n) % n;
+    }
+  }
+  // the folded order keeps every band entry within kKl of the diagonal
+  for (int i = 0; i < lat; ++i)
+    for (int d = 0; d < kNd; ++d)
+      if (std::abs(pos[nbr[(size_t)i * kNd + d]] - pos[i]) > 2 * kKb) {
+        B->ok = false;
+        return 0;
+      }
+  B->colours.assign(4, {});
+  for (int c = 0; c < 4; ++c) {
+    const int P = B->spacing[c];
+    std::vector<char> used(2 * P + 1, 0);
+    for (int sgi = 0; sgi < B->nseg; ++sgi) {
+      const int st = B->seg_start[sgi], n = B->seg_len[sgi];
+      const int full = (n / P) * P;
+      for (int i = 0; i < n; ++i) {
+        // full groups of P share P colours (members P apart, also across the
+        // ring's closure); the remainder markers get colours of their own
+        const int k = i < full ? i % P : P + (i - full);
+        col[(size_t)c * lat + st + i] = k;
+        used[k] = 1;
+      }
+    }
+    for (int k = 0; k < (int)used.size(); ++k)
+      if (used[k]) B->colours[c].push_back(k);
+  }
+  const int nzl = B->nzl, nq = B->nq;
+  int rc;
+  if ((rc = dev_alloc(h, &B->nbr_d, (int64_t)lat * kNd))) return rc;
+  if ((rc = dev_alloc(h, &B->pos_d, lat))) return rc;
+  if ((rc = dev_alloc(h, &B->seg_d, lat))) return rc;
+  if ((rc = dev_alloc(h, &B->segstart_d, B->nseg))) return rc;
+  if ((rc = dev_alloc(h, &B->seglen_d, B->nseg))) return rc;
+  if ((rc = dev_alloc(h, &B->colour_d, 4 * (int64_t)lat))) return rc;
+  if ((rc = dev_alloc(h, &B->T_d, (int64_t)nzl * 80 * lat))) return rc;
+  if ((rc = dev_alloc(h, &B->That_d, (int64_t)nq * 80 * lat))) return rc;
+  if ((rc = dev_alloc(h, &B->AB_d, (int64_t)nq * kLdab * 4 * lat))) return rc;
+  if ((rc = dev_alloc(h, &B->ipiv_d, (int64_t)nq * 4 * lat))) return rc;
+  if ((rc = dev_alloc(h, &B->rhs_d, (int64_t)nq * 4 * lat))) return rc;
+  if ((rc = dev_alloc(h, &B->tw_d, 2 * (int64_t)nzl))) return rc;
+  if ((rc = dev_alloc(h, &B->flag_d, 4))) return rc;
+  std::vector<double> tw(2 * (size_t)nzl);
+  for (int k = 0; k < nzl; ++k) {
+    const long double a = 2.0L * 3.141592653589793238462643383279503L * (long double)k / (long double)nzl;
+    tw[k] = (double)std::cos(a);
+    tw[nzl + k] = (double)std::sin(a);
+  }
+  cudaStream_t st = h->stream;
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(B->nbr_d, nbr.data(), 4 * nbr.size(), cudaMemcpyHostToDevice, st));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(B->pos_d, pos.data(), 4 * pos.size(), cudaMemcpyHostToDevice, st));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(B->seg_d, seg.data(), 4 * seg.size(), cudaMemcpyHostToDevice, st));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(B->segstart_d, B->seg_start.data(), 4 * B->nseg, cudaMemcpyHostToDevice, st));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(B->seglen_d, B->seg_len.data(), 4 * B->nseg, cudaMemcpyHostToDevice, st));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(B->colour_d, col.data(), 4 * col.size(), cudaMemcpyHostToDevice, st));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(B->tw_d, tw.data(), 8 * tw.size(), cudaMemcpyHostToDevice, st));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(st));
+  const int smax = *std::max_element(B->seg_len.begin(), B->seg_len.end());
+  const size_t solve_smem = sizeof(double2) * (2 * kSolveChunk * kLdab + 4 * (size_t)smax);
+  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_band_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem));
+  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_band_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(sizeof(double2) * kFactorWin * kLdab)));
+  return 0;
+}
+
+bool band_supported(Handle* h) {
+  IbState* s = h->ib;
+  if (!s) return false;
+  if (band_setup(h)) return false;
+  return s->band && s->band->ok;
+}
+
+// factor the band systems from the entries in T_d
+static int band_factor_from_T(Handle* h) {
+  IbState* s = h->ib;
+  BandState* B = s->band;
+  const int lat = B->lat, nzl = B->nzl, nq = B->nq, nl = 80 * lat;
+  const unsigned gb = 148 * 8;
+  k_band_dft_T<<<gb, 256, 0, h->stream>>>(nl, nzl, nq, B->tw_d, B->T_d, B->That_d);
+  C3D_LAUNCH_CHECK(h);
+  C3D_CUDA_TRY(h, cudaMemsetAsync(B->AB_d, 0, sizeof(double2) * (size_t)nq * kLdab * 4 * lat, h->stream));
+  k_band_assemble<<<gb, 256, 0, h->stream>>>(lat, nq, B->nbr_d, B->pos_d, B->seg_d, B->segstart_d, B->That_d,
+                                             B->AB_d);
+  C3D_LAUNCH_CHECK(h);
+  C3D_CUDA_TRY(h, cudaMemsetAsync(B->flag_d, 0, 4, h->stream));
+  k_band_factor<<<nq * B->nseg, 256, sizeof(double2) * kFactorWin * kLdab, h->stream>>>(
+      lat, B->nseg, B->segstart_d, B->seglen_d, B->AB_d, B->ipiv_d, B->flag_d);
+  C3D_LAUNCH_CHECK(h);
+  int flag = 0;
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(&flag, B->flag_d, 4, cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (flag) { h->last_error = "band preconditioner: singular band system"; return C3D_ERR_NAN; }
+  return 0;
+}
+
+// Probe the band of S at the current geometry and factor it.
+int band_build(Handle* h, double dt) {
+  IbState* s = h->ib;
+  if (!band_supported(h)) { h->last_error = "band preconditioner: unsupported marker lattice"; return C3D_ERR_UNSUPPORTED; }
+  BandState* B = s->band;
+  const int nb = s->nb, lat = B->lat, nzl = B->nzl;
+  const int64_t n = 4 * (int64_t)nb;
+  int rc;
+  if (s->prb == nullptr && (rc = dev_alloc(h, &s->prb, 4 * n))) return rc;
+  double* probe = s->prb;
+  double* resp = s->prb + n;
+  const unsigned gb = 148 * 8;
+  for (int c = 0; c < 4; ++c)
+    for (int colour : B->colours[c]) {
+      k_band_probe<<<gb, 256, 0, h->stream>>>(nb, lat, c, colour, B->colour_d, probe);
+      C3D_LAUNCH_CHECK(h);
+      if ((rc = ib_schur(h, probe, resp, dt))) return rc;
+      k_band_extract<<<gb, 256, 0, h->stream>>>(nb, lat, nzl, c, colour, B->colour_d, B->nbr_d, resp, B->T_d);
+      C3D_LAUNCH_CHECK(h);
+      B->probes++;
+    }
+  if ((rc = band_factor_from_T(h))) return rc;
+  B->built = true;
+  B->yb_at = s->yb;
+  B->xb_at = s->xb;
+  B->dt_at = dt;
+  B->builds++;
+  h->stats.precond_builds++;
+  return 0;
+}
+
+// The factors are rebuilt when dt changed or a marker moved by more than
+// 0.03 dymin since they were probed (about ten time steps of the cfg2 wave at
+// its fastest; a preconditioner 30 steps old no longer converges there).
+bool band_stale(Handle* h, double dt) {
+  IbState* s = h->ib;
+  BandState* B = s->band;
+  if (!B || !B->built || B->dt_at != dt || B->yb_at.size() != s->yb.size()) return true;
+  double mx = 0.0;
+  for (size_t k = 0; k < s->yb.size(); ++k) {
+    mx = std::max(mx, std::fabs(s->yb[k] - B->yb_at[k]));
+    mx = std::max(mx, std::fabs(s->xb[k] - B->xb_at[k]));
+  }
+  return mx > 0.03 * h->dymin;
+}
+
+void band_invalidate(Handle* h) {
+  if (h->ib && h->ib->band) h->ib->band->built = false;
+}
+
+// out = B^-1 in
+int band_apply(Handle* h, const double* in, double* out) {
+  IbState* s = h->ib;
+  BandState* B = s->band;
+  const int lat = B->lat, nzl = B->nzl, nq = B->nq, nb = s->nb;
+  const int64_t nr = (int64_t)nq * 4 * lat;
+  k_band_fwd<<<(unsigned)((nr + 127) / 128), 128, 0, h->stream>>>(nb, lat, nzl, nq, B->tw_d, B->pos_d, in, B->rhs_d);
+  C3D_LAUNCH_CHECK(h);
+  const int smax = *std::max_element(B->seg_len.begin(), B->seg_len.end());
+  const size_t smem = sizeof(double2) * (2 * kSolveChunk * kLdab + 4 * (size_t)smax);
+  k_band_solve<<<nq * B->nseg, 32, smem, h->stream>>>(lat, B->nseg, B->segstart_d, B->seglen_d, B->AB_d,
+                                                      B->ipiv_d, B->rhs_d);
+  C3D_LAUNCH_CHECK(h);
+  k_band_inv<<<(unsigned)((4 * (int64_t)nb + 127) / 128), 128, 0, h->stream>>>(nb, lat, nzl, nq, B->tw_d, B->pos_d,
+                                                                              B->rhs_d, out);
+  C3D_LAUNCH_CHECK(h);
+  return 0;
+}
+
+// Raw access for the learned preconditioner: the band entries T (caller
+// fills them) and the factorisation.
+double* band_T(Handle* h) { return (h->ib && h->ib->band) ? h->ib->band->T_d : nullptr; }
+int band_factor_T(Handle* h, double dt) {
+  int rc = band_factor_from_T(h);
+  if (rc) return rc;
+  IbState* s = h->ib;
+  BandState* B = s->band;
+  B->built = true;
+  B->yb_at = s->yb;
+  B->xb_at = s->xb;
+  B->dt_at = dt;
+  B->builds++;
+  return 0;
+}
+int band_probe_count(Handle* h) {
+  if (!band_supported(h)) return 0;
+  int n = 0;
+  for (auto& v : h->ib->band->colours) n += (int)v.size();
+  return n;
+}
+
+}  // namespace c3d

@@ -25,7 +25,7 @@ FIELD = dict(U=1, V=2, W=3, P=4, RHS_P=5, P_INTERIM=6, RHS_U=7, RHS_V=8, RHS_W=9
              HU_INTERIOR=16, HV_INTERIOR=17, HW_INTERIOR=18, HC_EXTERIOR=19)
 MARKER = dict(FB=40, UB=41, XB=42, YB=43, ZB=44, NORMALS=45, SB=46, E1NH_EXT=47, E1NHC_EXT=48)
 POISSON_FP64, POISSON_MIXED, POISSON_MIXED_UNREFINED = 0, 1, 2
-PRECOND_NONE, PRECOND_JACOBI, PRECOND_LEARNED, PRECOND_SPAI = 0, 1, 2, 3
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_LEARNED, PRECOND_SPAI, PRECOND_BAND = 0, 1, 2, 3, 4
 
 
 class Dims(C.Structure):
@@ -43,7 +43,8 @@ class Stats(C.Structure):
                 ("status", C.c_int32), ("precond_mode", C.c_int32),
                 ("last_bicgstab_ms", C.c_double), ("bicgstab_ms", C.c_double),
                 ("slab_cluster", C.c_int32 * 2), ("slab_narrow", C.c_int32 * 2),
-                ("qflow_y_0", C.c_double), ("qflow_z_0", C.c_double)]
+                ("qflow_y_0", C.c_double), ("qflow_z_0", C.c_double),
+                ("precond_builds", C.c_int64), ("precond_build_ms", C.c_double)]
 
 
 _D = C.POINTER(C.c_double)
@@ -96,6 +97,7 @@ PROTOTYPES = {
     "c3d_reg": [_INT, _INT, _D],
     "c3d_schur": [_INT, _D, _D],
     "c3d_bicgstab": [_INT, _D],
+    "c3d_precond_apply": [_INT, _D, _D],
     "c3d_compute_IB_projection": [_INT],
     "c3d_set_mode": [_INT, _INT, _INT],
     "c3d_get_stats": [_INT, C.POINTER(Stats)],

@@ -82,6 +82,7 @@ extern "C" {
 #define C3D_PRECOND_JACOBI      1   /* diagonal (Jacobi) preconditioner         */
 #define C3D_PRECOND_LEARNED     2   /* learned preconditioner + warm start      */
 #define C3D_PRECOND_SPAI        3   /* probed 4x4 block sparse approximate inverse */
+#define C3D_PRECOND_BAND        4   /* probed local band of S, solved exactly per z wavenumber */
 
 typedef struct c3d_dims {
   int32_t nx, ny, nz;          /* nx_global, ny_global, nz_global            */
@@ -109,6 +110,8 @@ typedef struct c3d_stats {
   int32_t slab_cluster[2];     /* CTAs per kx-slab cluster of the y-z solve: FP64, FP32 */
   int32_t slab_narrow[2];      /* 1: narrow slab CTAs (<= 192 threads, 3 per SM); FP64, FP32 */
   double  qflow_y_0, qflow_z_0;/* targets of the y and z constant-flux corrections */
+  int64_t precond_builds;      /* probed (or predicted) band preconditioners built */
+  double  precond_build_ms;    /* accumulated device time of those builds (ms) */
 } c3d_stats;
 
 /* ---- lifecycle ------------------------------------------------------------
@@ -232,6 +235,11 @@ int c3d_schur(int handle, const double* f, double* Sf);
 /* bicgstab(fb, rhs_ib), src/projection.f90:146-186: solves for the device
  * fb (warm start = current fb) with right-hand side rhs (4*nb, host).       */
 int c3d_bicgstab(int handle, const double* rhs);
+/* No counterpart in the reference (its BiCGSTAB is unpreconditioned): apply
+ * the Schur-solve preconditioner selected by c3d_set_mode to a host marker
+ * vector, out = M in (4*nb each), building it first when it is missing or
+ * stale; C3D_PRECOND_NONE copies.  For tests and diagnostics.             */
+int c3d_precond_apply(int handle, const double* in, double* out);
 /* compute_IB_projection, src/projection.f90:48-96 */
 int c3d_compute_IB_projection(int handle);
 

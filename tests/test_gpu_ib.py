@@ -1,9 +1,10 @@
 """GPU parity of the immersed-boundary path against the CPU oracle.
 
-Tolerances (max-norm relative): E / E1n / R and Heaviside fields 1e-12
-(R uses FP64 atomics, so sums are order-dependent at round-off); Schur
-operator 1e-11; BiCGSTAB solution and IB RK3 steps 1e-9 (the Krylov
-iterates amplify round-off by the conditioning of the Schur operator).
+Tolerances (max-norm relative): E / E1n / R and Heaviside fields 1e-12 (the
+delta weights come from the device's sqrt/asin); Schur operator 1e-11; IB
+RK3 steps after 1 and 10 steps, U, V, W and the surface unknowns fb, 1e-10
+with both Schur solves converged to 1e-14.  R is a fixed-order gather, so
+the Schur operator and whole IB steps repeat bit for bit.
 """
 import math
 
@@ -44,6 +45,13 @@ CASES = {
                         body_type="wall_plates", nxb=2, nzb=2, body_param_1=0.2,
                         body_param_2=0.01, body_param_3=2 * math.pi, body_param_4=7,
                         cfl=-1e-3),
+    # both walls with a wave travelling in x and a cosine ramp-up of its
+    # amplitude over the first 10 steps (src/immersed_boundary_geometry.f90:271-390)
+    "traveling_wave_x": dict(nx_global=34, ny_global=65, nz_global=10, Lxp=2.0, Lzp=0.5,
+                             grid_type=2, alpha_stretch=2.0, min_buffer_width=0.1,
+                             body_type="traveling_wave_x", nxb=16, nzb=3, body_param_1=0.05,
+                             body_param_2=0.5, body_param_3=math.pi, body_ramp_up_time=0.05,
+                             cfl=-0.005),
     # both walls with a standing wave (examples/input_parameters_ib_standing_wave)
     "standing_wave": dict(nx_global=34, ny_global=65, nz_global=10, Lxp=2.0, Lzp=0.5,
                           grid_type=2, alpha_stretch=2.0, min_buffer_width=0.1,
@@ -132,6 +140,17 @@ def test_heaviside(setup):
     assert rel(ch.download("E1NH_EXT"), ib.E1nH_ext) < 1e-10
 
 
+def test_spread_and_schur_are_bitwise_reproducible(setup):
+    case, p, g, st, ib, ch = setup
+    nb = ib.body.nb
+    f = np.random.default_rng(5).standard_normal(4 * nb)
+    assert np.array_equal(ch.schur(f), ch.schur(f))
+    ch.reg(2, f[:nb])
+    r1 = ch.download("V_REG")
+    ch.reg(2, f[:nb])
+    assert np.array_equal(r1, ch.download("V_REG"))
+
+
 def test_schur_operator(setup):
     case, p, g, st, ib, ch = setup
     rng = np.random.default_rng(9)
@@ -140,27 +159,64 @@ def test_schur_operator(setup):
     assert rel(ch.schur(f), ibo.schur(g, ib, f, dt)) < 1e-11
 
 
-@pytest.mark.parametrize("nsteps", [1, 2])
-def test_ib_rk3_steps(setup, nsteps):
-    case, p, g, st, ib, ch = setup
-    dt = -p["cfl"]
-    if case == "wall_plates":
-        # 32 x 16 markers per plate are 2-4 times denser than this grid: the
-        # Schur system stops at cg_max_iter, and two unconverged Krylov runs
-        # agree only to their amplified round-off.  What holds regardless:
-        # the step completes and the projected velocity is divergence-free.
+STEP_TOL = 1e-14     # BiCGSTAB tolerance of the step parity runs (both sides converge)
+
+
+@pytest.mark.parametrize("nsteps", [1, 10])
+@pytest.mark.parametrize("mode", ["none", "band"])
+@pytest.mark.parametrize("case", [c for c in CASES if c != "wall_plates"])
+def test_ib_rk3_steps(case, mode, nsteps):
+    """IB RK3 steps against the oracle (unpreconditioned BiCGSTAB, the
+    reference's), both Schur solves converged to 1e-14: U, V, W and the
+    surface unknowns fb within 1e-10 (max-norm relative) after 1 and 10 steps,
+    with the reference's solver and with the banded preconditioner."""
+    from channel3d_parallel_b200 import lib as L
+    p, g, st, ib, ch = build(case, cg_tol=STEP_TOL, cg_max_iter=600)
+    try:
+        ch.set_mode(precond=L.PRECOND_BAND if mode == "band" else L.PRECOND_NONE)
+        dt = -p["cfl"]
         ch.compute_time_step_RK3(nsteps)
+        for _ in range(nsteps):
+            ibo.compute_time_step_RK3_ib(g, st, ib, dt)
+        errs = {name: rel(ch.download(name), ref[1:, 1:, 1:])
+                for name, ref in (("U", st.U), ("V", st.V), ("W", st.W))}
+        errs["FB"] = rel(ch.download("FB"), ib.fb)
+        assert max(errs.values()) < 1e-10, errs
+        s = ch.stats()
+        assert s["bicgstab_solves"] == 3 * nsteps
+        assert s["last_residual"] < STEP_TOL
+        assert ib.last_err < STEP_TOL
+    finally:
+        ch.close()
+
+
+@pytest.mark.parametrize("case", ["wall_standing_wave", "two_cylinders_z"])
+def test_ib_steps_repeat_bitwise(case):
+    """Two handles advanced from the same state give identical fields and
+    surface unknowns (no order-dependent sums anywhere in the IB step)."""
+    out = []
+    for _ in range(2):
+        p, g, st, ib, ch = build(case, cg_tol=1e-13, cg_max_iter=400)
+        try:
+            ch.compute_time_step_RK3(3)
+            out.append([ch.download(n) for n in ("U", "V", "W", "FB")])
+        finally:
+            ch.close()
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+
+
+def test_wall_plates_steps():
+    """The plates of the test grid are resolved more finely than the grid
+    (2-4 markers per cell): the Schur system there is close to singular and
+    stops at cg_max_iter, so two unconverged Krylov runs agree only to their
+    amplified round-off.  What holds regardless: the step completes and the
+    projected velocity is divergence-free."""
+    p, g, st, ib, ch = build("wall_plates", cg_max_iter=50)
+    try:
+        ch.compute_time_step_RK3(2)
         assert ch.check_finite() == 0
         assert ch.check_divergence() < 1e-10
-        assert ch.stats()["bicgstab_solves"] == 3 * nsteps
-        return
-    ch.compute_time_step_RK3(nsteps)
-    for _ in range(nsteps):
-        ibo.compute_time_step_RK3_ib(g, st, ib, dt)
-    errs = {name: rel(ch.download(name), ref[1:, 1:, 1:])
-            for name, ref in (("U", st.U), ("V", st.V), ("W", st.W))}
-    assert max(errs.values()) < 1e-9, errs
-    assert rel(ch.download("FB"), ib.fb) < 1e-7
-    s = ch.stats()
-    assert s["bicgstab_solves"] == 3 * nsteps
-    assert s["last_residual"] < p["cg_tol"] or s["last_bicgstab_iters"] == p["cg_max_iter"]
+        assert ch.stats()["bicgstab_solves"] == 6
+    finally:
+        ch.close()
