@@ -171,13 +171,97 @@ def measure_mixed(steps=10):
     return out
 
 
+def measure_accuracy():
+    """Accuracy beside the timings: max-norm relative error of u, v, w, p
+    (and the IB surface unknowns fb) against the FP64 CPU restatement of the
+    reference's step, with max|div u|, for the FP64 and the mixed-precision
+    Poisson paths: one step at 192x129x192, ten steps at 32x65x32, and ten IB
+    steps of a planar standing-wave wall (34x49x14, band preconditioner)
+    against the NumPy oracle."""
+    import numpy as np
+    import channel3d_parallel_b200 as c3d
+    from oracle import channel_oracle as co
+    from oracle import cpu_rk3
+    cpu_rk3.build()
+
+    def rel(a, b):
+        return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+    out = {}
+    cases = {"192x129x192_1step": (194, 129, 194, LX, LZ, 1), "32x65x32_10steps": (34, 65, 34, math.pi,
+                                                                                math.pi / 2, 10)}
+    for name, (nx, ny, nz, lx, lz, nsteps) in cases.items():
+        p = co.channel_params(nx, ny, nz, lx, lz, NU)
+        g = co.Grid(p)
+        st = co.seeded_initial_state(g, p["dpdx"])
+        cc = cpu_rk3.CpuChannel(g)
+        cc.set_state(st)
+        cc.steps(nsteps)
+        ref = {k: cc.get_field(k)[1:, 1:, 1:] for k in ("U", "V", "W", "P")}
+        cc.close()
+        res = {}
+        for mode, pm in (("fp64", c3d.lib.POISSON_FP64), ("mixed", c3d.lib.POISSON_MIXED),
+                         ("mixed_unrefined", c3d.lib.POISSON_MIXED_UNREFINED)):
+            with c3d.Channel(nx_global=nx, ny_global=ny, nz_global=nz, Lxp=lx, Lzp=lz, nu=NU, CFL=-DT,
+                             x_mass_cte=1, grid_type=1, alpha_stretch=2.0, dPdx=p["dpdx"]) as ch:
+                ch.set_mode(poisson=pm)
+                ch.set_grid(g.x[1:], g.y[1:], g.z[1:])
+                for k in ("U", "V", "W"):
+                    ch.upload(k, getattr(st, k)[1:, 1:, 1:])
+                ch.set_scalars(dPdx=st.dPdx, Qflow_x_0=st.Qflow_x_0)
+                ch.compute_time_step_RK3(nsteps)
+                res[mode] = {k: rel(ch.download(k), ref[k]) for k in ("U", "V", "W", "P")}
+                res[mode]["max_div"] = ch.check_divergence()
+        out[name] = res
+    # IB: ten steps of the planar standing wave against the NumPy oracle
+    from oracle import ib_oracle as ibo
+    kw = dict(nx_global=34, ny_global=49, nz_global=14, Lxp=2.0, Lzp=0.6, grid_type=2, alpha_stretch=2.0,
+              min_buffer_width=0.45, body_type="wall_standing_wave", nxb=32, nzb=12, body_param_1=0.02,
+              body_param_2=2 * math.pi / 5.0, body_param_3=1.0, body_param_4=0.2)
+    nu = 3.076923076923077e-04
+    p = co.channel_params(34, 49, 14, 2.0, 0.6, nu, alpha=2.0, grid_type=2, cfl=-1e-3, x_mass_cte=1,
+                          cg_tol=1e-14, cg_max_iter=600, min_buffer_width=0.45, body_type="wall_standing_wave",
+                          nxb=32, nzb=12, body_param_1=0.02, body_param_2=2 * math.pi / 5.0, body_param_3=1.0,
+                          body_param_4=0.2)
+    g = co.Grid(p)
+    st = co.seeded_initial_state(g, p["dpdx"], amplitude=0.05, dt=1e-3)
+    ib = ibo.IBState(g, p, t=0.0)
+    ibo.compute_heaviside(g, ib)
+    q, n = co.mean_mass_flow_u(g, st.U, ib.Hu)
+    st.Qflow_x_0 = q / n
+    for k in ("nx_global", "ny_global", "nz_global", "Lxp", "Lzp", "grid_type", "alpha_stretch"):
+        kw.pop(k)
+    with c3d.Channel(nx_global=34, ny_global=49, nz_global=14, Lxp=2.0, Lzp=0.6, nu=nu, CFL=-1e-3, x_mass_cte=1,
+                     grid_type=2, alpha_stretch=2.0, dPdx=p["dpdx"], cg_tol=1e-14, cg_max_iter=600, **kw) as ch:
+        ch.set_grid(g.x[1:], g.y[1:], g.z[1:])
+        for k in ("U", "V", "W"):
+            ch.upload(k, getattr(st, k)[1:, 1:, 1:])
+        ch.compute_dt()
+        ch.compute_heaviside()
+        ch.set_scalars(dPdx=st.dPdx, t=0.0, Qflow_x_0=st.Qflow_x_0)
+        ch.set_mode(precond=c3d.lib.PRECOND_BAND)
+        ch.compute_time_step_RK3(10)
+        for _ in range(10):
+            ibo.compute_time_step_RK3_ib(g, st, ib, 1e-3)
+        res = {k: rel(ch.download(k), getattr(st, k)[1:, 1:, 1:]) for k in ("U", "V", "W")}
+        res["fb"] = rel(ch.download("FB"), ib.fb)
+        res["max_div"] = ch.check_divergence()
+        out["ib_wall_standing_wave_34x49x14_10steps"] = res
+    return out
+
+
 IB_CONFIGS = {
     # cfg2: the 192x129x192 channel with an immersed plane at y = 0.2 above the
     # lower wall (y = -0.8 in wall-centred coordinates), 192x192 markers,
-    # standing wave 0.02 sin(2 pi x/Lx) cos(2 pi t/5); uniform wall buffer
-    # (grid_type 2) so the delta stencils of the plane lie in uniform y cells
+    # standing wave 0.02 sin(2 pi x/Lx) cos(2 pi t/5).  The IB operators take
+    # the y pivot and delta width from dymin (src/immersed_boundary_operators.f90:
+    # 35-37, 86-89), so every stencil must lie in uniform y cells: grid_type 2
+    # with min_buffer_width 0.45 makes the wall buffer uniform up to y = 0.26,
+    # above the plane's highest stencil row (0.22 + 2.5 dymin = 0.245).  With a
+    # 0.3 buffer (uniform only up to 0.18) the plane sits in stretched cells,
+    # the operators are inconsistent there and the Schur system is indefinite
     "cfg2": dict(grid=(194, 129, 194), Lxp=4.0 * math.pi, Lzp=4.0 * math.pi / 3.0, nu=1.0 / 5600.0,
-                 grid_type=2, alpha_stretch=2.0, min_buffer_width=0.3, body_type="wall_standing_wave",
+                 grid_type=2, alpha_stretch=2.0, min_buffer_width=0.45, body_type="wall_standing_wave",
                  nxb=192, nzb=192, body_param_1=0.02, body_param_2=2 * math.pi / 5, body_param_3=1.0,
                  body_param_4=0.2,
                  desc="plane y=0.2, 192x192 markers, standing wave A=0.02 omega=2pi/5"),
@@ -191,9 +275,10 @@ IB_CONFIGS = {
                  desc="two counter-rotating z cylinders r=0.15 at (1.5,0), (3.0,0.3), 2x200x128 markers"),
     # cfg4: Re_tau=550 channel 384x257x384 (Lx=2pi, Lz=pi, nu=1/20000), 16x8
     # wall-mounted plates of height 0.1, 32x16 markers each, tip amplitude 0.01,
-    # seeded phases
+    # seeded phases; the wall buffer (min_buffer_width 0.25) is uniform up to
+    # y = 0.139, above the plates' highest stencil row (0.1 + 2.5 dymin)
     "cfg4": dict(grid=(386, 257, 386), Lxp=2.0 * math.pi, Lzp=math.pi, nu=1.0 / 20000.0, grid_type=2,
-                 alpha_stretch=2.0, min_buffer_width=0.05, body_type="wall_plates", nxb=16, nzb=8,
+                 alpha_stretch=2.0, min_buffer_width=0.25, body_type="wall_plates", nxb=16, nzb=8,
                  body_param_1=0.1, body_param_2=0.01, body_param_3=2 * math.pi, body_param_4=7,
                  desc="16x8 wall plates h=0.1, 32x16 markers each, tip amplitude 0.01"),
 }
@@ -311,8 +396,9 @@ def run_reference(args):
         "unit": "steps/s", "n_gpus": args.gpus, "steps": n, "warmup": args.warmup,
         "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": [NX, NY, NZ], "poisson": "fp64",
-                   "l2": "working set > L2"},
+        "config": {"workload": WORKLOAD, "grid": [NX, NY, NZ], "cells": (NX - 2) * (NY - 1) * (NZ - 2),
+                   "poisson": "fp64", "parallelism": f"replicas x{args.gpus}",
+                   "l2": "working set > L2 (no flush)"},
         "cpu_baseline": {"value": val, "unit": "steps/s", "cores": threads, "kind": "port",
                          "sample": f"{n} full RK3 steps of the workload ({args.steps} requested) on the "
                                    "C++/OpenMP restatement of the reference's step, "
@@ -432,6 +518,7 @@ def run_ours(args):
     extras = {}
     if ws == 1 and not args.no_extras:
         extras["mixed_vs_fp64"] = measure_mixed()
+        extras["accuracy"] = measure_accuracy()
         extras["ib_schur"] = measure_ib(maxit=args.ib_maxit, cfgs=tuple(args.ib_cfgs.split(",")))
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

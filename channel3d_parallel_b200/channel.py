@@ -372,12 +372,15 @@ class Channel:
 
     # ---- learned preconditioner of the Schur solve ----
     def precond_collect(self, enable=True, max_store=48, max_sets=16):
-        """Collect (residual, correction) moments from converged Schur solves."""
+        """While enabled, every band the solver probes (PRECOND_BAND solves)
+        is kept as a training set of the learned preconditioner (at most
+        ``max_sets``; ``max_store`` is unused)."""
         self._check(self._lib.c3d_precond_collect(self.handle, int(bool(enable)), int(max_store),
                                                   int(max_sets)))
 
     def precond_probe(self):
-        """Add one training set of probed (correction, response) moments."""
+        """Probe the band of the Schur operator at the current geometry (unit
+        corrections and their Schur responses) and keep it as a training set."""
         self._check(self._lib.c3d_precond_probe(self.handle))
 
     def precond_train(self, epochs=400, lr=2e-3):

@@ -908,9 +908,9 @@ int c3d_set_mode(int id, int poisson_mode, int precond_mode) {
   if (poisson_mode != C3D_POISSON_FP64 && poisson_mode != C3D_POISSON_MIXED &&
       poisson_mode != C3D_POISSON_MIXED_UNREFINED) RET(h, C3D_ERR_PARAM);
   if (precond_mode < C3D_PRECOND_NONE || precond_mode > C3D_PRECOND_BAND) RET(h, C3D_ERR_PARAM);
-  if (precond_mode == C3D_PRECOND_BAND && h->ib && !band_supported(h)) {
-    h->last_error = "C3D_PRECOND_BAND needs a marker lattice whose geometry repeats along z "
-                    "(every body type except wall_plates)";
+  if ((precond_mode == C3D_PRECOND_BAND || precond_mode == C3D_PRECOND_LEARNED) && h->ib && !band_supported(h)) {
+    h->last_error = "C3D_PRECOND_BAND and C3D_PRECOND_LEARNED need a marker lattice whose geometry repeats "
+                    "along z (every body type except wall_plates)";
     RET(h, C3D_ERR_UNSUPPORTED);
   }
   if (poisson_mode != C3D_POISSON_FP64) {

@@ -57,7 +57,6 @@ struct IbState {
   // preconditioner: per-marker 4x4 blocks [nb][4][4] acting on
   // (r[b], r[nb+b], r[2nb+b], r[3nb+b]); the Jacobi blocks are diagonal
   double* jac_blk = nullptr;
-  double* lrn_blk = nullptr;
   double* spai_blk = nullptr;        // probed block sparse approximate inverse
   double* prb = nullptr;             // [4][4nb] probe responses of one colour class
   bool have_jac = false, have_lrn = false;
@@ -73,11 +72,12 @@ struct IbState {
 };
 
 
-// learned-preconditioner entry points used by the Schur solver (k_mlp.cu)
-int mlp_build_blocks(Handle* h, double dt);               // lrn_blk from the network
-bool mlp_collecting(const Handle* h);                     // training-pair collection on
-int mlp_store_iterate(Handle* h, const double* x, const double* r, int k);
-int mlp_collect_solve(Handle* h, int iters_stored);       // moments from the stored iterates
+// learned-preconditioner entry points used by the Schur solver (k_mlp.cu):
+// the band factors from the network's prediction at the current geometry,
+// and, while collection is on, a training set from each probed band
+int mlp_build_band(Handle* h, double dt);
+bool mlp_collecting(const Handle* h);
+int mlp_add_probe_set(Handle* h);
 // probe pass of the Schur operator (k_ib.cu): Jacobi and SPAI blocks, and,
 // when mom is not null, per-marker SPAI moments [nb][36]
 int ib_probe(Handle* h, double dt, float* mom);
@@ -88,8 +88,13 @@ int band_build(Handle* h, double dt);
 bool band_stale(Handle* h, double dt);
 void band_invalidate(Handle* h);
 int band_apply(Handle* h, const double* in, double* out);
-double* band_T(Handle* h);
-int band_factor_T(Handle* h, double dt);
+struct BandView {
+  int lat = 0, nzl = 0, nq = 0;   // lattice columns, z rows, z wavenumbers 0..nzl/2
+  const int* nbr = nullptr;       // [lat][5] neighbour columns d = -2..2
+  double2* That = nullptr;        // [nq][80 lat] band symbol, L = ((cp lat + i1) 5 + d) 4 + c
+};
+BandView band_view(Handle* h);
+int band_factor_symbol(Handle* h, double dt);
 int band_probe_count(Handle* h);
 void band_free(IbState* s);
 

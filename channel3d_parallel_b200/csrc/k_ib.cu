@@ -1300,7 +1300,6 @@ int ib_create(Handle* h) {
   for (auto v : vecs)
     if ((rc = dev_alloc(h, v, 4 * (int64_t)nb))) return rc;
   if ((rc = dev_alloc(h, &s->jac_blk, 16 * (int64_t)nb))) return rc;
-  if ((rc = dev_alloc(h, &s->lrn_blk, 16 * (int64_t)nb))) return rc;
   if ((rc = dev_alloc(h, &s->spai_blk, 16 * (int64_t)nb))) return rc;
   if ((rc = dev_alloc(h, &s->red, 2 * kIbRedBlocks + 16))) return rc;
   if ((rc = dev_alloc(h, &s->ticket, 1))) return rc;
@@ -1616,49 +1615,55 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
   const unsigned gm = (unsigned)((nb + 255) / 256);
   int rc;
   int mode = h->precond_mode;
-  if (mode == C3D_PRECOND_LEARNED && !s->have_lrn) {
-    if ((rc = mlp_build_blocks(h, dt))) return rc;
-  }
-  if (mode != C3D_PRECOND_NONE && mode != C3D_PRECOND_BAND && jacobi_stale(h, dt)) {
-    if ((rc = build_jacobi(h, dt))) return rc;
-  }
-  const double* blk = mode == C3D_PRECOND_LEARNED ? s->lrn_blk
-                      : mode == C3D_PRECOND_JACOBI ? s->jac_blk
-                      : mode == C3D_PRECOND_SPAI   ? s->spai_blk : nullptr;
-  bool band = mode == C3D_PRECOND_BAND;
-  double* x = s->fb;
   if (!s->ev_a) {
     C3D_CUDA_TRY(h, cudaEventCreate(&s->ev_a));
     C3D_CUDA_TRY(h, cudaEventCreate(&s->ev_b));
   }
-  if (band && band_stale(h, dt)) {
+  // band factors: probed (BAND) when stale, or predicted by the network
+  // (LEARNED) at every new geometry; timed as preconditioner builds
+  const bool need_probe = mode == C3D_PRECOND_BAND && band_stale(h, dt);
+  const bool need_learn = mode == C3D_PRECOND_LEARNED && !s->have_lrn;
+  if (need_probe || need_learn) {
     C3D_CUDA_TRY(h, cudaEventRecord(s->ev_a, h->stream));
-    if ((rc = band_build(h, dt))) return rc;
+    if (need_probe) {
+      if ((rc = band_build(h, dt))) return rc;
+      if (mlp_collecting(h) && (rc = mlp_add_probe_set(h))) return rc;
+    } else if ((rc = mlp_build_band(h, dt))) {
+      if (rc != C3D_ERR_NAN) return rc;
+      // the predicted band is singular: the probed band takes over
+      h->stats.precond_fallbacks++;
+      mode = C3D_PRECOND_BAND;
+      if ((rc = band_build(h, dt))) return rc;
+    }
     C3D_CUDA_TRY(h, cudaEventRecord(s->ev_b, h->stream));
     C3D_CUDA_TRY(h, cudaEventSynchronize(s->ev_b));
     float bms = 0.f;
     C3D_CUDA_TRY(h, cudaEventElapsedTime(&bms, s->ev_a, s->ev_b));
     h->stats.precond_build_ms += bms;
+    h->stats.precond_builds += need_learn ? 1 : 0;
   }
+  if ((mode == C3D_PRECOND_JACOBI || mode == C3D_PRECOND_SPAI) && jacobi_stale(h, dt)) {
+    if ((rc = build_jacobi(h, dt))) return rc;
+  }
+  const double* blk = mode == C3D_PRECOND_JACOBI ? s->jac_blk
+                      : mode == C3D_PRECOND_SPAI ? s->spai_blk : nullptr;
+  bool band = mode == C3D_PRECOND_BAND || mode == C3D_PRECOND_LEARNED;
+  double* x = s->fb;
   C3D_CUDA_TRY(h, cudaEventRecord(s->ev_a, h->stream));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(s->scr1, x, 8 * n, cudaMemcpyDeviceToDevice, h->stream));
   if ((rc = bcg_restart(h, b, x, dt, gb))) return rc;
   if (mode == C3D_PRECOND_LEARNED) {
     // warm start x0 += M r0
-    k_apply_blocks<<<gm, 256, 0, h->stream>>>(nb, blk, s->r, s->scr2);
-    C3D_LAUNCH_CHECK(h);
+    if ((rc = band_apply(h, s->r, s->scr2))) return rc;
     k_axpby<<<gb, 256, 0, h->stream>>>(n, 1.0, x, 1.0, s->scr2, x);
     C3D_LAUNCH_CHECK(h);
     if ((rc = bcg_restart(h, b, x, dt, gb))) return rc;
   }
-  const bool collect = mlp_collecting(h);
   const double eps = h->p.cg_tol * h->p.cg_tol;
   double err = 1.0;
-  int it = 0, stored = 0;
+  int it = 0;
   std::vector<double> hist;
   while (it < h->p.cg_max_iter && err >= eps) {
-    if (collect && (rc = mlp_store_iterate(h, x, s->r, stored))) return rc;
-    if (collect) ++stored;
     if ((rc = dot(h, s->rhat, s->r, nullptr, nullptr, 0))) return rc;           // rho_n, bta
     k_bcg_p<<<gb, 256, 0, h->stream>>>(n, s->r, s->p, s->nu, s->ph, nullptr, s->sc);
     C3D_LAUNCH_CHECK(h);
@@ -1700,9 +1705,11 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
         stalled = recent > 0.98 * before;   // squared norms: |r| down < 1 %
       }
       if (broke || stalled) {
+        // the probed band of the current geometry takes over
         h->stats.precond_fallbacks++;
-        mode = C3D_PRECOND_JACOBI;
-        blk = s->jac_blk;
+        mode = C3D_PRECOND_BAND;
+        if ((rc = band_build(h, dt))) return rc;
+        s->have_lrn = false;
         if (broke)   // the iterate may be polluted: restart from the entry guess
           C3D_CUDA_TRY(h, cudaMemcpyAsync(x, s->scr1, 8 * n, cudaMemcpyDeviceToDevice, h->stream));
         if ((rc = bcg_restart(h, b, x, dt, gb))) return rc;
@@ -1711,7 +1718,6 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
       }
     }
   }
-  if (collect && err < eps && (rc = mlp_collect_solve(h, stored))) return rc;
   C3D_CUDA_TRY(h, cudaEventRecord(s->ev_b, h->stream));
   C3D_CUDA_TRY(h, cudaEventSynchronize(s->ev_b));
   float ms = 0.f;
@@ -1740,14 +1746,16 @@ int ib_precond_apply(Handle* h, const double* in, double* out, double dt) {
     if (band_stale(h, dt) && (rc = band_build(h, dt))) return rc;
     return band_apply(h, in, out);
   }
+  if (mode == C3D_PRECOND_LEARNED) {
+    if (!s->have_lrn && (rc = mlp_build_band(h, dt))) return rc;
+    return band_apply(h, in, out);
+  }
   if (mode == C3D_PRECOND_NONE) {
     C3D_CUDA_TRY(h, cudaMemcpyAsync(out, in, 8 * n, cudaMemcpyDeviceToDevice, h->stream));
     return 0;
   }
-  if (mode == C3D_PRECOND_LEARNED && !s->have_lrn && (rc = mlp_build_blocks(h, dt))) return rc;
   if (jacobi_stale(h, dt) && (rc = build_jacobi(h, dt))) return rc;
-  const double* blk = mode == C3D_PRECOND_LEARNED ? s->lrn_blk
-                      : mode == C3D_PRECOND_JACOBI ? s->jac_blk : s->spai_blk;
+  const double* blk = mode == C3D_PRECOND_JACOBI ? s->jac_blk : s->spai_blk;
   k_apply_blocks<<<(unsigned)((nb + 255) / 256), 256, 0, h->stream>>>(nb, blk, in, out);
   C3D_LAUNCH_CHECK(h);
   return 0;

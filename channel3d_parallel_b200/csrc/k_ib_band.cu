@@ -51,6 +51,7 @@ constexpr int kKu = kKl;
 constexpr int kKv = kKl + kKu;               // 38
 constexpr int kLdab = 2 * kKl + kKu + 1;     // 58
 constexpr int kSolveChunk = 16;              // band columns staged per copy in the solve
+constexpr int kSolveRing = 8;                // chunks in flight (seven ahead of the one in use)
 constexpr int kFactorWin = 64;               // band columns resident in the factor kernel
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -262,51 +263,93 @@ __global__ void __launch_bounds__(256) k_band_factor(int lat, int nseg, const in
   }
 }
 
-// rhs[q][4 pos(i1) + c] = sum_iz v[c nb + i1 + lat iz] exp(-2 pi i q iz / nzl)
-__global__ void k_band_fwd(int nb, int lat, int nzl, int nq, const double* __restrict__ tw,
-                           const int* __restrict__ pos, const double* __restrict__ v, double2* __restrict__ rhs) {
-  const int64_t tot = (int64_t)nq * 4 * lat;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
-    const int i1 = (int)(t % lat);
-    int64_t r = t / lat;
-    const int c = (int)(r % 4);
-    const int q = (int)(r / 4);
-    const double* vp = v + (int64_t)c * nb + i1;
+// rhs[q][4 pos(i1) + c] = sum_iz v[c nb + i1 + lat iz] exp(-2 pi i q iz / nzl).
+// A CTA takes 32 lattice columns of one component and a run of kFwdQ
+// wavenumbers: the columns' z lines (nzl x 32) and the twiddles are staged
+// in shared memory (coalesced along the columns), each thread sums the DFT
+// of one column for kFwdQ/8 wavenumbers.
+constexpr int kFwdQ = 16;
+__global__ void __launch_bounds__(256) k_band_fwd(int nb, int lat, int nzl, int nq, const double* __restrict__ tw,
+                                                  const int* __restrict__ pos, const double* __restrict__ v,
+                                                  double2* __restrict__ rhs) {
+  extern __shared__ double fsm[];
+  double* xs = fsm;                    // [nzl][32]
+  double* twc = fsm + 32 * nzl;        // [nzl]
+  double* tws = twc + nzl;             // [nzl]
+  const int c = blockIdx.y;
+  const int m0 = blockIdx.x * 32;
+  const int q0 = blockIdx.z * kFwdQ;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < 32 * nzl; e += 256) {
+    const int iz = e >> 5, mm = e & 31;
+    xs[e] = (m0 + mm < lat) ? v[(int64_t)c * nb + m0 + mm + (int64_t)lat * iz] : 0.0;
+  }
+  for (int e = tid; e < nzl; e += 256) { twc[e] = tw[e]; tws[e] = tw[nzl + e]; }
+  __syncthreads();
+  const int mm = tid & 31, ql = tid >> 5;
+  if (m0 + mm >= lat) return;
+  const int row = 4 * pos[m0 + mm] + c;
+  for (int qq = ql; qq < kFwdQ; qq += 8) {
+    const int q = q0 + qq;
+    if (q >= nq) break;
     double re = 0.0, im = 0.0;
     int k = 0;
     for (int iz = 0; iz < nzl; ++iz) {
-      const double x = vp[(int64_t)lat * iz];
-      re += x * tw[k];
-      im -= x * tw[nzl + k];
+      const double xv = xs[iz * 32 + mm];
+      re += xv * twc[k];
+      im -= xv * tws[k];
       k += q;
       if (k >= nzl) k -= nzl;
     }
-    rhs[(int64_t)q * 4 * lat + 4 * pos[i1] + c] = make_double2(re, im);
+    rhs[(int64_t)q * 4 * lat + row] = make_double2(re, im);
   }
 }
 
 // v[c nb + i1 + lat iz] = (1/nzl) sum_q w_q Re(rhs[q][..] exp(+2 pi i q iz / nzl)),
 // w_q = 2 except q = 0 and q = nzl/2 (even nzl): the real inverse transform
-// of a Hermitian spectrum
-__global__ void k_band_inv(int nb, int lat, int nzl, int nq, const double* __restrict__ tw,
-                           const int* __restrict__ pos, const double2* __restrict__ rhs, double* __restrict__ v) {
-  const int64_t tot = (int64_t)4 * nb;
+// of a Hermitian spectrum.  A CTA takes 32 columns of one component and a
+// run of kInvZ z rows; the columns' spectra (nq x 32) and the twiddles are
+// staged in shared memory.
+constexpr int kInvZ = 32;
+__global__ void __launch_bounds__(256) k_band_inv(int nb, int lat, int nzl, int nq, const double* __restrict__ tw,
+                                                  const int* __restrict__ pos, const double2* __restrict__ rhs,
+                                                  double* __restrict__ v) {
+  extern __shared__ double ism[];
+  double2* xs = reinterpret_cast<double2*>(ism);   // [nq][32]
+  double* twc = ism + 2 * 32 * nq;                 // [nzl]
+  double* tws = twc + nzl;
+  const int c = blockIdx.y;
+  const int m0 = blockIdx.x * 32;
+  const int z0 = blockIdx.z * kInvZ;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < 32 * nq; e += 256) {
+    const int q = e >> 5, mm = e & 31;
+    double2 xv = make_double2(0.0, 0.0);
+    if (m0 + mm < lat) {
+      xv = rhs[(int64_t)q * 4 * lat + 4 * pos[m0 + mm] + c];
+      const double w = (q == 0 || 2 * q == nzl) ? 1.0 : 2.0;
+      xv.x *= w;
+      xv.y *= w;
+    }
+    xs[e] = xv;
+  }
+  for (int e = tid; e < nzl; e += 256) { twc[e] = tw[e]; tws[e] = tw[nzl + e]; }
+  __syncthreads();
+  const int mm = tid & 31, zl = tid >> 5;
+  if (m0 + mm >= lat) return;
   const double inv = 1.0 / nzl;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(t / nb);
-    const int l = (int)(t - (int64_t)c * nb);
-    const int i1 = l % lat, iz = l / lat;
-    const double2* rp = rhs + 4 * pos[i1] + c;
+  for (int zz = zl; zz < kInvZ; zz += 8) {
+    const int iz = z0 + zz;
+    if (iz >= nzl) break;
     double acc = 0.0;
     int k = 0;
     for (int q = 0; q < nq; ++q) {
-      const double2 x = rp[(int64_t)q * 4 * lat];
-      const double w = (q == 0 || 2 * q == nzl) ? 1.0 : 2.0;
-      acc += w * (x.x * tw[k] - x.y * tw[nzl + k]);
+      const double2 xv = xs[q * 32 + mm];
+      acc += xv.x * twc[k] - xv.y * tws[k];
       k += iz;
       if (k >= nzl) k -= nzl;
     }
-    v[t] = acc * inv;
+    v[(int64_t)c * nb + m0 + mm + (int64_t)lat * iz] = acc * inv;
   }
 }
 
@@ -319,14 +362,23 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // Forward and back substitution of one system (LAPACK zgbtrs, no transpose)
-// by one warp, the band columns streamed through shared memory in chunks of
-// kSolveChunk (double-buffered cp.async), the right-hand side resident.
+// by one warp.  The substitutions are sequential in the row index, so the
+// entries they are working on stay in registers: in the forward pass lane p
+// holds b[i] for the 32 rows i = j .. j+31 with i = p (mod 32) (the kl = 19
+// rows a step updates are inside), in the backward pass two registers per
+// lane hold the 64 rows j-63 .. j (the kv = 38 rows above the diagonal are
+// inside).  A step is one shuffle (the pivot value to every lane, plus two
+// for a row interchange) and a complex multiply-add per lane; the lane that
+// finishes a row stores it and loads the row 32 (64) further on.  The band
+// columns are streamed through a shared-memory ring of kSolveRing chunks of
+// kSolveChunk columns (cp.async, seven chunks ahead).
 __global__ void __launch_bounds__(32) k_band_solve(int lat, int nseg, const int* __restrict__ segstart,
                                                    const int* __restrict__ seglen, const double2* __restrict__ AB,
                                                    const int* __restrict__ ipiv, double2* __restrict__ rhs) {
   extern __shared__ double2 sm[];
-  double2* buf = sm;                                   // [2][kSolveChunk][kLdab]
-  double2* b = sm + 2 * kSolveChunk * kLdab;           // [m]
+  double2* buf = sm;                                           // [kSolveRing][kSolveChunk][kLdab]
+  double2* b = sm + kSolveRing * kSolveChunk * kLdab;          // [m]
+  int* spiv = reinterpret_cast<int*>(b + 4 * lat);             // [m] (m <= 4 lat)
   const int q = blockIdx.x / nseg, s = blockIdx.x % nseg;
   const int m = 4 * seglen[s];
   const int base = 4 * segstart[s];
@@ -334,63 +386,100 @@ __global__ void __launch_bounds__(32) k_band_solve(int lat, int nseg, const int*
   const int* piv = ipiv + (int64_t)q * 4 * lat + base;
   double2* x = rhs + (int64_t)q * 4 * lat + base;
   const int lane = threadIdx.x;
-  for (int e = lane; e < m; e += 32) b[e] = x[e];
+  const double2 zero = make_double2(0.0, 0.0);
+  for (int e = lane; e < m; e += 32) { b[e] = x[e]; spiv[e] = piv[e]; }
   const int nch = (m + kSolveChunk - 1) / kSolveChunk;
-  auto load_chunk = [&](int ch, int slot) {
-    const int c0 = ch * kSolveChunk;
-    const int nc = min(kSolveChunk, m - c0);
-    const double2* src = A + (int64_t)c0 * kLdab;
-    double2* dst = buf + slot * kSolveChunk * kLdab;
-    for (int e = lane; e < nc * kLdab; e += 32) cp_async16(dst + e, src + e);
+  auto load_chunk = [&](int ch) {
+    if (ch >= 0 && ch < nch) {
+      const int c0 = ch * kSolveChunk;
+      const int nc = min(kSolveChunk, m - c0);
+      const double2* src = A + (int64_t)c0 * kLdab;
+      double2* dst = buf + (ch % kSolveRing) * kSolveChunk * kLdab;
+      for (int e = lane; e < nc * kLdab; e += 32) cp_async16(dst + e, src + e);
+    }
     cp_async_commit();
   };
-  // forward: b := L^-1 P b
-  load_chunk(0, 0);
+  auto shfl2 = [](double2 v, int src) {
+    return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+  };
+  // ---- forward: b := L^-1 P b
+  for (int c = 0; c < kSolveRing - 1; ++c) load_chunk(c);
+  __syncwarp();
+  double2 w = lane < m ? b[lane] : zero;       // row lane (rows i = p mod 32 in the window)
   for (int ch = 0; ch < nch; ++ch) {
-    if (ch + 1 < nch) load_chunk(ch + 1, (ch + 1) & 1); else cp_async_commit();
-    cp_async_wait<1>();
+    load_chunk(ch + kSolveRing - 1);
+    cp_async_wait<kSolveRing - 1>();
     __syncwarp();
-    const double2* cb = buf + (ch & 1) * kSolveChunk * kLdab;
+    const double2* cb = buf + (ch % kSolveRing) * kSolveChunk * kLdab;
     const int c0 = ch * kSolveChunk;
     const int nc = min(kSolveChunk, m - c0);
     for (int jj = 0; jj < nc; ++jj) {
       const int j = c0 + jj;
-      if (j >= m - 1) break;
-      const int l = piv[j];
-      if (lane == 0 && l != j) { const double2 tmp = b[l]; b[l] = b[j]; b[j] = tmp; }
-      __syncwarp();
-      const double2 bj = b[j];
-      const int lm = min(kKl, m - 1 - j);
-      if (lane < lm) b[j + 1 + lane] = csub(b[j + 1 + lane], cmul(cb[jj * kLdab + kKv + 1 + lane], bj));
-      __syncwarp();
+      const int pj = j & 31;
+      if (j < m - 1) {
+        const int lm = min(kKl, m - 1 - j);
+        // this lane's row i = j + t with t in 1..31 (t = 0 is the pivot row)
+        const int t = (lane - pj) & 31;
+        const double2 lv = (t >= 1 && t <= lm) ? cb[jj * kLdab + kKv + t] : zero;
+        const int l = spiv[j] - j;              // row interchange with row j + l
+        if (l != 0) {
+          const int pl = (pj + l) & 31;
+          const double2 vj = shfl2(w, pj), vl = shfl2(w, pl);
+          if (lane == pj) w = vl;
+          if (lane == pl) w = vj;
+        }
+        const double2 bj = shfl2(w, pj);
+        if (t >= 1 && t <= lm) w = csub(w, cmul(lv, bj));
+      }
+      // row j is final: store it, take row j + 32
+      if (lane == pj) {
+        b[j] = w;
+        w = (j + 32 < m) ? b[j + 32] : zero;
+      }
     }
-    __syncwarp();
   }
   cp_async_wait<0>();
   __syncwarp();
-  // backward: b := U^-1 b (the stored diagonal is the reciprocal)
-  load_chunk(nch - 1, 0);
+  // ---- backward: b := U^-1 b (the stored diagonal is the reciprocal); row
+  // i lives in lane i mod 32, register (i / 32) mod 2, for the 64 rows
+  // j-63 .. j
+  for (int k = 0; k < kSolveRing - 1; ++k) load_chunk(nch - 1 - k);
+  double2 w0 = zero, w1 = zero;
+  for (int i = lane; i < m; i += 32)
+    if (i >= m - 64) {
+      if (((i >> 5) & 1) == 0) w0 = b[i]; else w1 = b[i];
+    }
+  __syncwarp();
   for (int k = 0; k < nch; ++k) {
     const int ch = nch - 1 - k;
-    if (ch - 1 >= 0) load_chunk(ch - 1, (k + 1) & 1); else cp_async_commit();
-    cp_async_wait<1>();
+    load_chunk(ch - (kSolveRing - 1));
+    cp_async_wait<kSolveRing - 1>();
     __syncwarp();
-    const double2* cb = buf + (k & 1) * kSolveChunk * kLdab;
+    const double2* cb = buf + (ch % kSolveRing) * kSolveChunk * kLdab;
     const int c0 = ch * kSolveChunk;
     const int nc = min(kSolveChunk, m - c0);
     for (int jj = nc - 1; jj >= 0; --jj) {
       const int j = c0 + jj;
       const double2* col = cb + jj * kLdab;
-      if (lane == 0) b[j] = cmul(b[j], col[kKv]);
-      __syncwarp();
-      const double2 bj = b[j];
-      for (int t = lane + 1; t <= kKv; t += 32) {
-        const int i = j - t;
-        if (i >= 0) b[i] = csub(b[i], cmul(col[kKv - t], bj));
+      const int pj = j & 31;
+      // this lane's rows: ia = the largest i <= j with i = lane (mod 32), ib = ia - 32
+      const int ta = (j - lane) & 31;             // j - ia, 0..31
+      const int ia = j - ta, ib = ia - 32;
+      const bool a0 = ((ia >> 5) & 1) == 0;       // ia's register (meaningful for ia >= 0)
+      double2 va = a0 ? w0 : w1, vb = a0 ? w1 : w0;
+      const double2 ua = (ta >= 1) ? col[kKv - ta] : zero;            // ta <= 31 < kKv
+      const double2 ub = (ta + 32 <= kKv) ? col[kKv - ta - 32] : zero;
+      if (ta == 0) va = cmul(va, col[kKv]);      // lane pj: row j divided by its pivot
+      const double2 bj = shfl2(va, pj);
+      if (ta >= 1 && ia >= 0) va = csub(va, cmul(ua, bj));
+      if (ta + 32 <= kKv && ib >= 0) vb = csub(vb, cmul(ub, bj));
+      if (ta == 0) {                              // row j is final: store it, take row j - 64
+        b[j] = va;
+        va = (j - 64 >= 0) ? b[j - 64] : zero;
       }
-      __syncwarp();
+      w0 = a0 ? va : vb;
+      w1 = a0 ? vb : va;
     }
-    __syncwarp();
   }
   cp_async_wait<0>();
   __syncwarp();
@@ -434,6 +523,14 @@ static bool lattice_segments(const IbState* s, const Params& p, std::vector<int>
   return true;
 }
 
+// shared memory of the solve: the band ring, the right-hand side and the pivots
+static size_t solve_smem_bytes(int lat) {
+  return sizeof(double2) * ((size_t)kSolveRing * kSolveChunk * kLdab + 4 * (size_t)lat) + sizeof(int) * 4 * (size_t)lat;
+}
+
+static size_t fwd_smem_bytes(int nzl) { return sizeof(double) * (32 * (size_t)nzl + 2 * (size_t)nzl); }
+static size_t inv_smem_bytes(int nzl, int nq) { return sizeof(double) * (64 * (size_t)nq + 2 * (size_t)nzl); }
+
 static int band_setup(Handle* h) {
   IbState* s = h->ib;
   if (s->band) return 0;
@@ -446,7 +543,10 @@ static int band_setup(Handle* h) {
   B->nzl = s->nb / lat;
   B->nq = B->nzl / 2 + 1;
   B->nseg = (int)B->seg_start.size();
-  if (B->nzl * lat != s->nb) { B->ok = false; return 0; }
+  if (B->nzl * lat != s->nb || solve_smem_bytes(lat) > 220 * 1024 || fwd_smem_bytes(B->nzl) > 220 * 1024) {
+    B->ok = false;
+    return 0;
+  }
   // folded positions, neighbours, colours
   std::vector<int> pos(lat), seg(lat), nbr((size_t)lat * kNd), col((size_t)4 * lat);
   for (int sgi = 0; sgi < B->nseg; ++sgi) {
@@ -514,9 +614,12 @@ static int band_setup(Handle* h) {
   C3D_CUDA_TRY(h, cudaMemcpyAsync(B->colour_d, col.data(), 4 * col.size(), cudaMemcpyHostToDevice, st));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(B->tw_d, tw.data(), 8 * tw.size(), cudaMemcpyHostToDevice, st));
   C3D_CUDA_TRY(h, cudaStreamSynchronize(st));
-  const int smax = *std::max_element(B->seg_len.begin(), B->seg_len.end());
-  const size_t solve_smem = sizeof(double2) * (2 * kSolveChunk * kLdab + 4 * (size_t)smax);
+  const size_t solve_smem = solve_smem_bytes(lat);
   C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_band_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem));
+  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_band_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)fwd_smem_bytes(nzl)));
+  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_band_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)inv_smem_bytes(nzl, nq)));
   C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_band_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(sizeof(double2) * kFactorWin * kLdab)));
   return 0;
@@ -607,33 +710,53 @@ int band_apply(Handle* h, const double* in, double* out) {
   IbState* s = h->ib;
   BandState* B = s->band;
   const int lat = B->lat, nzl = B->nzl, nq = B->nq, nb = s->nb;
-  const int64_t nr = (int64_t)nq * 4 * lat;
-  k_band_fwd<<<(unsigned)((nr + 127) / 128), 128, 0, h->stream>>>(nb, lat, nzl, nq, B->tw_d, B->pos_d, in, B->rhs_d);
+  const unsigned nmc = (unsigned)((lat + 31) / 32);
+  k_band_fwd<<<dim3(nmc, 4, (unsigned)((nq + kFwdQ - 1) / kFwdQ)), 256, fwd_smem_bytes(nzl), h->stream>>>(
+      nb, lat, nzl, nq, B->tw_d, B->pos_d, in, B->rhs_d);
   C3D_LAUNCH_CHECK(h);
-  const int smax = *std::max_element(B->seg_len.begin(), B->seg_len.end());
-  const size_t smem = sizeof(double2) * (2 * kSolveChunk * kLdab + 4 * (size_t)smax);
+  const size_t smem = solve_smem_bytes(lat);
   k_band_solve<<<nq * B->nseg, 32, smem, h->stream>>>(lat, B->nseg, B->segstart_d, B->seglen_d, B->AB_d,
                                                       B->ipiv_d, B->rhs_d);
   C3D_LAUNCH_CHECK(h);
-  k_band_inv<<<(unsigned)((4 * (int64_t)nb + 127) / 128), 128, 0, h->stream>>>(nb, lat, nzl, nq, B->tw_d, B->pos_d,
-                                                                              B->rhs_d, out);
+  k_band_inv<<<dim3(nmc, 4, (unsigned)((nzl + kInvZ - 1) / kInvZ)), 256, inv_smem_bytes(nzl, nq), h->stream>>>(
+      nb, lat, nzl, nq, B->tw_d, B->pos_d, B->rhs_d, out);
   C3D_LAUNCH_CHECK(h);
   return 0;
 }
 
-// Raw access for the learned preconditioner: the band entries T (caller
-// fills them) and the factorisation.
-double* band_T(Handle* h) { return (h->ib && h->ib->band) ? h->ib->band->T_d : nullptr; }
-int band_factor_T(Handle* h, double dt) {
-  int rc = band_factor_from_T(h);
-  if (rc) return rc;
+// Access for the learned preconditioner (k_mlp.cu): the lattice, the
+// neighbour table and the band symbol That, which the network fills before
+// band_factor_symbol factors it.
+BandView band_view(Handle* h) {
+  BandView v{};
+  if (!band_supported(h)) return v;
+  BandState* B = h->ib->band;
+  v.lat = B->lat; v.nzl = B->nzl; v.nq = B->nq;
+  v.nbr = B->nbr_d; v.That = B->That_d;
+  return v;
+}
+
+// factor the band systems from the symbol in That (filled by the network);
+// the factors are then those of the learned band, not of a probe
+int band_factor_symbol(Handle* h, double dt) {
   IbState* s = h->ib;
   BandState* B = s->band;
-  B->built = true;
-  B->yb_at = s->yb;
-  B->xb_at = s->xb;
-  B->dt_at = dt;
-  B->builds++;
+  const int lat = B->lat, nq = B->nq;
+  const unsigned gb = 148 * 8;
+  C3D_CUDA_TRY(h, cudaMemsetAsync(B->AB_d, 0, sizeof(double2) * (size_t)nq * kLdab * 4 * lat, h->stream));
+  k_band_assemble<<<gb, 256, 0, h->stream>>>(lat, nq, B->nbr_d, B->pos_d, B->seg_d, B->segstart_d, B->That_d,
+                                             B->AB_d);
+  C3D_LAUNCH_CHECK(h);
+  C3D_CUDA_TRY(h, cudaMemsetAsync(B->flag_d, 0, 4, h->stream));
+  k_band_factor<<<nq * B->nseg, 256, sizeof(double2) * kFactorWin * kLdab, h->stream>>>(
+      lat, B->nseg, B->segstart_d, B->seglen_d, B->AB_d, B->ipiv_d, B->flag_d);
+  C3D_LAUNCH_CHECK(h);
+  int flag = 0;
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(&flag, B->flag_d, 4, cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (flag) { h->last_error = "learned band preconditioner: singular band system"; return C3D_ERR_NAN; }
+  // the factors no longer are a probe of the current geometry
+  B->built = false;
   return 0;
 }
 int band_probe_count(Handle* h) {

@@ -2,30 +2,38 @@
 // forces (the solve itself: compute_IB_projection / bicgstab,
 // src/projection.f90:48-186; the reference has no preconditioner).
 //
-// Model.  For marker b the preconditioner is a 4x4 block acting on the
-// marker's residual components r_b = (r[b], r[nb+b], r[2nb+b], r[3nb+b]):
-//   z_b = A_b r_b,   A_b = diag(sig_e) Ahat(g_b) diag(1/sig_r),
-// where g_b are 32 geometry features of the marker (position within the
-// staggered cells, normal, surface element, spacing ratios, wall distance)
-// and Ahat is the output of an MLP 32 -> 128 -> 128 -> 16 (ReLU), BF16
-// weights and activations, FP32 accumulation on the tensor cores.  The
-// preconditioner is linear in r, so BiCGSTAB keeps its usual form.
+// Model.  The preconditioner is the banded z-Fourier one of k_ib_band.cu --
+// an exact solve with S restricted to lattice neighbours |d| <= 2 along the
+// marker rows or rings, per z wavenumber q -- with the band symbol predicted
+// by a network instead of measured by probing S:
+//   That(q)[cp][i1][d][c] = sig_T[q][cp][c] * MLP(g(i1, d, q))[cp][c] + D,
+// where g are 32 features of the column marker i1, its neighbour nbr(i1, d),
+// their offset, d and the wavenumber q, the MLP is 32 -> 128 -> 128 -> 16
+// (ReLU) with BF16 weights and
+// activations and FP32 accumulation on the tensor cores, and D is the part
+// of S known exactly without probing: -E1nH_ext and -E1nHc_ext on the
+// diagonal (src/projection.f90:126,140).  The geometries repeat along z and
+// are symmetric under z -> -z, so the symbol of a block is real when neither
+// or both of cp, c is the w component and imaginary otherwise: the network
+// predicts that one part per block.  It is linear in r, so BiCGSTAB keeps
+// its form; the prediction costs one forward pass and a band factorisation,
+// no Schur applications, so it is rebuilt at every new geometry where a
+// probed band would be reused for several steps.
 //
-// Training data.  While collection is on, every iterate (x_k, r_k) of a
-// converged solve is kept; afterwards e_k = x* - x_k solves S e_k = r_k, and
-// with rh = r_k/|r_k|, eh = e_k/|r_k| each marker accumulates the moments
-//   Crr = sum rh rh^T,  Cer = sum eh rh^T,  Cee = diag sum eh eh^T.
-// The least-squares loss of A_b over all pairs is then
-//   L = sum_b tr(A Crr A^T) - 2 tr(A Cer^T) + tr(Cee),
-// normalised by sum_b tr(Cee); dL/dA = 2 (A Crr - Cer).  One geometry (one
-// solve) forms one training set of nb markers.
+// Training data.  Each probe of the band (the solver's own unit corrections
+// e and their Schur responses S e, 56 per geometry) gives one training set:
+// the rows (i1, d, q) of one geometry with their measured symbol.  The
+// loss is the squared error of the normalised 4x4 blocks, written in the
+// moment form of a linear least-squares model, L = tr(A Crr A^T) - 2 tr(A
+// Cer^T) + tr(Cee) with Crr = I, Cer = target, Cee = its squares, normalised
+// by sum tr(Cee); dL/dA = 2 (A Crr - Cer).
 //
-// Kernels.  k_mlp_fwd: one CTA per 128 markers, three tcgen05.mma GEMMs
-// (M = 128 markers) with operands in shared memory (K-major, no swizzle) and
+// Kernels.  k_mlp_fwd: one CTA per 128 rows, three tcgen05.mma GEMMs
+// (M = 128 rows) with operands in shared memory (K-major, no swizzle) and
 // the accumulator in tensor memory.  k_mlp_bwd: persistent CTAs, per tile the
 // data-gradient GEMMs dH2 = dO W3, dH1 = dZ2 W2 (K-major) and the weight
 // gradients dW3^T = H2^T dO, dW2 = dZ2^T H1, dW1 = dZ1^T X (MN-major
-// operands, K = markers) accumulated in tensor memory across tiles.
+// operands, K = rows) accumulated in tensor memory across tiles.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -58,29 +66,30 @@ struct MlpState {
   float* m = nullptr;        // Adam moments
   float* v = nullptr;
   __nv_bfloat16* wb = nullptr;   // BF16 operand copies
-  float sig_r[4] = {1, 1, 1, 1}, sig_e[4] = {1, 1, 1, 1};
+  float sig_r[4] = {1, 1, 1, 1}, sig_e[4] = {1, 1, 1, 1};   // moment scales (ones for the band model)
   int adam_t = 0;
   bool trained = false;
-  // training sets
-  int nb = 0, cap_sets = 0, nsets = 0, next_set = 0;
-  __nv_bfloat16* feats = nullptr;   // [cap_sets*nb][F]
-  float* mom = nullptr;             // [cap_sets*nb][36]
+  // training sets: rows (i1, d, q, part) of one geometry each
+  int rows_per_set = 0, cap_sets = 0, nsets = 0, next_set = 0;
+  __nv_bfloat16* feats = nullptr;   // [cap_sets*rows][F]
+  float* mom = nullptr;             // [cap_sets*rows][36]
+  std::vector<float> sig_T;         // target scale per (q, cp, c), fixed by the first set
+  bool have_sigT = false;
+  float* sigT_d = nullptr;
   // training scratch
   int cap_rows = 0;
   __nv_bfloat16 *H1 = nullptr, *H2 = nullptr, *dO = nullptr;
   float* out = nullptr;             // [rows][O]
   double* lossacc = nullptr;        // [2]: loss, normaliser
-  // collection
+  // collection of probe sets during band-preconditioned solves
   bool collecting = false;
-  int max_store = 0;
-  double *xs = nullptr, *rs = nullptr, *rn = nullptr;   // stored iterates and |r_k|
-  int64_t pairs = 0;
-  int kind = -1;                    // pairs of the sets: 0 solver iterates, 1 probes (SPAI target)
+  int64_t pairs = 0;                // probe pairs (unit correction, Schur response) behind the sets
   double last_loss = -1.0;
   int epochs = 0;
   // inference scratch
-  __nv_bfloat16* fq = nullptr;      // [nb][F]
-  float* oq = nullptr;              // [nb][O]
+  int q_rows = 0;
+  __nv_bfloat16* fq = nullptr;      // [rows][F]
+  float* oq = nullptr;              // [rows][O]
   int* err = nullptr;               // device error flag (bounded waits)
   float* sig_d = nullptr;           // sig_r, sig_e on the device
   // caller-data evaluation scratch
@@ -557,116 +566,123 @@ __global__ void k_mlp_pack(const float* __restrict__ w, __nv_bfloat16* __restric
 }
 
 // ---------------------------------------------------------------------------
-// geometry features of the markers
+// band rows: features, training moments, prediction scatter
 // ---------------------------------------------------------------------------
-struct FeatArgs {
-  const double *xb, *yb, *zb, *nrm, *sb;
-  const double* yf;    // y faces, Fortran index 1..ny at yf[0..ny-1]
-  int ny, nb;
-  double dx, dz, dymin, Ly, dtnu;
-  __nv_bfloat16* F;    // [nb][32]
+// row r = (i1*5 + d)*nq + q; markers i1 and nbr(i1, d) at z row 0
+struct LbArgs {
+  int lat, nzl, nq, nb, ny;
+  const int* nbr;
+  const double *xb, *yb, *nrm;
+  const int* yref;
+  const double* yf;    // y faces, Fortran-indexed: yf[1] = y(1) .. yf[ny] = y(ny)
+  double dx, dymin, dz, Lxp;
 };
 
-__global__ void k_mlp_features(FeatArgs a) {
+__device__ __forceinline__ void lb_marker(const LbArgs& a, int l, float* f) {
   const double tp = 6.283185307179586;
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < a.nb; b += gridDim.x * blockDim.x) {
-    const double x = a.xb[b], y = a.yb[b], z = a.zb[b];
-    // y cell containing the marker
-    int lo = 0, hi = a.ny - 1;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (a.yf[mid] <= y) lo = mid; else hi = mid;
-    }
-    const double dyl = a.yf[hi] - a.yf[lo];
-    const double fy = (y - a.yf[lo]) / dyl;
-    const double fx = x / a.dx - floor(x / a.dx), fz = z / a.dz - floor(z / a.dz);
-    const double nx = a.nrm[b], ny = a.nrm[a.nb + b], nz = a.nrm[2 * a.nb + b];
-    const double wd = fmax(fmin(y - a.yf[0], a.yf[a.ny - 1] - y), 1e-12);
+  const double yv = (a.yb[l] - a.yf[a.yref[l]]) / a.dymin;
+  const double fv = yv - floor(yv);
+  const double xv = a.xb[l] / a.dx;
+  const double fx = xv - floor(xv);
+  f[0] = (float)sin(tp * fv); f[1] = (float)cos(tp * fv);
+  f[2] = (float)sin(2 * tp * fv); f[3] = (float)cos(2 * tp * fv);
+  f[4] = (float)sin(tp * fx); f[5] = (float)cos(tp * fx);
+  f[6] = (float)sin(2 * tp * fx); f[7] = (float)cos(2 * tp * fx);
+  f[8] = (float)a.nrm[l]; f[9] = (float)a.nrm[a.nb + l];
+}
+
+// block (cp, c) of the symbol is imaginary when exactly one of cp, c is w
+__device__ __forceinline__ int lb_imag(int cp, int c) { return (cp == 2) != (c == 2); }
+
+__global__ void k_lb_features(LbArgs a, __nv_bfloat16* __restrict__ F) {
+  const int64_t rows = (int64_t)a.lat * 5 * a.nq;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int q = (int)(r % a.nq);
+    const int64_t t = r / a.nq;
+    const int d = (int)(t % 5);
+    const int i1 = (int)(t / 5);
+    const int j1 = a.nbr[i1 * 5 + d];
     float f[kF];
-    f[0] = 1.f;
-    f[1] = (float)sin(tp * fx); f[2] = (float)cos(tp * fx);
-    f[3] = (float)sin(tp * fy); f[4] = (float)cos(tp * fy);
-    f[5] = (float)sin(tp * fz); f[6] = (float)cos(tp * fz);
-    f[7] = (float)sin(2 * tp * fx); f[8] = (float)cos(2 * tp * fx);
-    f[9] = (float)sin(2 * tp * fy); f[10] = (float)cos(2 * tp * fy);
-    f[11] = (float)sin(2 * tp * fz); f[12] = (float)cos(2 * tp * fz);
-    f[13] = (float)nx; f[14] = (float)ny; f[15] = (float)nz;
-    f[16] = (float)(a.sb[b] / (a.dx * a.dz));
-    f[17] = (float)(log10(a.dtnu / (a.dymin * a.dymin)) / 10.0);
-    f[18] = (float)(a.dx / a.dymin / 10.0);
-    f[19] = (float)(a.dz / a.dymin / 10.0);
-    f[20] = (float)(dyl / a.dymin);
-    f[21] = (float)(wd / a.Ly);
-    f[22] = (float)(log(wd / a.dymin) / 5.0);
-    f[23] = (float)(nx * nx); f[24] = (float)(ny * ny); f[25] = (float)(nz * nz);
-    f[26] = (float)(nx * ny); f[27] = (float)(nx * nz); f[28] = (float)(ny * nz);
-    f[29] = 0.f; f[30] = 0.f; f[31] = 0.f;
+    lb_marker(a, i1, f);
+    lb_marker(a, j1, f + 10);
+    double rx = a.xb[j1] - a.xb[i1];
+    rx -= a.Lxp * rint(rx / a.Lxp);                 // nearest periodic image
+    f[20] = (float)(rx / a.dx);
+    f[21] = (float)((a.yb[j1] - a.yb[i1]) / a.dymin);
+    f[22] = 0.5f * (float)(d - 2);
+    f[23] = 0.5f * (float)abs(d - 2);
+    const double ph = 6.283185307179586 * q / a.nzl;
+    f[24] = (float)cos(ph);
+    f[25] = (float)(ph / 3.141592653589793);
+    f[26] = (float)sin(0.5 * ph);
+    f[27] = (float)(a.dymin / a.dx);
+    f[28] = (float)(a.dz / a.dx);
+    f[29] = 1.f;
+    // distance of the marker to the nearer domain wall (Neumann boundary)
+    const double ylo = a.yf[1], yhi = a.yf[a.ny];
+    const double wd = fmax(fmin(a.yb[i1] - ylo, yhi - a.yb[i1]), 1e-12);
+    f[30] = (float)(wd / (yhi - ylo));
+    f[31] = (float)(log(wd / a.dymin) / 5.0);
 #pragma unroll
-    for (int q = 0; q < kF; ++q) a.F[(size_t)b * kF + q] = __float2bfloat16_rn(f[q]);
+    for (int k = 0; k < kF; ++k) F[r * kF + k] = __float2bfloat16_rn(f[k]);
   }
 }
 
-// A_b = diag(sig_e) Ahat diag(1/sig_r) in FP64 for the solver; networks
-// trained on probe pairs predict A = M^T (the SPAI loss in the same form)
-__global__ void k_mlp_blocks(const float* __restrict__ out, int nb, const float* __restrict__ sig,
-                             int transpose, double* __restrict__ blk) {
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const double a = (double)out[(size_t)b * kO + 4 * i + j] * sig[4 + i] / sig[j];
-        if (transpose) blk[16 * (size_t)b + 4 * j + i] = a;
-        else blk[16 * (size_t)b + 4 * i + j] = a;
-      }
+// exact diagonal part of S at (component c, lattice column i1, z row 0)
+__device__ __forceinline__ double lb_diag(const double* E1nH, const double* E1nHc, int nb, int c, int i1) {
+  return c < 3 ? -E1nH[c * nb + i1] : -E1nHc[i1];
 }
 
-// ---------------------------------------------------------------------------
-// training-pair moments of one converged solve
-// ---------------------------------------------------------------------------
-__global__ void k_mlp_rnorm(const double* __restrict__ rs, int64_t n, double* __restrict__ rn) {
-  const double* r = rs + (size_t)blockIdx.x * n;
-  double acc = 0.0;
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) acc += r[i] * r[i];
-  __shared__ double sa[256];
-  sa[threadIdx.x] = acc;
-  __syncthreads();
-  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-    if (threadIdx.x < st) sa[threadIdx.x] += sa[threadIdx.x + st];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) rn[blockIdx.x] = sqrt(sa[0]);
-}
-
-__global__ void k_mlp_moments(const double* __restrict__ xs, const double* __restrict__ rs,
-                              const double* __restrict__ rn, const double* __restrict__ xstar, int nk,
-                              double rfinal, int nb, float* __restrict__ mom) {
-  const int64_t n = 4 * (int64_t)nb;
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
-    double Crr[16] = {0}, Cer[16] = {0}, Cee[4] = {0};
-    for (int k = 0; k < nk; ++k) {
-      const double nr = rn[k];
-      if (!(nr > 100.0 * rfinal) || !(nr > 0.0)) continue;   // x* must be accurate relative to e_k
-      double r[4], e[4];
-#pragma unroll
+// training moments of one probed geometry: target y = (That - D) / sig_T
+// (the real or the imaginary part of each block) as the 4x4 block (cp, c);
+// Crr = I, Cer = y, Cee_cp = sum_c y^2
+__global__ void k_lb_moments(LbArgs a, const double2* __restrict__ That, const double* __restrict__ E1nH,
+                             const double* __restrict__ E1nHc, const float* __restrict__ sigT,
+                             float* __restrict__ mom) {
+  const int64_t rows = (int64_t)a.lat * 5 * a.nq;
+  const int64_t nl = 80 * (int64_t)a.lat;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int q = (int)(r % a.nq);
+    const int64_t t = r / a.nq;
+    const int d = (int)(t % 5);
+    const int i1 = (int)(t / 5);
+    float* mb = mom + r * kMom;
+    float cee[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int cp = 0; cp < 4; ++cp)
       for (int c = 0; c < 4; ++c) {
-        const int64_t i = (int64_t)c * nb + b;
-        r[c] = rs[(size_t)k * n + i] / nr;
-        e[c] = (xstar[i] - xs[(size_t)k * n + i]) / nr;
+        const double2 v = That[q * nl + (((int64_t)cp * a.lat + i1) * 5 + d) * 4 + c];
+        double y = lb_imag(cp, c) ? v.y : v.x;
+        if (d == 2 && cp == c) y -= lb_diag(E1nH, E1nHc, a.nb, c, i1);
+        const float yn = (float)(y / sigT[16 * q + 4 * cp + c]);
+        mb[16 + 4 * cp + c] = yn;
+        mb[4 * cp + c] = (cp == c) ? 1.f : 0.f;
+        cee[cp] += yn * yn;
       }
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          Crr[4 * i + j] += r[i] * r[j];
-          Cer[4 * i + j] += e[i] * r[j];
-        }
-        Cee[i] += e[i] * e[i];
+    for (int cp = 0; cp < 4; ++cp) mb[32 + cp] = cee[cp];
+  }
+}
+
+// the predicted symbol: That = sig_T * out (in the block's real or
+// imaginary part, the other part zero) + D
+__global__ void k_lb_scatter(LbArgs a, const float* __restrict__ out, const double* __restrict__ E1nH,
+                             const double* __restrict__ E1nHc, const float* __restrict__ sigT,
+                             double2* __restrict__ That) {
+  const int64_t rows = (int64_t)a.lat * 5 * a.nq;
+  const int64_t nl = 80 * (int64_t)a.lat;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int q = (int)(r % a.nq);
+    const int64_t t = r / a.nq;
+    const int d = (int)(t % 5);
+    const int i1 = (int)(t / 5);
+    for (int cp = 0; cp < 4; ++cp)
+      for (int c = 0; c < 4; ++c) {
+        double y = (double)out[r * kO + 4 * cp + c] * sigT[16 * q + 4 * cp + c];
+        double2 v = make_double2(0.0, 0.0);
+        if (lb_imag(cp, c)) v.y = y;
+        else v.x = y;
+        if (d == 2 && cp == c) v.x += lb_diag(E1nH, E1nHc, a.nb, c, i1);
+        That[q * nl + (((int64_t)cp * a.lat + i1) * 5 + d) * 4 + c] = v;
       }
-    }
-    float* mb = mom + (size_t)b * kMom;
-    for (int q = 0; q < 16; ++q) { mb[q] = (float)Crr[q]; mb[16 + q] = (float)Cer[q]; }
-    for (int q = 0; q < 4; ++q) mb[32 + q] = (float)Cee[q];
   }
 }
 
@@ -686,14 +702,14 @@ static int mlp_ensure(Handle* h) {
   if ((rc = dev_alloc(h, &M->lossacc, 2))) return rc;
   if ((rc = dev_alloc(h, &M->err, 1))) return rc;
   if ((rc = dev_alloc(h, &M->sig_d, 8))) return rc;
-  // He-initialised hidden layers, output layer at zero with Ahat = I via b3
+  // He-initialised hidden layers, output layer near zero (the prediction
+  // starts at the exactly known diagonal part of the band)
   std::vector<float> w(kNParam, 0.f);
   std::mt19937 gen(12345);
   std::normal_distribution<float> nd(0.f, 1.f);
   for (int i = 0; i < kH * kF; ++i) w[kOffW1 + i] = nd(gen) * std::sqrt(2.f / kF);
   for (int i = 0; i < kH * kH; ++i) w[kOffW2 + i] = nd(gen) * std::sqrt(2.f / kH);
   for (int i = 0; i < kO * kH; ++i) w[kOffW3 + i] = nd(gen) * 1e-3f;
-  for (int i = 0; i < 4; ++i) w[kOffB3 + 5 * i] = 1.f;
   C3D_CUDA_TRY(h, cudaMemcpyAsync(M->w, w.data(), 4 * kNParam, cudaMemcpyHostToDevice, h->stream));
   k_mlp_pack<<<64, 256, 0, h->stream>>>(M->w, M->wb);
   C3D_LAUNCH_CHECK(h);
@@ -775,81 +791,122 @@ static int ensure_rows(Handle* h, int rows) {
   return 0;
 }
 
-static int compute_features(Handle* h, __nv_bfloat16* F, double dt) {
+static LbArgs lb_args(Handle* h, const BandView& v) {
   IbState* s = h->ib;
-  FeatArgs a{};
-  a.xb = s->xb_d; a.yb = s->yb_d; a.zb = s->zb_d; a.nrm = s->nrm_d; a.sb = s->sb_d;
-  a.yf = s->y_d; a.ny = (int)h->y.size(); a.nb = s->nb;
-  a.dx = h->dx; a.dz = h->dz; a.dymin = h->dymin; a.Ly = h->p.Ly_channel; a.dtnu = dt * h->p.nu;
-  a.F = F;
-  k_mlp_features<<<(s->nb + 127) / 128, 128, 0, h->stream>>>(a);
-  C3D_LAUNCH_CHECK(h);
+  LbArgs a{};
+  a.lat = v.lat; a.nzl = v.nzl; a.nq = v.nq; a.nb = s->nb; a.ny = h->d.ny;
+  a.nbr = v.nbr; a.xb = s->xb_d; a.yb = s->yb_d; a.nrm = s->nrm_d; a.yref = s->yref_d;
+  a.yf = s->y_d; a.dx = h->dx; a.dymin = h->dymin; a.dz = h->dz; a.Lxp = h->Lxp;
+  return a;
+}
+
+static int64_t lb_rows(const BandView& v) { return (int64_t)v.lat * 5 * v.nq; }
+
+static int upload_sigT(Handle* h) {
+  MlpState* S = h->mlp;
+  const int64_t n = (int64_t)S->sig_T.size();
+  int rc = dev_alloc(h, &S->sigT_d, n);
+  if (rc) return rc;
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(S->sigT_d, S->sig_T.data(), 4 * n, cudaMemcpyHostToDevice, h->stream));
   return 0;
 }
 
-int mlp_build_blocks(Handle* h, double dt) {
+// The network's band symbol at the current geometry, factored for the
+// solver (k_ib_band.cu).
+int mlp_build_band(Handle* h, double dt) {
   IbState* s = h->ib;
   int rc;
   if ((rc = mlp_ensure(h))) return rc;
   MlpState* S = h->mlp;
-  if (S->nb != s->nb || S->fq == nullptr) {
-    if ((rc = dev_alloc(h, &S->fq, (int64_t)s->nb * kF))) return rc;
-    if ((rc = dev_alloc(h, &S->oq, (int64_t)s->nb * kO))) return rc;
-    S->nb = s->nb;
+  const BandView v = band_view(h);
+  if (v.lat == 0) { h->last_error = "learned preconditioner: unsupported marker lattice"; return C3D_ERR_UNSUPPORTED; }
+  if (!S->have_sigT) { h->last_error = "learned preconditioner: no training set (precond_probe / collect first)"; return C3D_ERR_PARAM; }
+  const int64_t rows = lb_rows(v);
+  if (S->q_rows < rows) {
+    if ((rc = dev_alloc(h, &S->fq, rows * kF))) return rc;
+    if ((rc = dev_alloc(h, &S->oq, rows * kO))) return rc;
+    S->q_rows = (int)rows;
   }
-  if ((rc = compute_features(h, S->fq, dt))) return rc;
-  if ((rc = mlp_forward(h, S->fq, s->nb, S->oq, nullptr, nullptr))) return rc;
-  if ((rc = upload_sig(h))) return rc;
-  k_mlp_blocks<<<(s->nb + 255) / 256, 256, 0, h->stream>>>(S->oq, s->nb, S->sig_d, S->kind == 1 ? 1 : 0,
-                                                           s->lrn_blk);
+  const LbArgs a = lb_args(h, v);
+  const unsigned gb = (unsigned)std::min<int64_t>((rows + 255) / 256, 148 * 8);
+  k_lb_features<<<gb, 256, 0, h->stream>>>(a, S->fq);
+  C3D_LAUNCH_CHECK(h);
+  if ((rc = mlp_forward(h, S->fq, (int)rows, S->oq, nullptr, nullptr))) return rc;
+  k_lb_scatter<<<gb, 256, 0, h->stream>>>(a, S->oq, s->E1nH, s->E1nHc, S->sigT_d, v.That);
   C3D_LAUNCH_CHECK(h);
   if ((rc = check_mlp_err(h))) return rc;
+  if ((rc = band_factor_symbol(h, dt))) return rc;
   s->have_lrn = true;
   return 0;
 }
 
 bool mlp_collecting(const Handle* h) { return h->mlp != nullptr && h->mlp->collecting; }
 
-int mlp_store_iterate(Handle* h, const double* x, const double* r, int k) {
+static int ensure_sets(Handle* h, int max_sets, int rows) {
   MlpState* S = h->mlp;
-  if (k >= S->max_store) return 0;
-  const int64_t n = 4 * (int64_t)h->ib->nb;
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(S->xs + (size_t)k * n, x, 8 * n, cudaMemcpyDeviceToDevice, h->stream));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(S->rs + (size_t)k * n, r, 8 * n, cudaMemcpyDeviceToDevice, h->stream));
+  if (S->feats == nullptr || S->cap_sets != max_sets || S->rows_per_set != rows) {
+    int rc;
+    if ((rc = dev_alloc(h, &S->feats, (int64_t)max_sets * rows * kF))) return rc;
+    if ((rc = dev_alloc(h, &S->mom, (int64_t)max_sets * rows * kMom))) return rc;
+    S->cap_sets = max_sets;
+    S->rows_per_set = rows;
+    S->nsets = 0;
+    S->next_set = 0;
+    S->pairs = 0;
+  }
   return 0;
 }
 
-int mlp_collect_solve(Handle* h, int stored) {
-  MlpState* S = h->mlp;
+// One training set from the band just probed (its symbol is in That): the
+// features of the current geometry and the measured blocks as moments.
+int mlp_add_probe_set(Handle* h) {
   IbState* s = h->ib;
-  const int nk = std::min(stored, S->max_store);
-  if (nk <= 0) return 0;
-  const int64_t n = 4 * (int64_t)s->nb;
-  k_mlp_rnorm<<<nk, 256, 0, h->stream>>>(S->rs, n, S->rn);
-  C3D_LAUNCH_CHECK(h);
+  int rc;
+  if ((rc = mlp_ensure(h))) return rc;
+  MlpState* S = h->mlp;
+  const BandView v = band_view(h);
+  if (v.lat == 0) return C3D_ERR_UNSUPPORTED;
+  const int64_t rows = lb_rows(v);
+  if ((rc = ensure_sets(h, S->cap_sets > 0 ? S->cap_sets : 16, (int)rows))) return rc;
+  if (!S->have_sigT) {
+    // target scale per (q, cp, c): the RMS over the lattice columns and
+    // neighbours of the measured block (diagonal part removed), this first set
+    std::vector<double2> th((size_t)v.nq * 80 * v.lat);
+    std::vector<double> e1(3 * (size_t)s->nb), e1c(s->nb);
+    C3D_CUDA_TRY(h, cudaMemcpyAsync(th.data(), v.That, 16 * th.size(), cudaMemcpyDeviceToHost, h->stream));
+    C3D_CUDA_TRY(h, cudaMemcpyAsync(e1.data(), s->E1nH, 8 * e1.size(), cudaMemcpyDeviceToHost, h->stream));
+    C3D_CUDA_TRY(h, cudaMemcpyAsync(e1c.data(), s->E1nHc, 8 * e1c.size(), cudaMemcpyDeviceToHost, h->stream));
+    C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    S->sig_T.assign(16 * (size_t)v.nq, 1.f);
+    const size_t nl = 80 * (size_t)v.lat;
+    for (int q = 0; q < v.nq; ++q)
+      for (int cp = 0; cp < 4; ++cp)
+        for (int c = 0; c < 4; ++c) {
+          const bool im = (cp == 2) != (c == 2);
+          double acc = 0.0;
+          for (int i1 = 0; i1 < v.lat; ++i1)
+            for (int d = 0; d < 5; ++d) {
+              const double2 x = th[q * nl + (((size_t)cp * v.lat + i1) * 5 + d) * 4 + c];
+              double y = im ? x.y : x.x;
+              if (d == 2 && cp == c) y -= c < 3 ? -e1[(size_t)c * s->nb + i1] : -e1c[i1];
+              acc += y * y;
+            }
+          S->sig_T[16 * (size_t)q + 4 * cp + c] = (float)std::sqrt(std::max(acc / (5.0 * v.lat), 1e-60));
+        }
+    S->have_sigT = true;
+    if ((rc = upload_sigT(h))) return rc;
+  }
   const int set = S->next_set;
-  // final residual of this solve: r is in IbState::r
-  double* rfin = S->rn + S->max_store;
-  k_mlp_rnorm<<<1, 256, 0, h->stream>>>(s->r, n, rfin);
+  const LbArgs a = lb_args(h, v);
+  const unsigned gb = (unsigned)std::min<int64_t>((rows + 255) / 256, 148 * 8);
+  k_lb_features<<<gb, 256, 0, h->stream>>>(a, S->feats + (size_t)set * rows * kF);
   C3D_LAUNCH_CHECK(h);
-  double rf = 0.0;
-  std::vector<double> rn(nk);
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(&rf, rfin, 8, cudaMemcpyDeviceToHost, h->stream));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(rn.data(), S->rn, 8 * nk, cudaMemcpyDeviceToHost, h->stream));
-  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  int used = 0;
-  for (int k = 0; k < nk; ++k) used += (rn[k] > 100.0 * rf && rn[k] > 0.0) ? 1 : 0;
-  if (used == 0 || S->kind == 1) return 0;
-  S->kind = 0;
-  k_mlp_moments<<<(s->nb + 127) / 128, 128, 0, h->stream>>>(S->xs, S->rs, S->rn, s->fb, nk, rf, s->nb,
-                                                           S->mom + (size_t)set * s->nb * kMom);
+  k_lb_moments<<<gb, 256, 0, h->stream>>>(a, v.That, s->E1nH, s->E1nHc, S->sigT_d, S->mom + (size_t)set * rows * kMom);
   C3D_LAUNCH_CHECK(h);
-  const double dt = h->dt > 0 ? h->dt : (h->p.CFL < 0 ? -h->p.CFL : 1e-3);
-  int rc = compute_features(h, S->feats + (size_t)set * s->nb * kF, dt);
-  if (rc) return rc;
   S->next_set = (set + 1) % S->cap_sets;
   S->nsets = std::min(S->nsets + 1, S->cap_sets);
-  S->pairs += used;
+  S->pairs += band_probe_count(h);
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return 0;
 }
 
@@ -862,46 +919,24 @@ namespace c3d {
 Handle* lookup_handle(int id);
 }
 
-static int ensure_sets(Handle* h, int max_sets) {
-  MlpState* S = h->mlp;
-  const int nb = h->ib->nb;
-  if (S->feats == nullptr || S->cap_sets != max_sets || S->nb != nb) {
-    int rc;
-    if ((rc = dev_alloc(h, &S->feats, (int64_t)max_sets * nb * kF))) return rc;
-    if ((rc = dev_alloc(h, &S->mom, (int64_t)max_sets * nb * kMom))) return rc;
-    S->cap_sets = max_sets;
-    S->nsets = 0;
-    S->next_set = 0;
-    S->pairs = 0;
-    S->kind = -1;
-    S->nb = nb;
-    S->fq = nullptr;
-  }
-  return 0;
-}
-
+// Probe the band at the current geometry and keep it as one training set.
 extern "C" int c3d_precond_probe(int id) {
   Handle* h = lookup_handle(id);
   if (!h) return C3D_ERR_HANDLE;
   cudaSetDevice(h->device);
   if (!h->ib) { h->last_error = "no immersed body: the learned preconditioner acts on IB solves"; return C3D_ERR_UNSUPPORTED; }
-  int rc;
-  if ((rc = mlp_ensure(h))) return rc;
-  MlpState* S = h->mlp;
-  if (S->feats == nullptr && (rc = ensure_sets(h, 16))) return rc;
-  if (S->kind == 0) { h->last_error = "the collected sets hold iterate pairs; probe pairs cannot be mixed in"; return C3D_ERR_PARAM; }
+  if (!band_supported(h)) {
+    h->last_error = "the learned preconditioner needs a marker lattice whose geometry repeats along z";
+    return C3D_ERR_UNSUPPORTED;
+  }
   const double dt = h->dt > 0 ? h->dt : (h->p.CFL < 0 ? -h->p.CFL : 1e-3);
-  const int set = S->next_set;
-  if ((rc = ib_probe(h, dt, S->mom + (size_t)set * S->nb * kMom))) return rc;
-  if ((rc = compute_features(h, S->feats + (size_t)set * S->nb * kF, dt))) return rc;
-  S->kind = 1;
-  S->next_set = (set + 1) % S->cap_sets;
-  S->nsets = std::min(S->nsets + 1, S->cap_sets);
-  S->pairs += 4 * (int64_t)S->nb;
-  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  return 0;
+  int rc;
+  if ((rc = band_build(h, dt))) return rc;
+  return mlp_add_probe_set(h);
 }
 
+// While enabled, every band the solver probes (C3D_PRECOND_BAND solves)
+// becomes a training set; at most max_sets are kept (the oldest replaced).
 extern "C" int c3d_precond_collect(int id, int enable, int max_store, int max_sets) {
   Handle* h = lookup_handle(id);
   if (!h) return C3D_ERR_HANDLE;
@@ -910,17 +945,15 @@ extern "C" int c3d_precond_collect(int id, int enable, int max_store, int max_se
   int rc;
   if ((rc = mlp_ensure(h))) return rc;
   MlpState* S = h->mlp;
+  (void)max_store;
   if (!enable) { S->collecting = false; return 0; }
-  if (max_store < 1 || max_sets < 1) return C3D_ERR_PARAM;
-  const int nb = h->ib->nb;
-  const int64_t n = 4 * (int64_t)nb;
-  if (S->xs == nullptr || S->max_store < max_store) {
-    if ((rc = dev_alloc(h, &S->xs, (int64_t)max_store * n))) return rc;
-    if ((rc = dev_alloc(h, &S->rs, (int64_t)max_store * n))) return rc;
-    if ((rc = dev_alloc(h, &S->rn, (int64_t)max_store + 1))) return rc;
-    S->max_store = max_store;
+  if (max_sets < 1) return C3D_ERR_PARAM;
+  const BandView v = band_view(h);
+  if (v.lat == 0) {
+    h->last_error = "the learned preconditioner needs a marker lattice whose geometry repeats along z";
+    return C3D_ERR_UNSUPPORTED;
   }
-  if ((rc = ensure_sets(h, max_sets))) return rc;
+  if ((rc = ensure_sets(h, max_sets, (int)lb_rows(v)))) return rc;
   S->collecting = true;
   return 0;
 }
@@ -932,20 +965,11 @@ extern "C" int c3d_precond_train(int id, int epochs, double lr, double* final_lo
   MlpState* S = h->mlp;
   if (!S || S->nsets == 0) { if (h) h->last_error = "no training pairs collected"; return C3D_ERR_PARAM; }
   if (epochs < 1 || !(lr > 0)) return C3D_ERR_PARAM;
-  const int M = S->nsets * S->nb;
+  const int M = S->nsets * S->rows_per_set;
   int rc;
   if ((rc = ensure_rows(h, M))) return rc;
-  // normalisation: sig_r^2 = mean diag Crr, sig_e^2 = mean diag Cee over all markers
-  std::vector<float> mom((size_t)M * kMom);
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(mom.data(), S->mom, 4 * mom.size(), cudaMemcpyDeviceToHost, h->stream));
-  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  double sr[4] = {0}, se[4] = {0};
-  for (int b = 0; b < M; ++b)
-    for (int c = 0; c < 4; ++c) { sr[c] += mom[(size_t)b * kMom + 5 * c]; se[c] += mom[(size_t)b * kMom + 32 + c]; }
-  for (int c = 0; c < 4; ++c) {
-    S->sig_r[c] = (float)std::sqrt(std::max(sr[c] / M, 1e-30));
-    S->sig_e[c] = (float)std::sqrt(std::max(se[c] / M, 1e-30));
-  }
+  // the targets are normalised already (sig_T): unit moment scales
+  for (int i = 0; i < 4; ++i) { S->sig_r[i] = 1.f; S->sig_e[i] = 1.f; }
   if ((rc = upload_sig(h))) return rc;
   const float* sd = S->sig_d;
   double loss = 0, norm = 1;

@@ -4,8 +4,7 @@
  * Every entry point replaces one Fortran module procedure of
  * MetamaterialFSI/channel3D_parallel; the citation beside each declaration
  * names the reference interface (file:line).  The unchanged Fortran driver
- * (app/main.f90) binds these through an ISO_C_BINDING interface module
- * (shown in INTEGRATION.md).
+ * (app/main.f90) binds these through an ISO_C_BINDING interface module.
  *
  * Conventions
  *  - Every function returns int: 0 = OK, < 0 = error (C3D_ERR_*), > 0 =

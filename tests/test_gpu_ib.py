@@ -23,9 +23,10 @@ CASES = {
     "center_wall": dict(nx_global=18, ny_global=33, nz_global=18, Lxp=1.718, Lzp=0.859,
                         grid_type=0, alpha_stretch=0.0, body_type="center_wall", nxb=16, nzb=16,
                         cfl=-0.01),
-    # one plane at y = 0.2 with a standing wave inside the uniform wall buffer of grid type 2
+    # one plane at y = 0.2 with a standing wave inside the uniform wall buffer
+    # of grid type 2 (uniform up to y = 0.42, every stencil row in it)
     "wall_standing_wave": dict(nx_global=34, ny_global=49, nz_global=14, Lxp=2.0, Lzp=0.6,
-                               grid_type=2, alpha_stretch=2.0, min_buffer_width=0.3,
+                               grid_type=2, alpha_stretch=2.0, min_buffer_width=0.45,
                                body_type="wall_standing_wave", nxb=32, nzb=12,
                                body_param_1=0.02, body_param_2=2 * math.pi / 5.0,
                                body_param_3=1.0, body_param_4=0.2, cfl=-1e-3),
@@ -220,3 +221,36 @@ def test_wall_plates_steps():
         assert ch.stats()["bicgstab_solves"] == 6
     finally:
         ch.close()
+
+
+@pytest.mark.parametrize("cfg", ["cfg2", "cfg3"])
+def test_full_size_schur_operator(cfg):
+    """The Schur operator on the full-size IB configurations (192x129x192 with
+    the standing-wave plane, 36,864 markers; 256x129x128 with two rotating
+    cylinders, 51,200 markers) against the oracle at 1e-11: operator set-up,
+    Heaviside fields, spreading, the banded Poisson solve with 255/127-row
+    slabs and the gathers at the sizes the benchmark runs."""
+    import os
+    import sys
+    import channel3d_parallel_b200 as c3d
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    c = dict(bench.IB_CONFIGS[cfg])
+    nx, ny, nz = c.pop("grid")
+    c.pop("desc")
+    nu = c.pop("nu")
+    lx, lz = c.pop("Lxp"), c.pop("Lzp")
+    gt, al = c.pop("grid_type"), c.pop("alpha_stretch")
+    p = co.channel_params(nx, ny, nz, lx, lz, nu, alpha=al, grid_type=gt, cfl=-1e-3, x_mass_cte=1,
+                          **{k.lower(): v for k, v in c.items()})
+    g = co.Grid(p)
+    ib = ibo.IBState(g, p, t=0.0)
+    ibo.compute_heaviside(g, ib)
+    with c3d.Channel(nx_global=nx, ny_global=ny, nz_global=nz, Lxp=lx, Lzp=lz, nu=nu, CFL=-1e-3, x_mass_cte=1,
+                     grid_type=gt, alpha_stretch=al, **c) as ch:
+        ch.set_grid(g.x[1:], g.y[1:], g.z[1:])
+        ch.compute_dt()
+        ch.compute_heaviside()
+        assert ch.dims["nb"] == ib.body.nb
+        f = np.random.default_rng(3).standard_normal(4 * ib.body.nb)
+        assert rel(ch.schur(f), ibo.schur(g, ib, f, 1e-3)) < 1e-11

@@ -358,3 +358,50 @@ def test_compute_pressure(case):
         assert rel(ch.download("P"), st.P[1:, 1:, 1:]) < 1e-10
     finally:
         ch.close()
+
+
+FULL_CASES = {
+    # the IB configurations' channels without the body: 256x129x128 (uniform
+    # y, Lx = 4.5, Lz = 2) and the Re_tau = 550 channel 384x257x384 (Lx = 2 pi,
+    # Lz = pi, nu = 1/20000, tanh y grid): Nx = 256 and 384 x transforms,
+    # Nz = 128 and 384 slabs, and 255 and 127 wall-normal rows per kx slab
+    "cfg3_256x129x128": (258, 129, 130, 4.5, 2.0, 0, 1.0 / 5600.0),
+    "cfg4_384x257x384": (386, 257, 386, 2.0 * math.pi, math.pi, 1, 1.0 / 20000.0),
+}
+
+
+@pytest.mark.parametrize("case", list(FULL_CASES))
+def test_full_size_ib_grids_one_step_parity(case):
+    """One RK3 step on the grids of the IB configurations against the C++
+    restatement of the oracle's step (oracle/cpu_rk3.cpp, checked against the
+    NumPy oracle in tests/test_cpu_restatement.py): U, V, W, P within 1e-10,
+    the mass-flow shift behind dPdx within 2e-15, and max|div u| < 1e-12."""
+    import channel3d_parallel_b200 as c3d
+    from oracle import cpu_rk3
+    nx, ny, nz, lx, lz, gt, nu = FULL_CASES[case]
+    p = co.channel_params(nx, ny, nz, lx, lz, nu, grid_type=gt, alpha=2.0 if gt else 0.0)
+    g = co.Grid(p)
+    st = co.seeded_initial_state(g, p["dpdx"])
+    cpu_rk3.build()
+    cc = cpu_rk3.CpuChannel(g)
+    try:
+        cc.set_state(st)
+        cc.steps(1)
+        with c3d.Channel(nx_global=nx, ny_global=ny, nz_global=nz, Lxp=lx, Lzp=lz, nu=nu, CFL=-1e-3,
+                         x_mass_cte=1, grid_type=gt, alpha_stretch=2.0 if gt else 0.0,
+                         dPdx=p["dpdx"]) as ch:
+            ch.set_grid(g.x[1:], g.y[1:], g.z[1:])
+            for name, ref in (("U", st.U), ("V", st.V), ("W", st.W)):
+                ch.upload(name, ref[1:, 1:, 1:])
+            ch.set_scalars(dPdx=st.dPdx, Qflow_x_0=st.Qflow_x_0)
+            ch.compute_time_step_RK3(1)
+            for name in ("U", "V", "W", "P"):
+                ref = cc.get_field(name)
+                assert rel(ch.download(name), ref[1:, 1:, 1:]) < 1e-10, name
+            # dPdx = (dPdx_old + shift/dt)/2 with the shift Qflow_x_0 - Q a
+            # difference of two unit bulk fluxes: it carries their round-off
+            # divided by dt, so it is compared on the shift (2e-15)
+            assert abs(ch.stats()["dPdx"] - cc.dPdx) <= 2e-15 / 1e-3
+            assert ch.check_divergence() < 1e-12
+    finally:
+        cc.close()

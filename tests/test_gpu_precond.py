@@ -3,10 +3,16 @@
 Network: forward output and parameter gradient of the tcgen05 kernels
 against the CPU oracle with the same BF16 rounding points (tolerance 2e-2
 relative: FP32 accumulation in a different order can move values across a
-BF16 rounding boundary).  Solver: with the learned preconditioner the IB
-steps converge to the same tolerance and match the FP64 oracle (1e-9, as
-the other IB step tests); a network forced to break down (all-zero
-output) falls back to Jacobi and still converges."""
+BF16 rounding boundary).
+
+Solver: the network predicts the band of the Schur operator that the banded
+z-Fourier preconditioner otherwise measures by probing.  Trained on probe
+sets the solver generates, it must reach the same 1e-12 tolerance, match the
+FP64 oracle (1e-10, as the other IB step tests), and need at most half the
+iterations of the Jacobi-preconditioned solve; a network forced to break
+down (non-finite parameters) hands over to the probed band and still
+converges.
+"""
 import numpy as np
 import pytest
 
@@ -41,87 +47,101 @@ def test_network_forward_and_gradient_match_oracle(m):
         assert err < 2e-2, (name, err)
 
 
-def run_oracle(g, st, ib, dt, n):
-    for _ in range(n):
-        ibo.compute_time_step_RK3_ib(g, st, ib, dt)
-
-
-def test_learned_preconditioner_matches_oracle_and_trains():
-    import channel3d_parallel_b200 as c3d
-    p, g, st, ib, ch = build("wall_standing_wave", cg_tol=1e-12, cg_max_iter=400)
-    dt = -p["cfl"]
-    try:
-        # collect from Jacobi-preconditioned solves, then train
-        ch.set_mode(precond=c3d.lib.PRECOND_JACOBI)
-        ch.precond_collect(True, max_store=64, max_sets=8)
-        ch.compute_time_step_RK3(2)
-        info = ch.precond_info()
-        assert info["sets"] >= 1 and info["pairs"] > 0
-        s0 = ch.stats()
-        it_jac = s0["bicgstab_iters"] / s0["bicgstab_solves"]
-        ch.precond_collect(False)
-        loss = ch.precond_train(epochs=300, lr=2e-3)
-        assert 0.0 <= loss < 1.0
-        ch.set_mode(precond=c3d.lib.PRECOND_LEARNED)
-        ch.compute_time_step_RK3(2)
-        s1 = ch.stats()
-        run_oracle(g, st, ib, dt, 4)
-        for name, ref in (("U", st.U), ("V", st.V), ("W", st.W)):
-            assert rel(ch.download(name), ref[1:, 1:, 1:]) < 1e-9, name
-        assert s1["last_residual"] < p["cg_tol"]
-        assert s1["precond_mode"] in (c3d.lib.PRECOND_LEARNED, c3d.lib.PRECOND_JACOBI)
-        it_lrn = (s1["bicgstab_iters"] - s0["bicgstab_iters"]) / (s1["bicgstab_solves"] - s0["bicgstab_solves"])
-        print(f"iterations per solve: jacobi {it_jac:.1f}, learned {it_lrn:.1f}, loss {loss:.3f}")
-    finally:
-        ch.close()
-
-
-def test_broken_network_falls_back_to_jacobi():
-    import channel3d_parallel_b200 as c3d
-    p, g, st, ib, ch = build("wall_standing_wave", cg_tol=1e-12, cg_max_iter=400)
-    dt = -p["cfl"]
-    try:
-        ch.precond_set_params(np.zeros(c3d.lib.PRECOND_NPARAM, np.float32), np.ones(8, np.float32))
-        ch.set_mode(precond=c3d.lib.PRECOND_LEARNED)
-        ch.compute_time_step_RK3(1)
-        s = ch.stats()
-        assert s["precond_fallbacks"] >= 1
-        assert s["last_residual"] < p["cg_tol"]
-        run_oracle(g, st, ib, dt, 1)
-        for name, ref in (("U", st.U), ("V", st.V), ("W", st.W)):
-            assert rel(ch.download(name), ref[1:, 1:, 1:]) < 1e-9, name
-    finally:
-        ch.close()
-
-
 def iters_per_solve(s0, s1):
     return (s1["bicgstab_iters"] - s0["bicgstab_iters"]) / max(1, s1["bicgstab_solves"] - s0["bicgstab_solves"])
 
 
-def test_spai_and_probe_trained_network_match_oracle():
+TOL = 1e-12
+
+
+def count_iters(case, mode, nsteps, warm=0):
     import channel3d_parallel_b200 as c3d
-    p, g, st, ib, ch = build("wall_standing_wave", cg_tol=1e-12, cg_max_iter=400)
+    p, g, st, ib, ch = build(case, cg_tol=TOL, cg_max_iter=600)
+    try:
+        if warm:
+            ch.compute_time_step_RK3(warm)
+        ch.set_mode(precond=mode)
+        s0 = ch.stats()
+        ch.compute_time_step_RK3(nsteps)
+        return iters_per_solve(s0, ch.stats())
+    finally:
+        ch.close()
+
+
+@pytest.mark.parametrize("case,ratio", [("wall_standing_wave", 0.5), ("traveling_wave_x", None)])
+def test_learned_band_trains_and_beats_jacobi(case, ratio):
+    """Training sets: the band probed at five geometries 2 steps apart (the
+    solver's unit corrections and their Schur responses); then three steps
+    with the network's band, which must converge to 1e-12 with no hand-over
+    to the probed band where the geometries repeat closely (the standing
+    wave: at most half the Jacobi iterations), and match the oracle."""
+    import channel3d_parallel_b200 as c3d
+    L = c3d.lib
+    p, g, st, ib, ch = build(case, cg_tol=TOL, cg_max_iter=600)
     dt = -p["cfl"]
     try:
-        res = {}
-        for name, mode in (("jacobi", c3d.lib.PRECOND_JACOBI), ("spai", c3d.lib.PRECOND_SPAI)):
-            ch.set_mode(precond=mode)
-            s0 = ch.stats()
-            ch.compute_time_step_RK3(1)
-            res[name] = iters_per_solve(s0, ch.stats())
-            ch.precond_probe()                     # one training set per geometry
-        loss = ch.precond_train(epochs=400, lr=2e-3)
-        assert 0.0 <= loss < 1.0
-        ch.set_mode(precond=c3d.lib.PRECOND_LEARNED)
+        ch.set_mode(precond=L.PRECOND_BAND)
+        ch.precond_collect(True, max_sets=8)
+        for _ in range(5):
+            ch.precond_probe()
+            ch.compute_time_step_RK3(2)
+        ch.precond_collect(False)
+        info = ch.precond_info()
+        assert info["sets"] >= 5 and info["pairs"] > 0
+        loss = ch.precond_train(epochs=1500, lr=2e-3)
+        assert 0.0 <= loss < 0.05, loss
+        ch.set_mode(precond=L.PRECOND_LEARNED)
         s0 = ch.stats()
-        ch.compute_time_step_RK3(2)
+        ch.compute_time_step_RK3(3)
         s1 = ch.stats()
-        res["learned"] = iters_per_solve(s0, s1)
-        run_oracle(g, st, ib, dt, 4)
+        it_lrn = iters_per_solve(s0, s1)
+        assert s1["last_residual"] < TOL
+        for _ in range(13):
+            ibo.compute_time_step_RK3_ib(g, st, ib, dt)
+        errs = {name: rel(ch.download(name), ref[1:, 1:, 1:])
+                for name, ref in (("U", st.U), ("V", st.V), ("W", st.W))}
+        assert max(errs.values()) < 1e-10, errs
+    finally:
+        ch.close()
+    it_jac = count_iters(case, L.PRECOND_JACOBI, 3, warm=10)
+    it_band = count_iters(case, L.PRECOND_BAND, 3, warm=10)
+    print(f"{case}: iterations per solve jacobi {it_jac:.1f}, probed band {it_band:.1f}, "
+          f"learned {it_lrn:.1f}, loss {loss:.4f}, hand-overs {s1['precond_fallbacks'] - s0['precond_fallbacks']}")
+    if ratio is not None:
+        assert s1["precond_fallbacks"] == s0["precond_fallbacks"]
+        assert it_lrn <= ratio * it_jac, (it_lrn, it_jac)
+
+
+def test_broken_network_hands_over_to_the_probed_band():
+    import channel3d_parallel_b200 as c3d
+    L = c3d.lib
+    p, g, st, ib, ch = build("wall_standing_wave", cg_tol=TOL, cg_max_iter=600)
+    dt = -p["cfl"]
+    try:
+        ch.set_mode(precond=L.PRECOND_BAND)
+        ch.precond_probe()                       # fixes the target scales
+        # a diverged training run: non-finite parameters, so the predicted
+        # band cannot be factored
+        ch.precond_set_params(np.full(L.PRECOND_NPARAM, np.nan, np.float32), np.ones(8, np.float32))
+        ch.set_mode(precond=L.PRECOND_LEARNED)
+        ch.compute_time_step_RK3(1)
+        s = ch.stats()
+        assert s["precond_fallbacks"] >= 1
+        assert s["last_residual"] < TOL
+        ibo.compute_time_step_RK3_ib(g, st, ib, dt)
         for name, ref in (("U", st.U), ("V", st.V), ("W", st.W)):
-            assert rel(ch.download(name), ref[1:, 1:, 1:]) < 1e-9, name
-        assert s1["last_residual"] < p["cg_tol"]
-        print("iterations per solve:", {k: round(v, 1) for k, v in res.items()}, "loss", round(loss, 3),
-              "fallbacks", s1["precond_fallbacks"])
+            assert rel(ch.download(name), ref[1:, 1:, 1:]) < 1e-10, name
+    finally:
+        ch.close()
+
+
+def test_learned_unsupported_for_plates():
+    import channel3d_parallel_b200 as c3d
+    p, g, st, ib, ch = build("wall_plates", cg_max_iter=5)
+    try:
+        with pytest.raises(c3d.C3DError):
+            ch.set_mode(precond=c3d.lib.PRECOND_LEARNED)
+        with pytest.raises(c3d.C3DError):
+            ch.precond_probe()
     finally:
         ch.close()
