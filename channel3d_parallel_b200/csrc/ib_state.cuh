@@ -64,6 +64,14 @@ struct IbState {
   int jac_clipped[4] = {0, 0, 0, 0}; // safeguarded diagonal entries per component
   double dt_at_jac = 0;
   BandState* band = nullptr;         // banded z-Fourier preconditioner
+  // warm start of the learned mode: the last solutions of each RK stage
+  // (newest first) and the stage of the solve in progress (-1: none)
+  static constexpr int kHist = 4;
+  double* hist[3][kHist] = {};
+  int nhist[3] = {0, 0, 0};
+  int stage = -1;
+  int warm_order = -1;               // extrapolation order of the last warm start
+  double* ext_part = nullptr;        // block partials of the extrapolation errors
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;   // Schur-solve timing
   ~IbState() {
     if (ev_a) cudaEventDestroy(ev_a);

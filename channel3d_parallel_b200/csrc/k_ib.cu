@@ -1591,6 +1591,8 @@ static bool jacobi_stale(Handle* h, double dt);
 // kStallWindow iterations is not 1 % below the best before them) or breaks
 // down (non-finite scalars; restart from the entry guess).
 static const int kStallWindow = 20;
+static int learned_warm_start(Handle* h, double* x);
+static int push_history(Handle* h, const double* x);
 
 static int bcg_restart(Handle* h, const double* b, double* x, double dt, unsigned gb) {
   IbState* s = h->ib;
@@ -1650,6 +1652,7 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
   bool band = mode == C3D_PRECOND_BAND || mode == C3D_PRECOND_LEARNED;
   double* x = s->fb;
   C3D_CUDA_TRY(h, cudaEventRecord(s->ev_a, h->stream));
+  if (mode == C3D_PRECOND_LEARNED && (rc = learned_warm_start(h, x))) return rc;
   C3D_CUDA_TRY(h, cudaMemcpyAsync(s->scr1, x, 8 * n, cudaMemcpyDeviceToDevice, h->stream));
   if ((rc = bcg_restart(h, b, x, dt, gb))) return rc;
   if (mode == C3D_PRECOND_LEARNED) {
@@ -1718,6 +1721,7 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
       }
     }
   }
+  if (err == err && (rc = push_history(h, x))) return rc;
   C3D_CUDA_TRY(h, cudaEventRecord(s->ev_b, h->stream));
   C3D_CUDA_TRY(h, cudaEventSynchronize(s->ev_b));
   float ms = 0.f;
@@ -1731,6 +1735,100 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
   h->stats.last_residual = std::sqrt(err);
   if (!(err == err)) { h->last_error = "BiCGSTAB produced a non-finite residual"; return C3D_ERR_NAN; }
   if (it == h->p.cg_max_iter && err >= eps) return C3D_WARN_NOT_CONVERGED;
+  return 0;
+}
+
+// squared errors of the order-0, -1 and -2 extrapolations of the newest
+// solution h0 from the three before it: |h0 - h1|^2, |h0 - (2 h1 - h2)|^2,
+// |h0 - (3 h1 - 3 h2 + h3)|^2, block partials
+__global__ void __launch_bounds__(256) k_extrap_err(const double* __restrict__ h0, const double* __restrict__ h1,
+                                                   const double* __restrict__ h2, const double* __restrict__ h3,
+                                                   int64_t n, double* __restrict__ part) {
+  double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double a = h0[i] - h1[i];
+    const double b = h0[i] - (2.0 * h1[i] - h2[i]);
+    const double c = h0[i] - (3.0 * h1[i] - 3.0 * h2[i] + h3[i]);
+    e0 += a * a;
+    e1 += b * b;
+    e2 += c * c;
+  }
+  __shared__ double sa[3][256];
+  sa[0][threadIdx.x] = e0;
+  sa[1][threadIdx.x] = e1;
+  sa[2][threadIdx.x] = e2;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int q = 0; q < 3; ++q) sa[q][threadIdx.x] += sa[q][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 3; ++q) part[3 * blockIdx.x + q] = sa[q][0];
+}
+
+// x = extrapolation of order 0, 1 or 2 from h0 (newest), h1, h2
+__global__ void k_extrap(int64_t n, int order, const double* __restrict__ h0, const double* __restrict__ h1,
+                         const double* __restrict__ h2, double* __restrict__ x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = order == 0 ? h0[i] : order == 1 ? 2.0 * h0[i] - h1[i] : 3.0 * h0[i] - 3.0 * h1[i] + h2[i];
+}
+
+// Warm start of the learned mode: the surface unknowns are smooth in time at
+// a fixed RK stage, so the solution of this stage is extrapolated from the
+// same stage of the previous steps.  The order (0, 1 or 2) is the one that
+// best predicted the newest stored solution from those before it (chosen
+// on the solver's own past solutions).  Without two stored solutions of the
+// stage the current fb (the reference's warm start) is kept.
+static int learned_warm_start(Handle* h, double* x) {
+  IbState* s = h->ib;
+  const int st = s->stage;
+  s->warm_order = -1;
+  if (st < 0 || s->nhist[st] < 2) return 0;
+  const int64_t n = 4 * (int64_t)s->nb;
+  double** H = s->hist[st];
+  int order = 1;
+  if (s->nhist[st] >= IbState::kHist) {
+    int rc;
+    if (!s->ext_part && (rc = dev_alloc(h, &s->ext_part, 3 * kIbRedBlocks))) return rc;
+    k_extrap_err<<<kIbRedBlocks, 256, 0, h->stream>>>(H[0], H[1], H[2], H[3], n, s->ext_part);
+    C3D_LAUNCH_CHECK(h);
+    std::vector<double> part(3 * kIbRedBlocks);
+    C3D_CUDA_TRY(h, cudaMemcpyAsync(part.data(), s->ext_part, 8 * part.size(), cudaMemcpyDeviceToHost, h->stream));
+    C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    double e[3] = {0, 0, 0};
+    for (int b = 0; b < kIbRedBlocks; ++b)
+      for (int q = 0; q < 3; ++q) e[q] += part[3 * b + q];
+    order = 0;
+    for (int q = 1; q < 3; ++q)
+      if (e[q] < e[order]) order = q;
+  } else if (s->nhist[st] == 2) {
+    order = 1;
+  }
+  if (order == 2 && s->nhist[st] < 3) order = 1;
+  k_extrap<<<148 * 4, 256, 0, h->stream>>>(n, order, H[0], H[1], H[2], x);
+  C3D_LAUNCH_CHECK(h);
+  s->warm_order = order;
+  return 0;
+}
+
+// keep the converged solution of this RK stage (newest first)
+static int push_history(Handle* h, const double* x) {
+  IbState* s = h->ib;
+  const int st = s->stage;
+  if (st < 0) return 0;
+  const int64_t n = 4 * (int64_t)s->nb;
+  int rc;
+  double** H = s->hist[st];
+  if (!H[IbState::kHist - 1]) {
+    for (int k = 0; k < IbState::kHist; ++k)
+      if ((rc = dev_alloc(h, &H[k], n))) return rc;
+  }
+  double* oldest = H[IbState::kHist - 1];
+  for (int k = IbState::kHist - 1; k > 0; --k) H[k] = H[k - 1];
+  H[0] = oldest;
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(H[0], x, 8 * n, cudaMemcpyDeviceToDevice, h->stream));
+  s->nhist[st] = std::min(s->nhist[st] + 1, IbState::kHist);
   return 0;
 }
 
@@ -1866,7 +1964,9 @@ int ib_projection(Handle* h, double dt, int rk_step) {
   if ((rc = gather3(h, G_E, h->U, h->V, h->W, s->rhs, -1.0, nullptr, nullptr, s->ub_d))) return rc;
   if ((rc = gather_c(h, h->P_interim, 1.0, s->rhs + 3 * nb, -1.0))) return rc;
   if ((rc = remove_mean(h, s->rhs + 3 * nb, nullptr))) return rc;
+  s->stage = (rk_step >= 1 && rk_step <= 3) ? rk_step - 1 : -1;
   rc = ib_bicgstab(h, s->rhs, dt);                                              // :60
+  s->stage = -1;
   if (rc < 0) return rc;
   const int warn = rc;
   // R f, divergence, Poisson (P side effect at rk_step 1), final update   :63-94

@@ -58,6 +58,7 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 crcp(double2 a) {
   // 1/a with scaling against overflow (Smith's method)
   if (fabs(a.x) >= fabs(a.y)) {
@@ -87,6 +88,14 @@ struct BandState {
   double2* AB_d = nullptr;         // [nq][ldab * 4 lat]
   int* ipiv_d = nullptr;           // [nq][4 lat]
   double2* rhs_d = nullptr;        // [nq][4 lat]
+  // block-tridiagonal form (16 x 16 blocks: 4 lattice positions x 4 components)
+  std::vector<int> nblk, blkoff;   // block rows per segment, their offset within one q
+  int NBq = 0;                     // block rows per wavenumber (all segments)
+  int* nblk_d = nullptr;
+  int* blkoff_d = nullptr;
+  double2 *Ab_d = nullptr, *Bb_d = nullptr, *Cb_d = nullptr;   // [nq][NBq][16][16]
+  double2 *Pb_d = nullptr, *Gb_d = nullptr;                    // Delta^-1 and Delta^-1 C
+  bool block = false;              // the factors in use are the block ones
   double* tw_d = nullptr;          // [2][nzl] cos, sin of 2 pi k / nzl
   int* flag_d = nullptr;           // [0] zero pivot seen
   bool built = false;
@@ -353,6 +362,150 @@ __global__ void __launch_bounds__(256) k_band_inv(int nb, int lat, int nzl, int 
   }
 }
 
+// ---------------------------------------------------------------------------
+// block-tridiagonal form.  In folded order every band entry couples positions
+// at most 4 apart, so with blocks of 4 consecutive positions (16 rows: 4
+// markers x 4 components) each system is block tridiagonal; a block LU
+// without interchanges between blocks (Gauss-Jordan with partial pivoting
+// inside each 16 x 16 diagonal block) makes the solve 2 x (4 len / 16)
+// dependent block steps instead of 2 x 4 len scalar ones.
+// ---------------------------------------------------------------------------
+constexpr int kBs = 16;
+
+__device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
+
+// scatter the band symbol into the sub-diagonal (A), diagonal (B) and
+// super-diagonal (C) blocks; padding rows of the last block row get a unit
+// diagonal (k_blk_pad)
+__global__ void k_blk_assemble(int lat, int nq, int NBq, const int* __restrict__ nbr, const int* __restrict__ pos,
+                               const int* __restrict__ seg, const int* __restrict__ segstart,
+                               const int* __restrict__ blkoff, const double2* __restrict__ That,
+                               double2* __restrict__ Ab, double2* __restrict__ Bb, double2* __restrict__ Cb) {
+  const int nl = 80 * lat;
+  const int64_t tot = (int64_t)nq * nl;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+    const int L = (int)(t % nl);
+    const int q = (int)(t / nl);
+    const int c = L % 4;
+    int r = L / 4;
+    const int d = r % kNd; r /= kNd;
+    const int i1 = r % lat;
+    const int cp = r / lat;
+    const int sg = seg[i1];
+    const int base = 4 * segstart[sg];
+    const int col = 4 * pos[i1] + c - base;
+    const int row = 4 * pos[nbr[i1 * kNd + d]] + cp - base;
+    const int bi = row / kBs, bj = col / kBs;
+    const int64_t o = ((int64_t)q * NBq + blkoff[sg] + bi) * (kBs * kBs) + (row % kBs) * kBs + (col % kBs);
+    double2* dst = bj < bi ? Ab : (bj == bi ? Bb : Cb);
+    dst[o] = That[t];
+  }
+}
+
+__global__ void k_blk_pad(int nq, int nseg, int NBq, const int* __restrict__ seglen, const int* __restrict__ nblk,
+                          const int* __restrict__ blkoff, double2* __restrict__ Bb) {
+  const int q = blockIdx.x / nseg, sg = blockIdx.x % nseg;
+  const int m = 4 * seglen[sg];
+  const int i = nblk[sg] - 1;
+  const int64_t o = ((int64_t)q * NBq + blkoff[sg] + i) * (kBs * kBs);
+  for (int rr = threadIdx.x; rr < kBs; rr += blockDim.x)
+    if (kBs * i + rr >= m) Bb[o + rr * kBs + rr] = make_double2(1.0, 0.0);
+}
+
+// Block LU of one system: Delta_0 = B_0, Delta_i = B_i - A_i G_{i-1},
+// P_i = Delta_i^-1 (Gauss-Jordan, partial pivoting within the block),
+// G_i = P_i C_i.  A pivot below 1e-12 of the block's largest entry sets
+// flag[1]: the caller then uses the pivoted banded LU instead.
+__global__ void __launch_bounds__(256) k_blk_factor(int nseg, int NBq, const int* __restrict__ nblk,
+                                                    const int* __restrict__ blkoff, const double2* __restrict__ Ab,
+                                                    const double2* __restrict__ Bb, const double2* __restrict__ Cb,
+                                                    double2* __restrict__ Pb, double2* __restrict__ Gb,
+                                                    int* __restrict__ flag) {
+  __shared__ double2 Dm[kBs][2 * kBs];
+  __shared__ double2 Gp[kBs][kBs];
+  __shared__ double2 fk[kBs];
+  __shared__ int s_piv;
+  __shared__ double s_dmax;
+  const int q = blockIdx.x / nseg, sg = blockIdx.x % nseg;
+  const int N = nblk[sg];
+  const int64_t b0 = ((int64_t)q * NBq + blkoff[sg]) * (kBs * kBs);
+  const int tid = threadIdx.x;
+  const int r = tid / kBs, cc = tid % kBs;      // 256 threads: one per block entry
+  for (int i = 0; i < N; ++i) {
+    const int64_t o = b0 + (int64_t)i * kBs * kBs;
+    double2 v = Bb[o + tid];
+    if (i > 0) {
+      const double2* Ai = Ab + o + r * kBs;
+      for (int k = 0; k < kBs; ++k) v = csub(v, cmul(Ai[k], Gp[k][cc]));
+    }
+    Dm[r][cc] = v;
+    Dm[r][kBs + cc] = make_double2(r == cc ? 1.0 : 0.0, 0.0);
+    __syncthreads();
+    if (tid < 32) {
+      double mx = 0.0;
+      for (int e = tid; e < kBs * kBs; e += 32) mx = fmax(mx, cabs1(Dm[e / kBs][e % kBs]));
+      for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      if (tid == 0) s_dmax = mx;
+    }
+    __syncthreads();
+    for (int k = 0; k < kBs; ++k) {
+      if (tid < 32) {
+        double best = -1.0;
+        int bi = k;
+        if (tid >= k && tid < kBs) { best = cabs1(Dm[tid][k]); bi = tid; }
+        for (int off = 16; off > 0; off >>= 1) {
+          const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+          if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        }
+        if (tid == 0) {
+          s_piv = bi;
+          if (!(best > 1e-12 * s_dmax)) atomicExch(flag + 1, 1);
+        }
+      }
+      __syncthreads();
+      const int p = s_piv;
+      if (p != k && tid < 2 * kBs) {
+        const double2 t = Dm[k][tid];
+        Dm[k][tid] = Dm[p][tid];
+        Dm[p][tid] = t;
+      }
+      __syncthreads();
+      const double2 pv = Dm[k][k];
+      const double2 rp = cabs1(pv) > 0.0 ? crcp(pv) : make_double2(0.0, 0.0);
+      __syncthreads();
+      if (tid < 2 * kBs) Dm[k][tid] = cmul(Dm[k][tid], rp);
+      if (tid < kBs) fk[tid] = Dm[tid][k];
+      __syncthreads();
+      for (int e = tid; e < kBs * 2 * kBs; e += 256) {
+        const int rr = e / (2 * kBs), c2 = e % (2 * kBs);
+        if (rr != k) Dm[rr][c2] = csub(Dm[rr][c2], cmul(fk[rr], Dm[k][c2]));
+      }
+      __syncthreads();
+    }
+    Pb[o + tid] = Dm[r][kBs + cc];
+    if (i + 1 < N) {
+      const double2* Ci = Cb + o;
+      double2 g = make_double2(0.0, 0.0);
+      for (int k = 0; k < kBs; ++k) g = cadd(g, cmul(Dm[r][kBs + k], Ci[k * kBs + cc]));
+      Gb[o + tid] = g;
+      __syncthreads();
+      Gp[r][cc] = g;
+    }
+    __syncthreads();
+  }
+}
+
+// Block forward and back substitution of one system by one warp: lane 2r+h
+// forms half (8 terms) of row r's products; the blocks stream through a
+// shared-memory ring (cp.async, kBlkRing - 1 block rows ahead).
+constexpr int kBlkRing = 4;
+__global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, const int* __restrict__ segstart,
+                                                  const int* __restrict__ seglen, const int* __restrict__ nblk,
+                                                  const int* __restrict__ blkoff, const double2* __restrict__ Ab,
+                                                  const double2* __restrict__ Pb, const double2* __restrict__ Gb,
+                                                  double2* __restrict__ rhs);
+
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
@@ -360,6 +513,111 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, const int* __restrict__ segstart,
+                                                  const int* __restrict__ seglen, const int* __restrict__ nblk,
+                                                  const int* __restrict__ blkoff, const double2* __restrict__ Ab,
+                                                  const double2* __restrict__ Pb, const double2* __restrict__ Gb,
+                                                  double2* __restrict__ rhs) {
+  __shared__ __align__(16) double2 ring[kBlkRing][2][kBs * kBs];
+  __shared__ double2 vv[kBs], tt[kBs];
+  const int q = blockIdx.x / nseg, sg = blockIdx.x % nseg;
+  const int N = nblk[sg];
+  const int m = 4 * seglen[sg];
+  const int64_t b0 = ((int64_t)q * NBq + blkoff[sg]) * (kBs * kBs);
+  double2* x = rhs + (int64_t)q * 4 * lat + 4 * segstart[sg];
+  const int lane = threadIdx.x;
+  const int r = lane >> 1, hh = lane & 1;
+  const double2 zero = make_double2(0.0, 0.0);
+  // forward: slot holds (A_i, P_i)
+  auto load_fwd = [&](int i) {
+    if (i >= 0 && i < N) {
+      const int64_t o = b0 + (int64_t)i * kBs * kBs;
+      double2* d0 = ring[i % kBlkRing][0];
+      double2* d1 = ring[i % kBlkRing][1];
+      for (int e = lane; e < kBs * kBs; e += 32) {
+        cp_async16(d0 + e, Ab + o + e);
+        cp_async16(d1 + e, Pb + o + e);
+      }
+    }
+    cp_async_commit();
+  };
+  for (int i = 0; i < kBlkRing - 1; ++i) load_fwd(i);
+  for (int i = 0; i < N; ++i) {
+    load_fwd(i + kBlkRing - 1);
+    cp_async_wait<kBlkRing - 1>();
+    __syncwarp();
+    const double2* Ai = ring[i % kBlkRing][0];
+    const double2* Pi = ring[i % kBlkRing][1];
+    const int row = kBs * i + r;
+    const double2 bv = row < m ? x[row] : zero;
+    double2 acc = zero;
+    if (i > 0)
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const double2 a = Ai[r * kBs + 8 * hh + k], y = vv[8 * hh + k];
+        acc.x += a.x * y.x - a.y * y.y;
+        acc.y += a.x * y.y + a.y * y.x;
+      }
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+    __syncwarp();
+    if (hh == 0) tt[r] = csub(bv, acc);
+    __syncwarp();
+    double2 y2 = zero;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const double2 a = Pi[r * kBs + 8 * hh + k], t = tt[8 * hh + k];
+      y2.x += a.x * t.x - a.y * t.y;
+      y2.y += a.x * t.y + a.y * t.x;
+    }
+    y2.x += __shfl_xor_sync(0xffffffffu, y2.x, 1);
+    y2.y += __shfl_xor_sync(0xffffffffu, y2.y, 1);
+    __syncwarp();
+    if (hh == 0) {
+      vv[r] = y2;
+      if (row < m) x[row] = y2;
+    }
+    __syncwarp();
+  }
+  cp_async_wait<0>();
+  __syncwarp();
+  // backward: x_i = y_i - G_i x_{i+1}; vv holds x_{i+1}
+  auto load_bwd = [&](int i) {
+    if (i >= 0 && i < N - 1) {
+      const int64_t o = b0 + (int64_t)i * kBs * kBs;
+      double2* d0 = ring[i % kBlkRing][0];
+      for (int e = lane; e < kBs * kBs; e += 32) cp_async16(d0 + e, Gb + o + e);
+    }
+    cp_async_commit();
+  };
+  for (int k = 0; k < kBlkRing - 1; ++k) load_bwd(N - 2 - k);
+  for (int i = N - 2; i >= 0; --i) {
+    load_bwd(i - (kBlkRing - 1));
+    cp_async_wait<kBlkRing - 1>();
+    __syncwarp();
+    const double2* Gi = ring[i % kBlkRing][0];
+    double2 acc = zero;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const double2 a = Gi[r * kBs + 8 * hh + k], y = vv[8 * hh + k];
+      acc.x += a.x * y.x - a.y * y.y;
+      acc.y += a.x * y.y + a.y * y.x;
+    }
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+    const int row = kBs * i + r;
+    const double2 yv = row < m ? x[row] : zero;
+    __syncwarp();
+    if (hh == 0) {
+      const double2 xr = csub(yv, acc);
+      vv[r] = xr;
+      if (row < m) x[row] = xr;
+    }
+    __syncwarp();
+  }
+  cp_async_wait<0>();
+}
 
 // Forward and back substitution of one system (LAPACK zgbtrs, no transpose)
 // by one warp.  The substitutions are sequential in the row index, so the
@@ -597,6 +855,22 @@ static int band_setup(Handle* h) {
   if ((rc = dev_alloc(h, &B->AB_d, (int64_t)nq * kLdab * 4 * lat))) return rc;
   if ((rc = dev_alloc(h, &B->ipiv_d, (int64_t)nq * 4 * lat))) return rc;
   if ((rc = dev_alloc(h, &B->rhs_d, (int64_t)nq * 4 * lat))) return rc;
+  B->nblk.resize(B->nseg);
+  B->blkoff.resize(B->nseg);
+  B->NBq = 0;
+  for (int sgi = 0; sgi < B->nseg; ++sgi) {
+    B->nblk[sgi] = (4 * B->seg_len[sgi] + kBs - 1) / kBs;
+    B->blkoff[sgi] = B->NBq;
+    B->NBq += B->nblk[sgi];
+  }
+  const int64_t nbe = (int64_t)nq * B->NBq * kBs * kBs;
+  if ((rc = dev_alloc(h, &B->nblk_d, B->nseg))) return rc;
+  if ((rc = dev_alloc(h, &B->blkoff_d, B->nseg))) return rc;
+  if ((rc = dev_alloc(h, &B->Ab_d, nbe))) return rc;
+  if ((rc = dev_alloc(h, &B->Bb_d, nbe))) return rc;
+  if ((rc = dev_alloc(h, &B->Cb_d, nbe))) return rc;
+  if ((rc = dev_alloc(h, &B->Pb_d, nbe))) return rc;
+  if ((rc = dev_alloc(h, &B->Gb_d, nbe))) return rc;
   if ((rc = dev_alloc(h, &B->tw_d, 2 * (int64_t)nzl))) return rc;
   if ((rc = dev_alloc(h, &B->flag_d, 4))) return rc;
   std::vector<double> tw(2 * (size_t)nzl);
@@ -613,6 +887,8 @@ static int band_setup(Handle* h) {
   C3D_CUDA_TRY(h, cudaMemcpyAsync(B->seglen_d, B->seg_len.data(), 4 * B->nseg, cudaMemcpyHostToDevice, st));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(B->colour_d, col.data(), 4 * col.size(), cudaMemcpyHostToDevice, st));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(B->tw_d, tw.data(), 8 * tw.size(), cudaMemcpyHostToDevice, st));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(B->nblk_d, B->nblk.data(), 4 * B->nseg, cudaMemcpyHostToDevice, st));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(B->blkoff_d, B->blkoff.data(), 4 * B->nseg, cudaMemcpyHostToDevice, st));
   C3D_CUDA_TRY(h, cudaStreamSynchronize(st));
   const size_t solve_smem = solve_smem_bytes(lat);
   C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_band_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem));
@@ -632,14 +908,33 @@ bool band_supported(Handle* h) {
   return s->band && s->band->ok;
 }
 
-// factor the band systems from the entries in T_d
-static int band_factor_from_T(Handle* h) {
+// Factor the band systems from the symbol in That: the block-tridiagonal
+// LU, or, when one of its diagonal blocks has a pivot below 1e-12 of the
+// block's largest entry, the banded LU with partial pivoting.
+static int band_factor_that(Handle* h) {
   IbState* s = h->ib;
   BandState* B = s->band;
-  const int lat = B->lat, nzl = B->nzl, nq = B->nq, nl = 80 * lat;
+  const int lat = B->lat, nq = B->nq;
   const unsigned gb = 148 * 8;
-  k_band_dft_T<<<gb, 256, 0, h->stream>>>(nl, nzl, nq, B->tw_d, B->T_d, B->That_d);
+  const size_t nbe = sizeof(double2) * (size_t)nq * B->NBq * kBs * kBs;
+  C3D_CUDA_TRY(h, cudaMemsetAsync(B->Ab_d, 0, nbe, h->stream));
+  C3D_CUDA_TRY(h, cudaMemsetAsync(B->Bb_d, 0, nbe, h->stream));
+  C3D_CUDA_TRY(h, cudaMemsetAsync(B->Cb_d, 0, nbe, h->stream));
+  k_blk_assemble<<<gb, 256, 0, h->stream>>>(lat, nq, B->NBq, B->nbr_d, B->pos_d, B->seg_d, B->segstart_d,
+                                            B->blkoff_d, B->That_d, B->Ab_d, B->Bb_d, B->Cb_d);
   C3D_LAUNCH_CHECK(h);
+  k_blk_pad<<<nq * B->nseg, 32, 0, h->stream>>>(nq, B->nseg, B->NBq, B->seglen_d, B->nblk_d, B->blkoff_d, B->Bb_d);
+  C3D_LAUNCH_CHECK(h);
+  C3D_CUDA_TRY(h, cudaMemsetAsync(B->flag_d, 0, 8, h->stream));
+  k_blk_factor<<<nq * B->nseg, 256, 0, h->stream>>>(B->nseg, B->NBq, B->nblk_d, B->blkoff_d, B->Ab_d, B->Bb_d,
+                                                    B->Cb_d, B->Pb_d, B->Gb_d, B->flag_d);
+  C3D_LAUNCH_CHECK(h);
+  int flag[2] = {0, 0};
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(flag, B->flag_d, 8, cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  B->block = flag[1] == 0;
+  if (B->block) return 0;
+  // pivoted banded LU
   C3D_CUDA_TRY(h, cudaMemsetAsync(B->AB_d, 0, sizeof(double2) * (size_t)nq * kLdab * 4 * lat, h->stream));
   k_band_assemble<<<gb, 256, 0, h->stream>>>(lat, nq, B->nbr_d, B->pos_d, B->seg_d, B->segstart_d, B->That_d,
                                              B->AB_d);
@@ -648,11 +943,21 @@ static int band_factor_from_T(Handle* h) {
   k_band_factor<<<nq * B->nseg, 256, sizeof(double2) * kFactorWin * kLdab, h->stream>>>(
       lat, B->nseg, B->segstart_d, B->seglen_d, B->AB_d, B->ipiv_d, B->flag_d);
   C3D_LAUNCH_CHECK(h);
-  int flag = 0;
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(&flag, B->flag_d, 4, cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(flag, B->flag_d, 4, cudaMemcpyDeviceToHost, h->stream));
   C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  if (flag) { h->last_error = "band preconditioner: singular band system"; return C3D_ERR_NAN; }
+  if (flag[0]) { h->last_error = "band preconditioner: singular band system"; return C3D_ERR_NAN; }
   return 0;
+}
+
+// factor the band systems from the entries in T_d
+static int band_factor_from_T(Handle* h) {
+  IbState* s = h->ib;
+  BandState* B = s->band;
+  const int lat = B->lat, nzl = B->nzl, nq = B->nq, nl = 80 * lat;
+  const unsigned gb = 148 * 8;
+  k_band_dft_T<<<gb, 256, 0, h->stream>>>(nl, nzl, nq, B->tw_d, B->T_d, B->That_d);
+  C3D_LAUNCH_CHECK(h);
+  return band_factor_that(h);
 }
 
 // Probe the band of S at the current geometry and factor it.
@@ -714,9 +1019,14 @@ int band_apply(Handle* h, const double* in, double* out) {
   k_band_fwd<<<dim3(nmc, 4, (unsigned)((nq + kFwdQ - 1) / kFwdQ)), 256, fwd_smem_bytes(nzl), h->stream>>>(
       nb, lat, nzl, nq, B->tw_d, B->pos_d, in, B->rhs_d);
   C3D_LAUNCH_CHECK(h);
-  const size_t smem = solve_smem_bytes(lat);
-  k_band_solve<<<nq * B->nseg, 32, smem, h->stream>>>(lat, B->nseg, B->segstart_d, B->seglen_d, B->AB_d,
-                                                      B->ipiv_d, B->rhs_d);
+  if (B->block) {
+    k_blk_solve<<<nq * B->nseg, 32, 0, h->stream>>>(lat, B->nseg, B->NBq, B->segstart_d, B->seglen_d, B->nblk_d,
+                                                    B->blkoff_d, B->Ab_d, B->Pb_d, B->Gb_d, B->rhs_d);
+  } else {
+    const size_t smem = solve_smem_bytes(lat);
+    k_band_solve<<<nq * B->nseg, 32, smem, h->stream>>>(lat, B->nseg, B->segstart_d, B->seglen_d, B->AB_d,
+                                                        B->ipiv_d, B->rhs_d);
+  }
   C3D_LAUNCH_CHECK(h);
   k_band_inv<<<dim3(nmc, 4, (unsigned)((nzl + kInvZ - 1) / kInvZ)), 256, inv_smem_bytes(nzl, nq), h->stream>>>(
       nb, lat, nzl, nq, B->tw_d, B->pos_d, B->rhs_d, out);
@@ -739,24 +1049,13 @@ BandView band_view(Handle* h) {
 // factor the band systems from the symbol in That (filled by the network);
 // the factors are then those of the learned band, not of a probe
 int band_factor_symbol(Handle* h, double dt) {
-  IbState* s = h->ib;
-  BandState* B = s->band;
-  const int lat = B->lat, nq = B->nq;
-  const unsigned gb = 148 * 8;
-  C3D_CUDA_TRY(h, cudaMemsetAsync(B->AB_d, 0, sizeof(double2) * (size_t)nq * kLdab * 4 * lat, h->stream));
-  k_band_assemble<<<gb, 256, 0, h->stream>>>(lat, nq, B->nbr_d, B->pos_d, B->seg_d, B->segstart_d, B->That_d,
-                                             B->AB_d);
-  C3D_LAUNCH_CHECK(h);
-  C3D_CUDA_TRY(h, cudaMemsetAsync(B->flag_d, 0, 4, h->stream));
-  k_band_factor<<<nq * B->nseg, 256, sizeof(double2) * kFactorWin * kLdab, h->stream>>>(
-      lat, B->nseg, B->segstart_d, B->seglen_d, B->AB_d, B->ipiv_d, B->flag_d);
-  C3D_LAUNCH_CHECK(h);
-  int flag = 0;
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(&flag, B->flag_d, 4, cudaMemcpyDeviceToHost, h->stream));
-  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  if (flag) { h->last_error = "learned band preconditioner: singular band system"; return C3D_ERR_NAN; }
-  // the factors no longer are a probe of the current geometry
-  B->built = false;
+  (void)dt;
+  int rc = band_factor_that(h);
+  if (rc) {
+    if (rc == C3D_ERR_NAN) h->last_error = "learned band preconditioner: singular band system";
+    return rc;
+  }
+  h->ib->band->built = false;
   return 0;
 }
 int band_probe_count(Handle* h) {
