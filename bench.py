@@ -322,7 +322,7 @@ def measure_ib(maxit=300, steps=2, modes=("none", "jacobi", "band", "learned"), 
                 "total_ms_per_solve": (ms + bms) / ns, "iters_per_step": it / n,
                 "last_residual": s1["last_residual"], "converged": s1["last_residual"] < 1e-10,
                 "fallbacks": s1["precond_fallbacks"] - s0["precond_fallbacks"],
-                "max_div": ch.check_divergence()}
+                "max_div": ch.check_divergence(), "ib_rows": list(s1["ib_rows"])}
 
     out = {}
     for cfg in cfgs:
@@ -343,6 +343,26 @@ def measure_ib(maxit=300, steps=2, modes=("none", "jacobi", "band", "learned"), 
                 res["modes"][name] = {"unavailable": str(e)}
             finally:
                 ch.close()
+        # Bytes of one Schur application on the band of y rows it touches
+        # (the stencil rows and one row either side; Nb = Nx * rows * Nz):
+        # spread writes 3 fields (24 Nb), divergence reads them (24) and
+        # writes the x spectrum (8.08 = 16 B x 97/192 per cell at 192), the
+        # band y-z solve reads and writes it (16.17), the inverse x transform
+        # reads it and writes phi (8.08 + 8), the gathers read phi and the
+        # three fields (32): 120.3 B per band cell.
+        rows = next((m.get("ib_rows") for m in res["modes"].values() if m.get("ib_rows")), None)
+        if rows and rows[1] >= rows[0]:
+            nx, nz = c["grid"][0] - 2, c["grid"][2] - 2
+            spec = 16.0 * (nx // 2 + 1) / nx
+            nb_cells = nx * (rows[1] - rows[0] + 3) * nz
+            per_cell = 24 + 24 + spec + 2 * spec + spec + 8 + 32
+            byt = per_cell * nb_cells
+            res["schur_bytes"] = {"band_rows": rows, "band_cells": nb_cells, "bytes_per_cell": per_cell,
+                                  "bytes_per_application": byt,
+                                  "hbm_ms_per_application": byt / (measured_peaks()[0] * 1e9) * 1e3}
+            for m in res["modes"].values():
+                if "ms_per_iter" in m:
+                    m["iter_frac_of_hbm_bound"] = 2 * res["schur_bytes"]["hbm_ms_per_application"] / m["ms_per_iter"]
         out[cfg] = res
     return out
 
@@ -570,7 +590,7 @@ def main():
                     help="skip the mixed-precision and IB Schur-solve measurements")
     ap.add_argument("--ib-maxit", type=int, default=300,
                     help="BiCGSTAB iteration cap of the IB measurement without the band preconditioner")
-    ap.add_argument("--ib-cfgs", default="cfg2",
+    ap.add_argument("--ib-cfgs", default="cfg2,cfg3,cfg4",
                     help="IB configurations to measure (cfg2, cfg3, cfg4)")
     ap.add_argument("--only-ib", action="store_true",
                     help="only the IB Schur-solve measurement (--steps steps per preconditioner)")

@@ -935,6 +935,7 @@ int c3d_get_stats(int id, c3d_stats* out) {
   h->stats.qflow_y_0 = h->Qflow_y_0; h->stats.qflow_z_0 = h->Qflow_z_0;
   h->stats.slab_cluster[0] = h->sp.cs64; h->stats.slab_cluster[1] = h->sp.cs32;
   h->stats.slab_narrow[0] = h->sp.nw64; h->stats.slab_narrow[1] = h->sp.nw32;
+  ib_rows(h, h->stats.ib_rows);
   *out = h->stats;
   return 0;
 }

@@ -99,6 +99,9 @@ struct SpectralState {
   double *mult = nullptr, *rdp = nullptr;
   float *mult32 = nullptr, *rdp32 = nullptr;
   double *dl = nullptr, *du = nullptr;       // Dyy(j+1, j) and Dyy(j, j+1), j = 0..Ny-1 (0 past the end)
+  // x(j)/y(j) of the homogeneous tail (right-hand side zero from row j on),
+  // same layout as rdp; built on first use by the band-restricted solve
+  double* tail = nullptr;
   float *dl32 = nullptr, *du32 = nullptr;
   // spectra, layout [m][j][k] = [(m*Ny + (j-2))*pz + (k-2)]: one kx slab is
   // Ny rows of pz complex values (pz*sizeof(complex) a multiple of 16 bytes)
@@ -316,6 +319,8 @@ int ib_regT_1n(Handle* h, const double* U, const double* V, const double* W, dou
 int ib_reg(Handle* h, int comp, const double* f_dev, double* F);
 int ib_schur(Handle* h, const double* f_dev, double* Sf_dev, double dt);
 int ib_bicgstab(Handle* h, const double* rhs_dev, double dt);
+// y rows (Fortran j) that the markers' stencils reach; 0 0 without IB
+void ib_rows(const Handle* h, int32_t rows[2]);
 int ib_precond_apply(Handle* h, const double* in_dev, double* out_dev, double dt);
 double* ib_marker_ptr(Handle* h, int id, int64_t* len);
 double* ib_field_ptr(Handle* h, int id);

@@ -71,9 +71,25 @@ struct IbState {
   int nhist[3] = {0, 0, 0};
   int stage = -1;
   int warm_order = -1;               // extrapolation order of the last warm start
+  // LEARNED against the probed band: iterations per solve of the recent
+  // BAND solves, and consecutive LEARNED solves that were slow against them
+  double band_iters_ref = 0.0;
+  int lrn_slow = 0;
   double* ext_part = nullptr;        // block partials of the extrapolation errors
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;   // Schur-solve timing
+  // the BiCGSTAB iteration loop as a CUDA graph (a conditional WHILE node
+  // whose body is one iteration), rebuilt when what it bakes in changes
+  cudaGraph_t bcg_graph = nullptr;
+  cudaGraphExec_t bcg_exec = nullptr;
+  std::vector<double> bcg_key;       // mode, factors, operands, dt, tolerance, stencil rows
+  int64_t bcg_body_launches = 0;     // kernels in one iteration
+  bool bcg_graph_off = false;        // conditional graphs unavailable: host-driven loop
+  int* loop_d = nullptr;             // [0] iterations done, [1] limit of this launch
+  double* hist_d = nullptr;          // squared residual after each iteration
+  int hist_cap = 0;
   ~IbState() {
+    if (bcg_exec) cudaGraphExecDestroy(bcg_exec);
+    if (bcg_graph) cudaGraphDestroy(bcg_graph);
     if (ev_a) cudaEventDestroy(ev_a);
     if (ev_b) cudaEventDestroy(ev_b);
   }
@@ -96,6 +112,7 @@ int band_build(Handle* h, double dt);
 bool band_stale(Handle* h, double dt);
 void band_invalidate(Handle* h);
 int band_apply(Handle* h, const double* in, double* out);
+bool band_is_block(Handle* h);
 struct BandView {
   int lat = 0, nzl = 0, nq = 0;   // lattice columns, z rows, z wavenumbers 0..nzl/2
   const int* nbr = nullptr;       // [lat][5] neighbour columns d = -2..2

@@ -20,6 +20,7 @@
 #include <cstring>
 #include <vector>
 
+#include <climits>
 #include "c3d_internal.cuh"
 #include "ib_state.cuh"
 
@@ -553,8 +554,12 @@ __global__ void __launch_bounds__(128) k_ib_gather(GatherArgs a) {
   const Dims& d = a.d;
   const GField& g = a.f[c];
   double acc = 0.0;
+  // fully unrolled: the stencil tables stay in registers
+#pragma unroll
   for (int qk = 0; qk < 5; ++qk) {
+#pragma unroll
     for (int qj = 0; qj < 5; ++qj) {
+      if (wy[qj] == 0.0 || wz[qk] == 0.0) continue;   // the row adds exactly nothing
       const double wjk = T.scale * wy[qj] * wz[qk];
 #pragma unroll
       for (int qi = 0; qi < 5; ++qi) {
@@ -620,8 +625,10 @@ __global__ void __launch_bounds__(128) k_ib_gather8(GatherArgs a) {
     }
     for (int rr = sub; rr < 25; rr += kGatherLanes) {
       const int qj = rr % 5, qk = rr / 5;
+      const double wy = T.w1[tslot(nb, t, 1, qj, l)], wz = T.w1[tslot(nb, t, 2, qk, l)];
+      if (wy == 0.0 || wz == 0.0) continue;            // the row adds exactly nothing
       const int iy = T.idx[tslot(nb, t, 1, qj, l)], iz = T.idx[tslot(nb, t, 2, qk, l)];
-      const double wjk = T.scale * T.w1[tslot(nb, t, 1, qj, l)] * T.w1[tslot(nb, t, 2, qk, l)];
+      const double wjk = T.scale * wy * wz;
       const double oyz = e1n ? ny_ * T.off[tslot(nb, t, 1, qj, l)] + nz_ * T.off[tslot(nb, t, 2, qk, l)] : 0.0;
 #pragma unroll
       for (int qi = 0; qi < 5; ++qi) {
@@ -668,6 +675,11 @@ enum SpreadMode { S_RAW = 0, S_JUMP = 1, S_NORMAL = 2 };
 // tensor weight w = wx (wy wz) beside each entry.  It is rebuilt whenever the
 // operators are (every RK stage for moving bodies).
 
+// Stencil points whose one-dimensional weight is exactly zero along some
+// axis (the five-point tables hold the delta function's support of four
+// cells plus one point at distance >= 2) contribute exactly nothing and get
+// no entry.
+
 // count the entries of each grid point: one thread per (marker, qj, qk)
 __global__ void k_sp_count(OpTables T, int c, int n1, int n2, int* __restrict__ cnt) {
   const int nb = T.nb;
@@ -676,9 +688,12 @@ __global__ void k_sp_count(OpTables T, int c, int n1, int n2, int* __restrict__ 
   const int l = (int)(gid % nb);
   const int r = (int)(gid / nb);
   const int qj = r % 5, qk = r / 5;
+  if (T.w1[tslot(nb, c, 1, qj, l)] == 0.0 || T.w1[tslot(nb, c, 2, qk, l)] == 0.0) return;
   const int iy = T.idx[tslot(nb, c, 1, qj, l)], iz = T.idx[tslot(nb, c, 2, qk, l)];
 #pragma unroll
-  for (int qi = 0; qi < 5; ++qi) atomicAdd(cnt + lin(n1, n2, T.idx[tslot(nb, c, 0, qi, l)], iy, iz, 0), 1);
+  for (int qi = 0; qi < 5; ++qi)
+    if (T.w1[tslot(nb, c, 0, qi, l)] != 0.0)
+      atomicAdd(cnt + lin(n1, n2, T.idx[tslot(nb, c, 0, qi, l)], iy, iz, 0), 1);
 }
 
 // place the entries (arbitrary order within a point; sorted next)
@@ -690,9 +705,11 @@ __global__ void k_sp_fill(OpTables T, int c, int n1, int n2, const int* __restri
   const int l = (int)(gid % nb);
   const int r = (int)(gid / nb);
   const int qj = r % 5, qk = r / 5;
+  if (T.w1[tslot(nb, c, 1, qj, l)] == 0.0 || T.w1[tslot(nb, c, 2, qk, l)] == 0.0) return;
   const int iy = T.idx[tslot(nb, c, 1, qj, l)], iz = T.idx[tslot(nb, c, 2, qk, l)];
 #pragma unroll
   for (int qi = 0; qi < 5; ++qi) {
+    if (T.w1[tslot(nb, c, 0, qi, l)] == 0.0) continue;
     const int64_t p = lin(n1, n2, T.idx[tslot(nb, c, 0, qi, l)], iy, iz, 0);
     const int slot = off[p] + atomicAdd(cur + p, 1);
     ent[slot] = ((uint32_t)l << 7) | (uint32_t)(qi + 5 * qj + 25 * qk);
@@ -749,9 +766,15 @@ struct SpGather {
 };
 
 // F(i, j, k) = sum over the point's entries of w * amp(marker), for the
-// rows jlo..jhi of up to three fields; points without entries get 0
+// rows jlo..jhi of up to three fields; points without entries get 0.
+// A warp takes 32 consecutive points, whose entries are one contiguous run
+// of the map: the run streams through shared memory in chunks (weights and
+// marker amplitudes loaded by consecutive lanes), and each lane then adds
+// its own point's terms in entry order.
+constexpr int kSpChunk = 128;
 __global__ void __launch_bounds__(256) k_sp_gather(SpGather g0, SpGather g1, SpGather g2, int ncomp,
                                                    const double* __restrict__ amp, int nb) {
+  __shared__ double sw[8][kSpChunk], sa[8][kSpChunk];
   if ((int)blockIdx.y >= ncomp) return;
   // field description of this component, picked member by member (a
   // reference to one of the parameters would copy them to local memory)
@@ -764,19 +787,44 @@ __global__ void __launch_bounds__(256) k_sp_gather(SpGather g0, SpGather g1, SpG
   const int nrow = g.jhi - g.jlo + 1;
   const int64_t tot = (int64_t)g.n1 * nrow * g.n3;
   const double* a = amp + (int64_t)blockIdx.y * nb;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
-    const int i = (int)(t % g.n1);
-    const int64_t r = t / g.n1;
-    const int j = g.jlo + (int)(r % nrow);
-    const int k = (int)(r / nrow);
-    const int64_t p = (int64_t)i + (int64_t)g.n1 * ((j - 1) + (int64_t)g.n2 * k);
-    const int n = g.cnt[p];
-    double acc = 0.0;
-    if (n) {
-      const int o = g.off[p];
-      for (int e = 0; e < n; ++e) acc += g.w[o + e] * a[g.ent[o + e] >> 7];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* ws = sw[warp];
+  double* as = sa[warp];
+  for (int64_t t0 = (blockIdx.x * (int64_t)blockDim.x + warp * 32); t0 < tot;
+       t0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = t0 + lane;
+    const bool valid = t < tot;
+    int64_t p = 0;
+    int n = 0, o = 0;
+    if (valid) {
+      const int i = (int)(t % g.n1);
+      const int64_t r = t / g.n1;
+      const int j = g.jlo + (int)(r % nrow);
+      const int k = (int)(r / nrow);
+      p = (int64_t)i + (int64_t)g.n1 * ((j - 1) + (int64_t)g.n2 * k);
+      n = g.cnt[p];
+      o = g.off[p];
     }
-    g.F[p] = acc;
+    // the warp's run of entries [lo, hi)
+    int lo = n ? o : INT_MAX, hi = n ? o + n : INT_MIN;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, s));
+      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, s));
+    }
+    double acc = 0.0;
+    for (int cb = lo; cb < hi; cb += kSpChunk) {
+      const int m = min(kSpChunk, hi - cb);
+      for (int u = lane; u < m; u += 32) {
+        ws[u] = g.w[cb + u];
+        as[u] = a[g.ent[cb + u] >> 7];
+      }
+      __syncwarp();
+      const int e1 = min(o + n, cb + m);
+      for (int e = max(o, cb); e < e1; ++e) acc += ws[e - cb] * as[e - cb];
+      __syncwarp();
+    }
+    if (valid) g.F[p] = acc;
   }
 }
 
@@ -1580,17 +1628,25 @@ static int dot(Handle* h, const double* a, const double* b, const double* c, con
 static int build_jacobi(Handle* h, double dt);
 static bool jacobi_stale(Handle* h, double dt);
 
-// bicgstab(x, b), src/projection.f90:146-186, right-preconditioned with
-// per-marker 4x4 blocks when a preconditioner is selected.
-// Preconditioner modes: NONE (the reference's unpreconditioned solver),
-// JACOBI (diagonal blocks from lattice probing), SPAI (probed 4x4 block
-// sparse approximate inverse), LEARNED (4x4 blocks per marker from the
-// network, which also supplies a warm start x0 += M r0).  In
-// LEARNED mode the solve falls back to Jacobi, restarting from the current
-// iterate, when the residual stalls (the best residual of the last
-// kStallWindow iterations is not 1 % below the best before them) or breaks
-// down (non-finite scalars; restart from the entry guess).
+// bicgstab(x, b), src/projection.f90:146-186, right-preconditioned when a
+// preconditioner is selected.  Modes: NONE (the reference's unpreconditioned
+// solver), JACOBI (per-marker 4x4 diagonal blocks from lattice probing), SPAI
+// (probed 4x4 block sparse approximate inverse), BAND (the banded z-Fourier
+// inverse of the probed lattice band of S) and LEARNED (the same banded
+// inverse with the band predicted by the network, plus a warm start: the
+// extrapolated solution history, then x0 += M r0).  In LEARNED mode the
+// probed band takes over, restarting from the current iterate, when the
+// residual stalls (the best residual of the last kStallWindow iterations is
+// not 1 % below the best before them), when the solve is slow (twice the
+// iterations of the recent probed-band solves, and 20 more) or when it
+// breaks down (non-finite scalars; restart from the entry guess); after
+// kSlowLimit slow solves in a row the probed band serves LEARNED until the
+// network is trained again.  The iterations run as one CUDA graph launch
+// per solve (per kBcgChunk iterations in LEARNED mode, which checks between
+// launches).
 static const int kStallWindow = 20;
+static const int kBcgChunk = 10;       // LEARNED: iterations per graph launch between stall checks
+static const int kSlowLimit = 2;       // consecutive slow LEARNED solves before the probed band serves
 static int learned_warm_start(Handle* h, double* x);
 static int push_history(Handle* h, const double* x);
 
@@ -1609,14 +1665,129 @@ static int bcg_restart(Handle* h, const double* b, double* x, double dt, unsigne
   return 0;
 }
 
-int ib_bicgstab(Handle* h, const double* b, double dt) {
+// One BiCGSTAB iteration (src/projection.f90:160-184): the launches only,
+// no host synchronisation, so that it can be captured into a graph.
+static int bcg_iteration(Handle* h, double* x, double dt, const double* blk, bool band) {
   IbState* s = h->ib;
   const int nb = s->nb;
   const int64_t n = 4 * (int64_t)nb;
   const unsigned gb = 148 * 4;
   const unsigned gm = (unsigned)((nb + 255) / 256);
   int rc;
+  if ((rc = dot(h, s->rhat, s->r, nullptr, nullptr, 0))) return rc;           // rho_n, bta
+  k_bcg_p<<<gb, 256, 0, h->stream>>>(n, s->r, s->p, s->nu, s->ph, nullptr, s->sc);
+  C3D_LAUNCH_CHECK(h);
+  if (band) {
+    if ((rc = band_apply(h, s->p, s->ph))) return rc;
+  } else if (blk) {
+    k_apply_blocks<<<gm, 256, 0, h->stream>>>(nb, blk, s->p, s->ph);
+    C3D_LAUNCH_CHECK(h);
+  }
+  if ((rc = ib_schur(h, s->ph, s->nu, dt))) return rc;
+  if ((rc = dot(h, s->rhat, s->nu, nullptr, nullptr, 1))) return rc;          // alpha
+  k_bcg_s<<<gb, 256, 0, h->stream>>>(n, s->r, s->nu, s->s, s->sh, x, s->ph, nullptr, s->sc);
+  C3D_LAUNCH_CHECK(h);
+  if (band) {
+    if ((rc = band_apply(h, s->s, s->sh))) return rc;
+  } else if (blk) {
+    k_apply_blocks<<<gm, 256, 0, h->stream>>>(nb, blk, s->s, s->sh);
+    C3D_LAUNCH_CHECK(h);
+  }
+  if ((rc = ib_schur(h, s->sh, s->t, dt))) return rc;
+  if ((rc = dot(h, s->t, s->s, s->t, s->t, 2))) return rc;                    // om
+  k_bcg_x<<<kIbRedBlocks, 256, 0, h->stream>>>(n, x, s->r, s->s, s->sh, s->t, s->sc, s->red);
+  C3D_LAUNCH_CHECK(h);
+  k_dot_final<<<1, 256, 0, h->stream>>>(s->red, kIbRedBlocks, s->sc, 0, 3);   // err
+  C3D_LAUNCH_CHECK(h);
+  return 0;
+}
+
+// End of a captured iteration: count it, record its squared residual and
+// keep the WHILE node looping while the residual is finite and at or above
+// the tolerance and the launch's iteration limit is not reached.
+__global__ void k_bcg_loop(cudaGraphConditionalHandle cond, const double* __restrict__ sc, int* __restrict__ loop,
+                           double* __restrict__ hist, double eps) {
+  const double err = sc[5];
+  const int it = loop[0] + 1;
+  loop[0] = it;
+  hist[it - 1] = err;
+  const bool go = isfinite(err) && err >= eps && it < loop[1];
+  cudaGraphSetConditional(cond, go ? 1u : 0u);
+}
+
+// The iteration loop as one executable graph: a conditional WHILE node
+// whose body (one iteration and k_bcg_loop) runs until k_bcg_loop stops it,
+// so a solve costs one graph launch and one host synchronisation instead of
+// one per iteration.  What the body bakes in (mode, factors, operand
+// pointers, dt, tolerance, the band of stencil rows) is the graph's key;
+// the graph is re-captured when it changes.  Sets bcg_graph_off, and
+// leaves the loop to the host, when conditional nodes are unavailable.
+static int bcg_graph_ready(Handle* h, double* x, double dt, const double* blk, bool band, int mode, double eps) {
+  IbState* s = h->ib;
+  const bool block = band && s->band ? band_is_block(h) : false;
+  const std::vector<double> key = {(double)mode, (double)block, (double)(uintptr_t)blk, (double)(uintptr_t)x,
+                                   dt, eps, (double)s->iy_lo, (double)s->iy_hi, (double)h->p.cg_max_iter,
+                                   (double)s->nb};
+  if (s->bcg_exec && key == s->bcg_key) return 0;
+  if (s->bcg_exec) { cudaGraphExecDestroy(s->bcg_exec); s->bcg_exec = nullptr; }
+  if (s->bcg_graph) { cudaGraphDestroy(s->bcg_graph); s->bcg_graph = nullptr; }
+  cudaGraph_t g = nullptr;
+  C3D_CUDA_TRY(h, cudaGraphCreate(&g, 0));
+  s->bcg_graph = g;
+  cudaGraphConditionalHandle cond;
+  cudaGraphNodeParams np{};
+  cudaGraphNode_t node;
+  if (cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault) != cudaSuccess ||
+      (np.type = cudaGraphNodeTypeConditional, np.conditional.handle = cond,
+       np.conditional.type = cudaGraphCondTypeWhile, np.conditional.size = 1,
+       cudaGraphAddNode(&node, g, nullptr, 0, &np) != cudaSuccess)) {
+    cudaGetLastError();
+    s->bcg_graph_off = true;
+    return 0;
+  }
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  const bool pdl = h->use_pdl;
+  h->use_pdl = false;                 // plain kernel nodes in the body
+  const int64_t l0 = h->launches;
+  C3D_CUDA_TRY(h, cudaStreamBeginCaptureToGraph(h->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  int rc = bcg_iteration(h, x, dt, blk, band);
+  if (rc == 0) {
+    k_bcg_loop<<<1, 1, 0, h->stream>>>(cond, s->sc, s->loop_d, s->hist_d, eps);
+    if (cudaGetLastError() != cudaSuccess) rc = C3D_ERR_CUDA;
+    else h->launches++;
+  }
+  cudaGraph_t captured = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(h->stream, &captured);
+  h->use_pdl = pdl;
+  s->bcg_body_launches = h->launches - l0;
+  h->launches = l0;
+  if (rc) return rc;
+  if (ec != cudaSuccess) { h->last_error = std::string("BiCGSTAB graph capture: ") + cudaGetErrorString(ec); return C3D_ERR_CUDA; }
+  cudaGraphExec_t ex = nullptr;
+  C3D_CUDA_TRY(h, cudaGraphInstantiate(&ex, g, 0));
+  s->bcg_exec = ex;
+  s->bcg_key = key;
+  return 0;
+}
+
+void ib_rows(const Handle* h, int32_t rows[2]) {
+  rows[0] = h->ib ? h->ib->iy_lo : 0;
+  rows[1] = h->ib ? h->ib->iy_hi : 0;
+}
+
+int ib_bicgstab(Handle* h, const double* b, double dt) {
+  IbState* s = h->ib;
+  const int64_t n = 4 * (int64_t)s->nb;
+  const unsigned gb = 148 * 4;
+  int rc;
   int mode = h->precond_mode;
+  if (mode == C3D_PRECOND_LEARNED && s->lrn_slow >= kSlowLimit) {
+    // the network's band was slow on consecutive solves: the probed band
+    // serves until the network is trained again
+    h->stats.precond_fallbacks++;
+    mode = C3D_PRECOND_BAND;
+  }
+  const bool pure_band = mode == C3D_PRECOND_BAND;
   if (!s->ev_a) {
     C3D_CUDA_TRY(h, cudaEventCreate(&s->ev_a));
     C3D_CUDA_TRY(h, cudaEventCreate(&s->ev_b));
@@ -1666,36 +1837,39 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
   double err = 1.0;
   int it = 0;
   std::vector<double> hist;
-  while (it < h->p.cg_max_iter && err >= eps) {
-    if ((rc = dot(h, s->rhat, s->r, nullptr, nullptr, 0))) return rc;           // rho_n, bta
-    k_bcg_p<<<gb, 256, 0, h->stream>>>(n, s->r, s->p, s->nu, s->ph, nullptr, s->sc);
-    C3D_LAUNCH_CHECK(h);
-    if (band) {
-      if ((rc = band_apply(h, s->p, s->ph))) return rc;
-    } else if (blk) {
-      k_apply_blocks<<<gm, 256, 0, h->stream>>>(nb, blk, s->p, s->ph);
-      C3D_LAUNCH_CHECK(h);
+  const int maxit = h->p.cg_max_iter;
+  if (s->hist_cap < maxit) {
+    if ((rc = dev_alloc(h, &s->hist_d, maxit))) return rc;
+    s->hist_cap = maxit;
+  }
+  if (!s->loop_d && (rc = dev_alloc(h, &s->loop_d, 2))) return rc;
+  while (it < maxit && err >= eps) {
+    // LEARNED checks for stalls every kBcgChunk iterations; the other modes
+    // run the whole solve in one launch
+    const int lim = mode == C3D_PRECOND_LEARNED ? std::min(maxit, it + kBcgChunk) : maxit;
+    int done = it;
+    if (!s->bcg_graph_off && (rc = bcg_graph_ready(h, x, dt, blk, band, mode, eps)) == 0 && !s->bcg_graph_off) {
+      const int lc[2] = {it, lim};
+      C3D_CUDA_TRY(h, cudaMemcpyAsync(s->loop_d, lc, sizeof(lc), cudaMemcpyHostToDevice, h->stream));
+      C3D_CUDA_TRY(h, cudaGraphLaunch(s->bcg_exec, h->stream));
+      C3D_CUDA_TRY(h, cudaMemcpyAsync(&done, s->loop_d, 4, cudaMemcpyDeviceToHost, h->stream));
+      C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+      if (done <= it || done > lim) { h->last_error = "BiCGSTAB graph: bad iteration count"; return C3D_ERR_CUDA; }
+      h->launches += s->bcg_body_launches * (done - it);
+    } else {
+      if (rc) return rc;
+      // host-driven iteration (conditional graphs unavailable)
+      if ((rc = bcg_iteration(h, x, dt, blk, band))) return rc;
+      done = it + 1;
+      C3D_CUDA_TRY(h, cudaMemcpyAsync(s->hist_d + it, s->sc + 5, 8, cudaMemcpyDeviceToDevice, h->stream));
     }
-    if ((rc = ib_schur(h, s->ph, s->nu, dt))) return rc;
-    if ((rc = dot(h, s->rhat, s->nu, nullptr, nullptr, 1))) return rc;          // alpha
-    k_bcg_s<<<gb, 256, 0, h->stream>>>(n, s->r, s->nu, s->s, s->sh, x, s->ph, nullptr, s->sc);
-    C3D_LAUNCH_CHECK(h);
-    if (band) {
-      if ((rc = band_apply(h, s->s, s->sh))) return rc;
-    } else if (blk) {
-      k_apply_blocks<<<gm, 256, 0, h->stream>>>(nb, blk, s->s, s->sh);
-      C3D_LAUNCH_CHECK(h);
-    }
-    if ((rc = ib_schur(h, s->sh, s->t, dt))) return rc;
-    if ((rc = dot(h, s->t, s->s, s->t, s->t, 2))) return rc;                    // om
-    k_bcg_x<<<kIbRedBlocks, 256, 0, h->stream>>>(n, x, s->r, s->s, s->sh, s->t, s->sc, s->red);
-    C3D_LAUNCH_CHECK(h);
-    k_dot_final<<<1, 256, 0, h->stream>>>(s->red, kIbRedBlocks, s->sc, 0, 3);   // err
-    C3D_LAUNCH_CHECK(h);
-    C3D_CUDA_TRY(h, cudaMemcpyAsync(&err, s->sc + 5, 8, cudaMemcpyDeviceToHost, h->stream));
+    const size_t h0 = hist.size();
+    hist.resize(h0 + (done - it));
+    C3D_CUDA_TRY(h, cudaMemcpyAsync(hist.data() + h0, s->hist_d + it, 8 * (size_t)(done - it),
+                                    cudaMemcpyDeviceToHost, h->stream));
     C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-    ++it;
-    hist.push_back(err);
+    it = done;
+    err = hist.back();
     if (mode == C3D_PRECOND_LEARNED) {
       const bool broke = !(err == err) || std::isinf(err);
       // stall: the best residual of the last kStallWindow iterations is not
@@ -1707,7 +1881,12 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
         const double recent = *std::min_element(hist.begin() + cut, hist.end());
         stalled = recent > 0.98 * before;   // squared norms: |r| down < 1 %
       }
-      if (broke || stalled) {
+      // slow: the probed band's recent solves needed fewer than half as many
+      // iterations (and 20 fewer): the predicted band fits this geometry badly
+      const double ref = s->band_iters_ref;
+      const bool slow = ref > 0.0 && it >= std::max(2.0 * ref, ref + 20.0);
+      if (slow) s->lrn_slow++;
+      if (broke || stalled || slow) {
         // the probed band of the current geometry takes over
         h->stats.precond_fallbacks++;
         mode = C3D_PRECOND_BAND;
@@ -1722,6 +1901,9 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
     }
   }
   if (err == err && (rc = push_history(h, x))) return rc;
+  if (pure_band && err < eps)
+    s->band_iters_ref = s->band_iters_ref > 0.0 ? 0.5 * (s->band_iters_ref + it) : (double)it;
+  if (h->precond_mode == C3D_PRECOND_LEARNED && mode == C3D_PRECOND_LEARNED && err < eps) s->lrn_slow = 0;
   C3D_CUDA_TRY(h, cudaEventRecord(s->ev_b, h->stream));
   C3D_CUDA_TRY(h, cudaEventSynchronize(s->ev_b));
   float ms = 0.f;

@@ -1034,6 +1034,13 @@ int band_apply(Handle* h, const double* in, double* out) {
   return 0;
 }
 
+// whether the factors in use are the block-tridiagonal ones (else the
+// pivoted banded LU)
+bool band_is_block(Handle* h) {
+  const BandState* B = h->ib ? h->ib->band : nullptr;
+  return B != nullptr && B->block;
+}
+
 // Access for the learned preconditioner (k_mlp.cu): the lattice, the
 // neighbour table and the band symbol That, which the network fills before
 // band_factor_symbol factors it.

@@ -988,7 +988,7 @@ extern "C" int c3d_precond_train(int id, int epochs, double lr, double* final_lo
   if ((rc = mlp_train_pass(h, S->feats, S->mom, M, sd, &loss, &norm))) return rc;
   S->last_loss = loss / std::max(norm, 1e-300);
   S->trained = true;
-  if (h->ib) h->ib->have_lrn = false;
+  if (h->ib) { h->ib->have_lrn = false; h->ib->lrn_slow = 0; }
   if (final_loss) *final_loss = S->last_loss;
   return 0;
 }
@@ -1031,7 +1031,7 @@ extern "C" int c3d_precond_set_params(int id, const float* params, int n, const 
     for (int i = 0; i < 4; ++i) { h->mlp->sig_r[i] = sig[i]; h->mlp->sig_e[i] = sig[4 + i]; }
   if ((rc = upload_sig(h))) return rc;
   h->mlp->trained = true;
-  if (h->ib) h->ib->have_lrn = false;
+  if (h->ib) { h->ib->have_lrn = false; h->ib->lrn_slow = 0; }
   C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return 0;
 }

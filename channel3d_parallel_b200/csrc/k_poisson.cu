@@ -300,12 +300,14 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_fwd(XfwdArgs<T> a) {
     }
   }
   __syncthreads();
-  if (a.linesum && tid < 2 * kLinesX) {   // FP64 line sum in a fixed order
-    const int64_t r = r0 + tid;
-    if (r < nreal) {
+  if (a.linesum) {   // FP64 line sums: one full warp per line, a fixed shuffle tree
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int rl = warp; rl < 2 * kLinesX && (warp + 1) * 32 <= nt; rl += nt >> 5) {
       double sum = 0.0;
-      for (int q = 0; q < N; ++q) sum += sm.sval[tid * N + q];
-      a.linesum[r] = sum;
+      for (int q = lane; q < N; q += 32) sum += sm.sval[rl * N + q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      if (lane == 0 && r0 + rl < nreal) a.linesum[r0 + rl] = sum;
     }
   }
   fft_rows_dif<T, kXMaxR>(sm.buf, kLinesX, RS, sm.tw, a.P);
@@ -683,26 +685,186 @@ __global__ void __launch_bounds__(yz_threads<NARROW>(), yz_min_blocks<NARROW>())
 }
 
 // ---------------------------------------------------------------------------
+// Band-restricted z transform and y solve (FP64), for the Poisson solve of
+// the Schur complement: the right-hand side is zero outside the rows
+// [rlo, rhi] and only those rows of the solution are read.  Thomas on the
+// band alone: the forward sweep starts at rlo from zero, and the back
+// substitution starts from x(rhi+1) = S(rhi+1) y(rhi+1), y(rhi+1) =
+// -MULT(rhi) y(rhi), where S(j) = x(j)/y(j) of the homogeneous tail is
+// tabulated once (build_tail_table).  One CTA per kx slab, the band rows in
+// shared memory; the same z transform as k_spectral_yz.
+// ---------------------------------------------------------------------------
+struct BandYzArgs {
+  Dims d;
+  double2* __restrict__ spec;
+  const double2* __restrict__ tw;
+  const double* __restrict__ rdp;
+  const double* __restrict__ tail;
+  const double* __restrict__ dl;
+  const double* __restrict__ du;
+  FftPasses P;
+  int rs, pz;
+  int rlo, rhi;
+};
+
+__global__ void __launch_bounds__(256) k_spectral_band(BandYzArgs a) {
+  extern __shared__ __align__(16) unsigned char sb_smem[];
+  const int m = blockIdx.x;
+  const int Ny = a.d.Ny, Nz = a.d.Nz, nkzs = a.d.nkzs, RS = a.rs;
+  const int nr = a.rhi - a.rlo + 1;
+  double2* data = reinterpret_cast<double2*>(sb_smem);   // [nr][RS]
+  double2* tw = data + (size_t)nr * RS;                   // [Nz]
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double2* g = a.spec + ((int64_t)m * Ny + a.rlo) * a.pz;
+  for (int t = tid; t < Nz; t += nt) tw[t] = a.tw[t];
+  pdl_wait();
+  pdl_trigger();
+  for (int t = tid; t < nr * Nz; t += nt) {
+    const int r = t / Nz, c = t - r * Nz;
+    data[r * RS + c] = g[(int64_t)r * a.pz + c];
+  }
+  __syncthreads();
+  fft_rows_dif<double, kYzMaxRWide>(data, nr, RS, tw, a.P);
+  const double* rdp_m = a.rdp + (int64_t)m * Ny * nkzs;
+  const double* tail_m = a.tail + (int64_t)m * Ny * nkzs;
+  for (int col = tid; col < Nz; col += nt) {
+    const int kz = dif_position_to_k(col, a.P);
+    const int kzs = kz <= Nz - kz ? kz : Nz - kz;
+    // forward: y(j) = b(j) - DL(j-1)/D'(j-1) y(j-1), y(rlo-1) = 0
+    double2 prev = make_double2(0.0, 0.0);
+    for (int r = 0; r < nr; ++r) {
+      const int j = a.rlo + r;
+      double2 b = data[r * RS + col];
+      if (r > 0) {
+        const double mu = a.dl[j - 1] * rdp_m[(int64_t)(j - 1) * nkzs + kzs];
+        b.x -= mu * prev.x;
+        b.y -= mu * prev.y;
+      }
+      data[r * RS + col] = b;
+      prev = b;
+    }
+    // the rows above the band, through the tail ratio
+    double2 xn = make_double2(0.0, 0.0);
+    if (a.rhi + 1 < Ny) {
+      const double mu = a.dl[a.rhi] * rdp_m[(int64_t)a.rhi * nkzs + kzs];
+      const double sx = -mu * tail_m[(int64_t)(a.rhi + 1) * nkzs + kzs];
+      xn.x = sx * prev.x;
+      xn.y = sx * prev.y;
+    }
+    // back substitution x(j) = (y(j) - DU(j) x(j+1)) / D'(j)
+    for (int r = nr - 1; r >= 0; --r) {
+      const int j = a.rlo + r;
+      const double rp = rdp_m[(int64_t)j * nkzs + kzs];
+      const double u = a.du[j];
+      double2 b = data[r * RS + col];
+      b.x = (b.x - u * xn.x) * rp;
+      b.y = (b.y - u * xn.y) * rp;
+      data[r * RS + col] = b;
+      xn = b;
+    }
+  }
+  __syncthreads();
+  fft_rows_dit_inv<double, kYzMaxRWide>(data, nr, RS, tw, a.P);
+  for (int t = tid; t < nr * Nz; t += nt) {
+    const int r = t / Nz, c = t - r * Nz;
+    g[(int64_t)r * a.pz + c] = data[r * RS + c];
+  }
+}
+
+// S(j) = x(j)/y(j) when the right-hand side vanishes from row j on:
+// S(Ny-1) = 1/D'(Ny-1), S(j) = (1 + DU(j) MULT(j) S(j+1)) / D'(j), with
+// MULT(j) = DL(j)/D'(j) formed as the solves form it
+static int build_tail_table(Handle* h) {
+  const Dims& d = h->d;
+  SpectralState& S = h->sp;
+  const int Ny = d.Ny, nkx = d.nkx, nkzs = d.nkzs;
+  const int64_t nt = (int64_t)Ny * nkzs * nkx;
+  std::vector<double> rdp(nt), tail(nt), dl(Ny), du(Ny);
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(rdp.data(), S.rdp, 8 * nt, cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(dl.data(), S.dl, 8 * Ny, cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(du.data(), S.du, 8 * Ny, cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  for (int m = 0; m < nkx; ++m)
+    for (int kzs = 0; kzs < nkzs; ++kzs) {
+      auto o = [&](int j) { return ((int64_t)m * Ny + j) * nkzs + kzs; };
+      double sj = rdp[o(Ny - 1)];
+      tail[o(Ny - 1)] = sj;
+      for (int j = Ny - 2; j >= 0; --j) {
+        const double mu = dl[j] * rdp[o(j)];
+        sj = (1.0 + du[j] * mu * sj) * rdp[o(j)];
+        tail[o(j)] = sj;
+      }
+    }
+  int rc;
+  if ((rc = dev_alloc(h, &S.tail, nt))) return rc;
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(S.tail, tail.data(), 8 * nt, cudaMemcpyHostToDevice, h->stream));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+static size_t band_yz_smem(const Dims& d, int rs, int nr) {
+  return sizeof(double2) * ((size_t)nr * rs + d.Nz);
+}
+static const size_t kBandYzSmemMax = 200 * 1024;
+
+// the band solve of rows [blo, bhi] when it fits in shared memory; false
+// (nothing launched) otherwise
+static int launch_band_yz(Handle* h, int blo, int bhi, bool* done) {
+  const Dims& d = h->d;
+  SpectralState& S = h->sp;
+  *done = false;
+  const int nr = bhi - blo + 1;
+  const size_t smem = band_yz_smem(d, S.rs64, nr);
+  if (nr <= 0 || smem > kBandYzSmemMax) return 0;
+  int rc;
+  if (!S.tail) {   // first use (outside any graph capture: the table build synchronises)
+    if ((rc = build_tail_table(h))) return rc;
+    C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_spectral_band, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kBandYzSmemMax));
+  }
+  BandYzArgs a{};
+  a.d = d; a.spec = S.spec; a.tw = S.twz; a.rdp = S.rdp; a.tail = S.tail; a.dl = S.dl; a.du = S.du;
+  a.P = get_passes(d.Nz, kYzMaxRWide); a.rs = S.rs64; a.pz = S.pz64; a.rlo = blo; a.rhi = bhi;
+  C3D_CUDA_TRY(h, launch_pdl(h->use_pdl, k_spectral_band, dim3((unsigned)d.nkx), dim3(256), smem, h->stream, a));
+  C3D_LAUNCH_CHECK(h);
+  *done = true;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
 // FP64 kx = kz = 0 mode of the mixed path: plane sums and the pinned solve
 // ---------------------------------------------------------------------------
-__global__ void k_mode00(Dims d, const double* __restrict__ linesum, const double* __restrict__ mult,
-                         const double* __restrict__ rdp, const double* __restrict__ du,
-                         double* __restrict__ phi00) {
-  extern __shared__ double b00[];
+__global__ void __launch_bounds__(1024) k_mode00(Dims d, const double* __restrict__ linesum,
+                                                 const double* __restrict__ mult, const double* __restrict__ rdp,
+                                                 const double* __restrict__ du, double* __restrict__ phi00) {
+  extern __shared__ double m00[];
   const int Ny = d.Ny, Nz = d.Nz, nkzs = d.nkzs;
-  for (int j = threadIdx.x; j < Ny; j += blockDim.x) {
+  double* b00 = m00;                 // plane sums, then the solution
+  double* sm_ = m00 + Ny;            // the (0, 0) rows of the factor tables
+  double* sr = m00 + 2 * Ny;
+  double* su = m00 + 3 * Ny;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  // plane sums: one warp per row j, a fixed shuffle tree over its z lines
+  for (int j = warp; j < Ny; j += nw) {
     double s = 0.0;
-    for (int k = 0; k < Nz; ++k) s += linesum[(int64_t)j * Nz + k];   // fixed order
-    b00[j] = s;
+    for (int k = lane; k < Nz; k += 32) s += linesum[(int64_t)j * Nz + k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) b00[j] = s;
+  }
+  for (int j = threadIdx.x; j < Ny; j += blockDim.x) {
+    sm_[j] = j > 0 ? mult[(int64_t)(j - 1) * nkzs] : 0.0;
+    sr[j] = rdp[(int64_t)j * nkzs];
+    su[j] = du[j];
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    // mode (0, 0): table entries (m = 0, kz' = 0)
-    for (int j = 1; j < Ny; ++j) b00[j] = b00[j] - mult[(int64_t)(j - 1) * nkzs] * b00[j - 1];
-    double xn = b00[Ny - 1] * rdp[(int64_t)(Ny - 1) * nkzs];
+    // mode (0, 0): table entries (m = 0, kz' = 0), elimination in shared memory
+    for (int j = 1; j < Ny; ++j) b00[j] = b00[j] - sm_[j] * b00[j - 1];
+    double xn = b00[Ny - 1] * sr[Ny - 1];
     b00[Ny - 1] = xn;
     for (int j = Ny - 2; j >= 0; --j) {
-      xn = (b00[j] - du[j] * xn) * rdp[(int64_t)j * nkzs];
+      xn = (b00[j] - su[j] * xn) * sr[j];
       b00[j] = xn;
     }
   }
@@ -739,6 +901,7 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
   // per real line: offset of the x = 2 value of phi(j,k), and of phi(j,nzp+2)
   // for the plane k = 2 that the reference duplicates (else -1)
   __shared__ int64_t s_bo[2 * kLinesX], s_bo2[2 * kLinesX];
+  __shared__ double s_p00[2 * kLinesX];   // FP64 mean mode of each line's row (mixed path)
   const Dims& d = a.d;
   const int N = d.Nx, nk = d.nkx, RS = a.rs;
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -765,6 +928,7 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
   }
   pdl_wait();
   pdl_trigger();
+  if (a.phi00 && tid < 2 * kLinesX) s_p00[tid] = s_j[tid] >= 2 ? a.phi00[s_j[tid] - 2] : 0.0;
   __syncthreads();
   // Z = A + iB on the full circle from the two half spectra, placed at the
   // digit-reversed positions the inverse transform expects
@@ -815,7 +979,7 @@ __global__ void __launch_bounds__(kMaxNx) k_xfft_inv(XinvArgs<T> a) {
     if (bo < 0) continue;
     const C z = sm.buf[(rl >> 1) * RS + ii];
     double v = (double)((rl & 1) ? z.y : z.x) * rsd;
-    if (a.phi00) v += a.phi00[s_j[rl] - 2];
+    if (a.phi00) v += s_p00[rl];
     const int64_t o = bo + ii;
     if (a.accumulate) v += a.rhs[o];
     a.rhs[o] = v;
@@ -1057,13 +1221,20 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     }
     C3D_LAUNCH_CHECK(h);
     if (f32) {
-      k_mode00<<<1, 256, sizeof(double) * d.Ny, s>>>(d, S.linesum, S.mult, S.rdp, S.du, S.phi00);
+      k_mode00<<<1, 1024, 4 * sizeof(double) * d.Ny, s>>>(d, S.linesum, S.mult, S.rdp, S.du, S.phi00);
       C3D_LAUNCH_CHECK(h);
     }
   }
   if (parts & 2) {
-    int rc = launch_yz<T>(h, spec, twz, rdp, dl, du, cs, jc, rs, pz, nt, smem, narrow, f32 ? 1 : 0, blo, bhi);
-    if (rc) return rc;
+    bool band_done = false;
+    if (!f32 && (blo > 0 || bhi < d.Ny - 1)) {   // a band of rows: the band-restricted solve
+      int rc = launch_band_yz(h, blo, bhi, &band_done);
+      if (rc) return rc;
+    }
+    if (!band_done) {
+      int rc = launch_yz<T>(h, spec, twz, rdp, dl, du, cs, jc, rs, pz, nt, smem, narrow, f32 ? 1 : 0, blo, bhi);
+      if (rc) return rc;
+    }
   }
   if (parts & 4) {
     XinvArgs<T> a{};

@@ -201,6 +201,7 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
   double (*sU)[PN] = reinterpret_cast<double (*)[PN]>(rhs_smem);
   double (*sV)[PN] = reinterpret_cast<double (*)[PN]>(rhs_smem + NSLOT * PN);
   double (*sW)[PN] = reinterpret_cast<double (*)[PN]>(rhs_smem + 2 * NSLOT * PN);
+  double* sZ = rhs_smem + 3 * NSLOT * PN;     // z factors of planes k0..k1: [6][KC]
   const Dims& d = a.d;
   const Metric& m = a.m;
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -231,6 +232,11 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
     offW[q] = okW[q] ? idxW(d, gi, gj, 1) : 0;
   }
   const int64_t plU = (int64_t)d.nx * d.nyg, plV = (int64_t)d.nxg * d.ny, plW = (int64_t)d.nxg * d.nyg;
+  for (int t = tid; t < 6 * KC; t += TX * TY) {
+    const int q = t / KC, kk = k0 + (t - q * KC);
+    const double* f = q == 0 ? m.rdz : q == 1 ? m.rdzg : q == 2 ? m.czpC : q == 3 ? m.czmC : q == 4 ? m.czpF : m.czmF;
+    sZ[t] = kk <= k1 ? f[kk] : 0.0;
+  }
   pdl_wait();
   pdl_trigger();
   // asynchronous copy of plane k (tile + halo) of U, V, W into a slot
@@ -264,23 +270,33 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
   const double rdy_j = m.rdy[jc], rdyg_j = m.rdyg[jc];
   const double cypC_j = m.cypC[jc], cymC_j = m.cymC[jc], cypF_j = m.cypF[jc], cymF_j = m.cymF[jc];
   const int64_t iu0 = idxU(d, ic, jc, 1), iv0 = idxV(d, ic, jc, 1), iw0 = idxW(d, ic, jc, 1);
+  // accumulators, loaded one plane ahead of their use
+  double gu = 0.0, gv = 0.0, gw = 0.0;
+  if (MODE == 2 && active) {
+    const int64_t kk = k0 - 1;
+    gu = __ldg(a.Gu + iu0 + kk * plU);
+    gw = __ldg(a.Gw + iw0 + kk * plW);
+    if (hasv) gv = __ldg(a.Gv + iv0 + kk * plV);
+  }
   for (int k = k0; k <= k1; ++k) {
     if (k + 1 + AHEAD <= k1 + 1) issue_plane(k + 1 + AHEAD);
     else cp_async_commit();                   // keep the group count uniform
     cp_async_wait<AHEAD>();                   // planes up to k+1 have landed
     __syncthreads();
     const int sm = (k - 1) & (NSLOT - 1), s0 = k & (NSLOT - 1), sp = (k + 1) & (NSLOT - 1);
-    const double rdz_k = m.rdz[k], rdzg_k = m.rdzg[k];
-    const double czpC_k = m.czpC[k], czmC_k = m.czmC[k], czpF_k = m.czpF[k], czmF_k = m.czmF[k];
+    const int kz = k - k0;
+    const double rdz_k = sZ[kz], rdzg_k = sZ[KC + kz];
+    const double czpC_k = sZ[2 * KC + kz], czmC_k = sZ[3 * KC + kz];
+    const double czpF_k = sZ[4 * KC + kz], czmF_k = sZ[5 * KC + kz];
     if (active) {
       const int64_t kk = k - 1;
       const int64_t iu = iu0 + kk * plU, iw = iw0 + kk * plW;
       const int64_t iv = iv0 + kk * plV;
-      double gu = 0.0, gv = 0.0, gw = 0.0;
-      if (MODE == 2) {                        // issue the accumulator loads early
-        gu = __ldg(a.Gu + iu);
-        gw = __ldg(a.Gw + iw);
-        if (hasv) gv = __ldg(a.Gv + iv);
+      double gu_n = 0.0, gv_n = 0.0, gw_n = 0.0;
+      if (MODE == 2 && k < k1) {              // the next plane's accumulators
+        gu_n = __ldg(a.Gu + iu + plU);
+        gw_n = __ldg(a.Gw + iw + plW);
+        if (hasv) gv_n = __ldg(a.Gv + iv + plV);
       }
 #define AU(s, di, dj) sU[s][c + (di) + (dj) * PX]
 #define AV(s, di, dj) sV[s][c + (di) + (dj) * PX]
@@ -351,6 +367,7 @@ __global__ void __launch_bounds__(TX * TY, 2) k_rhs_tiled(RhsArgs a) {
         a.Us[iu] = gu + a.cs * Fu;
         a.Ws[iw] = gw + a.cs * Fw;
         if (hasv) a.Vs[iv] = gv + a.cs * Fv;
+        gu = gu_n; gv = gv_n; gw = gw_n;
       }
     }
     // No barrier here: the slot the next iteration refills, (k+5) mod 8, held
@@ -377,7 +394,7 @@ static dim3 rhs_grid(const Dims& d) {
   return dim3((d.Nx + b.x - 1) / b.x, (d.Ny + b.y - 1) / b.y, (d.Nz + b.z - 1) / b.z);
 }
 
-static const int kRhsSmem = 3 * NSLOT * PN * (int)sizeof(double);
+static const int kRhsSmem = (3 * NSLOT * PN + 6 * KC) * (int)sizeof(double);
 
 int rhs_setup(Handle* h) {
   C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_rhs_tiled<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRhsSmem));

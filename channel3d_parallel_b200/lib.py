@@ -44,7 +44,8 @@ class Stats(C.Structure):
                 ("last_bicgstab_ms", C.c_double), ("bicgstab_ms", C.c_double),
                 ("slab_cluster", C.c_int32 * 2), ("slab_narrow", C.c_int32 * 2),
                 ("qflow_y_0", C.c_double), ("qflow_z_0", C.c_double),
-                ("precond_builds", C.c_int64), ("precond_build_ms", C.c_double)]
+                ("precond_builds", C.c_int64), ("precond_build_ms", C.c_double),
+                ("ib_rows", C.c_int32 * 2)]
 
 
 _D = C.POINTER(C.c_double)

@@ -97,7 +97,7 @@ typedef struct c3d_stats {
   int64_t bicgstab_iters;      /* accumulated BiCGSTAB iterations (cg_accum_iter) */
   int32_t last_bicgstab_iters; /* iterations of the last Schur solve          */
   int32_t refinement_sweeps;   /* mixed-precision refinement sweeps, last solve */
-  int64_t precond_fallbacks;   /* learned-preconditioner stalls -> Jacobi     */
+  int64_t precond_fallbacks;   /* learned-preconditioner hand-overs to the probed band */
   double  last_residual;       /* ||r||_2 at exit of the last Schur solve     */
   double  dPdx, dPdy, dPdz;    /* current mean pressure gradients             */
   double  t, dt;               /* simulation time and last dt                 */
@@ -111,6 +111,7 @@ typedef struct c3d_stats {
   double  qflow_y_0, qflow_z_0;/* targets of the y and z constant-flux corrections */
   int64_t precond_builds;      /* probed (or predicted) band preconditioners built */
   double  precond_build_ms;    /* accumulated device time of those builds (ms) */
+  int32_t ib_rows[2];          /* y rows (Fortran j) the markers' stencils reach; 0 0 without IB */
 } c3d_stats;
 
 /* ---- lifecycle ------------------------------------------------------------
