@@ -367,6 +367,31 @@ def measure_ib(maxit=300, steps=2, modes=("none", "jacobi", "band", "learned"), 
     return out
 
 
+def profile_schur(cfg, apps):
+    """N applications of the Schur operator S (src/projection.f90:98-144)
+    and of the probed band preconditioner, as plain stream launches (no time
+    step, no BiCGSTAB): the kernels of one BiCGSTAB iteration's operators in
+    isolation, for launch lists and captures.  Host vectors in and out."""
+    import numpy as np
+    import channel3d_parallel_b200 as c3d
+    ch = make_ib_channel(600, cfg)
+    try:
+        ch.setup_IB_operators()
+        ch.set_mode(precond=c3d.lib.PRECOND_BAND)
+        ch.precond_probe()
+        f = np.random.default_rng(0).standard_normal(4 * ch.dims["nb"])
+        ch.schur(f)
+        t0 = time.perf_counter()
+        for _ in range(apps):
+            ch.schur(f)
+            ch.precond_apply(f)
+        wall = (time.perf_counter() - t0) / apps * 1e3
+        return {"cfg": cfg, "schur_apps": apps, "wall_ms_per_schur_and_band_apply": wall,
+                "ib_rows": list(ch.stats()["ib_rows"])}
+    finally:
+        ch.close()
+
+
 def learned_run(ch, run, steps):
     """Learned preconditioner: trained on probe pairs at three geometries
     (RK stages of band-preconditioned steps), then used."""
@@ -597,9 +622,15 @@ def main():
     ap.add_argument("--ib-modes", default="none,jacobi,band,learned")
     ap.add_argument("--device-only", action="store_true",
                     help="only the device-timed step loop (used for profiler captures)")
+    ap.add_argument("--schur-apps", type=int, default=0,
+                    help="only N Schur-operator and band-preconditioner applications at the first of "
+                         "--ib-cfgs, outside any time step (a profiler target)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.schur_apps > 0:
+        print(json.dumps(profile_schur(args.ib_cfgs.split(",")[0], args.schur_apps)), flush=True)
+        return
     if args.only_ib:
         print(json.dumps(measure_ib(maxit=args.ib_maxit, steps=args.steps,
                                     modes=tuple(args.ib_modes.split(",")),
