@@ -494,7 +494,7 @@ struct GField {
   double mul;         // value multiplier
 };
 
-enum GatherMode { G_E = 0, G_E1N = 1, G_GRAD = 2 };
+enum GatherMode { G_E = 0, G_E1N = 1 };
 
 struct GatherArgs {
   OpTables T;
@@ -504,9 +504,6 @@ struct GatherArgs {
   int type[3];        // table type per component
   int ncomp;
   int mode;
-  const double* phi;  // G_GRAD: potential (rhs_p extents)
-  double phimul;
-  const double* reg[3];   // G_GRAD: subtract these fields (U_reg...)
   double* out;        // out[c*nb + l]
   const double* sub;  // optional: out = gathered - sub_mul*sub[c*nb+l]*subv[c*nb+l]
   const double* subv;
@@ -519,82 +516,12 @@ __device__ __forceinline__ int64_t lin(int n1, int n2, int i, int j, int k, int 
   return (int64_t)(i - 1) + (int64_t)n1 * ((j - 1) + (int64_t)n2 * (k - 1));
 }
 
-// one thread per (marker, component): the 15 one-dimensional weights and
-// indices of its stencil load coalesced (consecutive markers, consecutive
-// addresses), then the 5x5x5 tensor product is walked in registers
-__global__ void __launch_bounds__(128) k_ib_gather(GatherArgs a) {
-  const int nb = a.T.nb;
-  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= nb * a.ncomp) return;
-  const int c = gid / nb;
-  const int l = gid - c * nb;
-  const int t = a.type[c];
-  const OpTables& T = a.T;
-  int ix[5], iy[5], iz[5];
-  double wx[5], wy[5], wz[5], ox[5], oy[5], oz[5];
-#pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    ix[q] = T.idx[tslot(nb, t, 0, q, l)];
-    iy[q] = T.idx[tslot(nb, t, 1, q, l)];
-    iz[q] = T.idx[tslot(nb, t, 2, q, l)];
-    wx[q] = T.w1[tslot(nb, t, 0, q, l)];
-    wy[q] = T.w1[tslot(nb, t, 1, q, l)];
-    wz[q] = T.w1[tslot(nb, t, 2, q, l)];
-  }
-  const bool e1n = a.mode == G_E1N;
-  if (e1n) {
-    const double nx_ = T.nrm[l], ny_ = T.nrm[nb + l], nz_ = T.nrm[2 * nb + l];
-#pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      ox[q] = nx_ * T.off[tslot(nb, t, 0, q, l)];
-      oy[q] = ny_ * T.off[tslot(nb, t, 1, q, l)];
-      oz[q] = nz_ * T.off[tslot(nb, t, 2, q, l)];
-    }
-  }
-  const Dims& d = a.d;
-  const GField& g = a.f[c];
-  double acc = 0.0;
-  // fully unrolled: the stencil tables stay in registers
-#pragma unroll
-  for (int qk = 0; qk < 5; ++qk) {
-#pragma unroll
-    for (int qj = 0; qj < 5; ++qj) {
-      if (wy[qj] == 0.0 || wz[qk] == 0.0) continue;   // the row adds exactly nothing
-      const double wjk = T.scale * wy[qj] * wz[qk];
-#pragma unroll
-      for (int qi = 0; qi < 5; ++qi) {
-        double v;
-        if (a.mode == G_GRAD) {
-          const double* P = a.phi;
-          const double p0 = P[idxR(d, ix[qi], iy[qj], iz[qk])];
-          double gv;
-          if (t == 0) gv = (P[idxR(d, ix[qi] + 1, iy[qj], iz[qk])] - p0) * a.m.rdxg[ix[qi]];
-          else if (t == 1)
-            gv = (iy[qj] >= 2 && iy[qj] <= d.ny - 1)
-                     ? (P[idxR(d, ix[qi], iy[qj] + 1, iz[qk])] - p0) * a.m.rdyg[iy[qj]] : 0.0;
-          else gv = (P[idxR(d, ix[qi], iy[qj], iz[qk] + 1)] - p0) * a.m.rdzg[iz[qk]];
-          v = gv * a.phimul - a.reg[c][lin(g.n1, g.n2, ix[qi], iy[qj], iz[qk], 0)];
-        } else {
-          v = g.F[lin(g.n1, g.n2, ix[qi], iy[qj], iz[qk], g.rhsp)] * g.mul;
-        }
-        double term = wjk * wx[qi] * v;
-        if (e1n) term *= ox[qi] + oy[qj] + oz[qk];
-        acc += term;
-      }
-    }
-  }
-  double r = a.sign * acc;
-  const int i = c * nb + l;
-  if (a.sub) r -= a.sub[i] * a.subv[i];
-  if (a.addv) r += a.addv[i];
-  a.out[i] = r;
-}
-
-// The same gather with LANES threads per (marker, component): thread r of
-// the group walks the stencil rows (qj, qk) with qj + 5 qk = r, r+LANES, ...
-// (25/LANES rounds of five loads instead of 25), and the group adds its
-// partial sums by a fixed shuffle tree.  Eight lanes for the one-component
-// gathers, whose 36,864 threads are too few to hide 25 rounds of latency.
+// Gather of grid values to the markers, E (src/immersed_boundary_operators.f90
+// regT) and E1n (regT_1n, weights times the stencil point's offset along the
+// normal), with LANES threads per (marker, component): thread r of the group
+// walks the stencil rows (qj, qk) with qj + 5 qk = r, r+LANES, ... (25/LANES
+// rounds of five loads instead of 25), and the group adds its partial sums
+// by a fixed shuffle tree.  Rows of zero weight are skipped.
 constexpr int kGatherLanes = 8;
 template <int LANES>
 __global__ void __launch_bounds__(128) k_ib_gather8(GatherArgs a) {
@@ -608,7 +535,6 @@ __global__ void __launch_bounds__(128) k_ib_gather8(GatherArgs a) {
   const int l = valid ? (int)(gid - (int64_t)c * nb) : 0;
   const int t = a.type[c];
   const OpTables& T = a.T;
-  const Dims& d = a.d;
   const GField& g = a.f[c];
   const bool e1n = a.mode == G_E1N;
   double acc = 0.0;
@@ -632,19 +558,7 @@ __global__ void __launch_bounds__(128) k_ib_gather8(GatherArgs a) {
       const double oyz = e1n ? ny_ * T.off[tslot(nb, t, 1, qj, l)] + nz_ * T.off[tslot(nb, t, 2, qk, l)] : 0.0;
 #pragma unroll
       for (int qi = 0; qi < 5; ++qi) {
-        double v;
-        if (a.mode == G_GRAD) {
-          const double* P = a.phi;
-          const double p0 = P[idxR(d, ix[qi], iy, iz)];
-          double gv;
-          if (t == 0) gv = (P[idxR(d, ix[qi] + 1, iy, iz)] - p0) * a.m.rdxg[ix[qi]];
-          else if (t == 1)
-            gv = (iy >= 2 && iy <= d.ny - 1) ? (P[idxR(d, ix[qi], iy + 1, iz)] - p0) * a.m.rdyg[iy] : 0.0;
-          else gv = (P[idxR(d, ix[qi], iy, iz + 1)] - p0) * a.m.rdzg[iz];
-          v = gv * a.phimul - a.reg[c][lin(g.n1, g.n2, ix[qi], iy, iz, 0)];
-        } else {
-          v = g.F[lin(g.n1, g.n2, ix[qi], iy, iz, g.rhsp)] * g.mul;
-        }
+        const double v = g.F[lin(g.n1, g.n2, ix[qi], iy, iz, g.rhsp)] * g.mul;
         double term = wjk * wx[qi] * v;
         if (e1n) term *= ox[qi] + oyz;
         acc += term;
@@ -1428,6 +1342,39 @@ int ib_setup_operators(Handle* h) {
   return build_spread_maps(h);
 }
 
+// G phi - U_reg at the x-z interior points of the stencil rows [jlo, jhi]
+// (src/projection.f90:135-139: the gradient of the potential, its boundary
+// values, minus the spread field), into fields of the u, v, w shapes; v is
+// zero on the wall faces.  Rows, columns and planes are those the stencil
+// tables index (x and z interior, y rows [iy_lo, iy_hi]).
+__global__ void __launch_bounds__(256) k_grad_minus_reg(Dims d, Metric m, const double* __restrict__ P,
+                                                       const double* __restrict__ Ur,
+                                                       const double* __restrict__ Vr,
+                                                       const double* __restrict__ Wr, double* __restrict__ Gu,
+                                                       double* __restrict__ Gv, double* __restrict__ Gw, int jlo,
+                                                       int jhi) {
+  const int nxi = d.Nx, nzi = d.Nz, nr = jhi - jlo + 1;
+  const int64_t tot = (int64_t)nxi * nr * nzi;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = 2 + (int)(t % nxi);
+    const int64_t r = t / nxi;
+    const int j = jlo + (int)(r % nr);
+    const int k = 2 + (int)(r / nr);
+    const bool centre = j >= 2 && j <= d.ny;       // u and w rows
+    const double p0 = centre ? P[idxR(d, i, j, k)] : 0.0;
+    if (centre) {
+      const int64_t iu = idxU(d, i, j, k), iw = idxW(d, i, j, k);
+      Gu[iu] = (P[idxR(d, i + 1, j, k)] - p0) * m.rdxg[i] - Ur[iu];
+      Gw[iw] = (P[idxR(d, i, j, k + 1)] - p0) * m.rdzg[k] - Wr[iw];
+    }
+    if (j >= 1 && j <= d.ny) {                     // v faces
+      const double gv = (j >= 2 && j <= d.ny - 1) ? (P[idxR(d, i, j + 1, k)] - p0) * m.rdyg[j] : 0.0;
+      const int64_t iv = idxV(d, i, j, k);
+      Gv[iv] = gv - Vr[iv];
+    }
+  }
+}
+
 // gather helpers
 static GField gf_u(const Dims& d, const double* F) { return GField{F, d.nx, d.nyg, 0, 1.0}; }
 static GField gf_v(const Dims& d, const double* F) { return GField{F, d.nxg, d.ny, 0, 1.0}; }
@@ -1441,7 +1388,7 @@ static int gather3(Handle* h, int mode, const double* U, const double* V, const 
   a.f[0] = gf_u(h->d, U); a.f[1] = gf_v(h->d, V); a.f[2] = gf_w(h->d, W);
   a.type[0] = 0; a.type[1] = 1; a.type[2] = 2;
   a.ncomp = 3; a.mode = mode; a.out = out; a.sign = sign; a.sub = sub; a.subv = subv; a.addv = addv;
-  k_ib_gather<<<thread_blocks(3 * (int64_t)h->ib->nb), 128, 0, h->stream>>>(a);
+  k_ib_gather8<kGatherLanes><<<thread_blocks(3 * kGatherLanes * (int64_t)h->ib->nb), 128, 0, h->stream>>>(a);
   C3D_LAUNCH_CHECK(h);
   return 0;
 }
@@ -1600,16 +1547,13 @@ int ib_schur(Handle* h, const double* f, double* Sf, double dt) {
   if ((rc = gather_c(h, h->rhs_p, 1.0 / dt, Sf + 3 * nb, -1.0))) return rc;
   if ((rc = remove_mean(h, Sf + 3 * nb, f + 3 * nb))) return rc;
   // Sf(u) = E(G phi - U_reg) - E1nH_ext*dudn                          :129-140
-  GatherArgs a{};
-  a.T = tables(h); a.d = h->d; a.m = h->m;
-  a.f[0] = gf_u(h->d, s->Ureg); a.f[1] = gf_v(h->d, s->Vreg); a.f[2] = gf_w(h->d, s->Wreg);
-  a.type[0] = 0; a.type[1] = 1; a.type[2] = 2; a.ncomp = 3;
-  a.mode = G_GRAD; a.phi = h->rhs_p; a.phimul = 1.0;
-  a.reg[0] = s->Ureg; a.reg[1] = s->Vreg; a.reg[2] = s->Wreg;
-  a.out = Sf; a.sign = 1.0; a.sub = s->E1nH; a.subv = f;
-  k_ib_gather<<<thread_blocks(3 * (int64_t)nb), 128, 0, h->stream>>>(a);
+  // (G phi - U_reg formed once on the stencil rows, then gathered)
+  const Dims& d = h->d;
+  const int64_t npts = (int64_t)d.Nx * (s->iy_hi - s->iy_lo + 1) * d.Nz;
+  k_grad_minus_reg<<<(unsigned)std::min<int64_t>((npts + 255) / 256, 148 * 8), 256, 0, h->stream>>>(
+      d, h->m, h->rhs_p, s->Ureg, s->Vreg, s->Wreg, s->Ut, s->Vt, s->Wt, s->iy_lo, s->iy_hi);
   C3D_LAUNCH_CHECK(h);
-  return 0;
+  return gather3(h, G_E, s->Ut, s->Vt, s->Wt, Sf, 1.0, s->E1nH, f);
 }
 
 static int dot(Handle* h, const double* a, const double* b, const double* c, const double* e, int op,

@@ -91,6 +91,7 @@ struct BandState {
   // block-tridiagonal form (16 x 16 blocks: 4 lattice positions x 4 components)
   std::vector<int> nblk, blkoff;   // block rows per segment, their offset within one q
   int NBq = 0;                     // block rows per wavenumber (all segments)
+  int nblk_max = 0;                // block rows of the longest segment
   int* nblk_d = nullptr;
   int* blkoff_d = nullptr;
   double2 *Ab_d = nullptr, *Bb_d = nullptr, *Cb_d = nullptr;   // [nq][NBq][16][16]
@@ -498,8 +499,13 @@ __global__ void __launch_bounds__(256) k_blk_factor(int nseg, int NBq, const int
 
 // Block forward and back substitution of one system by one warp: lane 2r+h
 // forms half (8 terms) of row r's products; the blocks stream through a
-// shared-memory ring (cp.async, kBlkRing - 1 block rows ahead).
-constexpr int kBlkRing = 4;
+// shared-memory ring (cp.async, kBlkRing - 1 block rows ahead), and the
+// system's right-hand side sits in shared memory for the whole solve (no
+// global access inside the two sequential sweeps).
+constexpr int kBlkRing = 6;
+static size_t blk_solve_smem(int nmax) {
+  return sizeof(double2) * ((size_t)kBlkRing * 2 * kBs * kBs + (size_t)kBs * nmax);
+}
 __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, const int* __restrict__ segstart,
                                                   const int* __restrict__ seglen, const int* __restrict__ nblk,
                                                   const int* __restrict__ blkoff, const double2* __restrict__ Ab,
@@ -519,7 +525,9 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
                                                   const int* __restrict__ blkoff, const double2* __restrict__ Ab,
                                                   const double2* __restrict__ Pb, const double2* __restrict__ Gb,
                                                   double2* __restrict__ rhs) {
-  __shared__ __align__(16) double2 ring[kBlkRing][2][kBs * kBs];
+  extern __shared__ __align__(16) double2 bs_smem[];
+  double2 (*ring)[2][kBs * kBs] = reinterpret_cast<double2 (*)[2][kBs * kBs]>(bs_smem);
+  double2* xs = bs_smem + (size_t)kBlkRing * 2 * kBs * kBs;   // [kBs * N] right-hand side / solution
   __shared__ double2 vv[kBs], tt[kBs];
   const int q = blockIdx.x / nseg, sg = blockIdx.x % nseg;
   const int N = nblk[sg];
@@ -529,6 +537,7 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
   const int lane = threadIdx.x;
   const int r = lane >> 1, hh = lane & 1;
   const double2 zero = make_double2(0.0, 0.0);
+  for (int e = lane; e < kBs * N; e += 32) xs[e] = e < m ? x[e] : zero;
   // forward: slot holds (A_i, P_i)
   auto load_fwd = [&](int i) {
     if (i >= 0 && i < N) {
@@ -550,7 +559,7 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
     const double2* Ai = ring[i % kBlkRing][0];
     const double2* Pi = ring[i % kBlkRing][1];
     const int row = kBs * i + r;
-    const double2 bv = row < m ? x[row] : zero;
+    const double2 bv = xs[row];
     double2 acc = zero;
     if (i > 0)
 #pragma unroll
@@ -576,7 +585,7 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
     __syncwarp();
     if (hh == 0) {
       vv[r] = y2;
-      if (row < m) x[row] = y2;
+      xs[row] = y2;
     }
     __syncwarp();
   }
@@ -607,16 +616,18 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
     acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
     acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
     const int row = kBs * i + r;
-    const double2 yv = row < m ? x[row] : zero;
+    const double2 yv = xs[row];
     __syncwarp();
     if (hh == 0) {
       const double2 xr = csub(yv, acc);
       vv[r] = xr;
-      if (row < m) x[row] = xr;
+      xs[row] = xr;
     }
     __syncwarp();
   }
   cp_async_wait<0>();
+  __syncwarp();
+  for (int e = lane; e < m; e += 32) x[e] = xs[e];
 }
 
 // Forward and back substitution of one system (LAPACK zgbtrs, no transpose)
@@ -858,10 +869,16 @@ static int band_setup(Handle* h) {
   B->nblk.resize(B->nseg);
   B->blkoff.resize(B->nseg);
   B->NBq = 0;
+  B->nblk_max = 0;
   for (int sgi = 0; sgi < B->nseg; ++sgi) {
     B->nblk[sgi] = (4 * B->seg_len[sgi] + kBs - 1) / kBs;
     B->blkoff[sgi] = B->NBq;
     B->NBq += B->nblk[sgi];
+    B->nblk_max = std::max(B->nblk_max, B->nblk[sgi]);
+  }
+  if (blk_solve_smem(B->nblk_max) > 200 * 1024) {
+    h->last_error = "band preconditioner: a lattice segment is too long for the block solve";
+    return C3D_ERR_UNSUPPORTED;
   }
   const int64_t nbe = (int64_t)nq * B->NBq * kBs * kBs;
   if ((rc = dev_alloc(h, &B->nblk_d, B->nseg))) return rc;
@@ -898,6 +915,8 @@ static int band_setup(Handle* h) {
                                        (int)inv_smem_bytes(nzl, nq)));
   C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_band_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(sizeof(double2) * kFactorWin * kLdab)));
+  C3D_CUDA_TRY(h, cudaFuncSetAttribute(k_blk_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)blk_solve_smem(B->nblk_max)));
   return 0;
 }
 
@@ -1020,8 +1039,9 @@ int band_apply(Handle* h, const double* in, double* out) {
       nb, lat, nzl, nq, B->tw_d, B->pos_d, in, B->rhs_d);
   C3D_LAUNCH_CHECK(h);
   if (B->block) {
-    k_blk_solve<<<nq * B->nseg, 32, 0, h->stream>>>(lat, B->nseg, B->NBq, B->segstart_d, B->seglen_d, B->nblk_d,
-                                                    B->blkoff_d, B->Ab_d, B->Pb_d, B->Gb_d, B->rhs_d);
+    k_blk_solve<<<nq * B->nseg, 32, blk_solve_smem(B->nblk_max), h->stream>>>(
+        lat, B->nseg, B->NBq, B->segstart_d, B->seglen_d, B->nblk_d, B->blkoff_d, B->Ab_d, B->Pb_d, B->Gb_d,
+        B->rhs_d);
   } else {
     const size_t smem = solve_smem_bytes(lat);
     k_band_solve<<<nq * B->nseg, 32, smem, h->stream>>>(lat, B->nseg, B->segstart_d, B->seglen_d, B->AB_d,
