@@ -415,10 +415,12 @@ __global__ void k_blk_pad(int nq, int nseg, int NBq, const int* __restrict__ seg
 
 // Block LU of one system: Delta_0 = B_0, Delta_i = B_i - A_i G_{i-1},
 // P_i = Delta_i^-1 (Gauss-Jordan, partial pivoting within the block),
-// G_i = P_i C_i.  A pivot below 1e-12 of the block's largest entry sets
-// flag[1]: the caller then uses the pivoted banded LU instead.
+// G_i = P_i C_i, and Q_i = P_i A_i, which replaces A_i (the forward sweep
+// is then y_i = P_i b_i - Q_i y_{i-1}: one dependent product per block row).
+// A pivot below 1e-12 of the block's largest entry sets flag[1]: the caller
+// then uses the pivoted banded LU instead.
 __global__ void __launch_bounds__(256) k_blk_factor(int nseg, int NBq, const int* __restrict__ nblk,
-                                                    const int* __restrict__ blkoff, const double2* __restrict__ Ab,
+                                                    const int* __restrict__ blkoff, double2* __restrict__ Ab,
                                                     const double2* __restrict__ Bb, const double2* __restrict__ Cb,
                                                     double2* __restrict__ Pb, double2* __restrict__ Gb,
                                                     int* __restrict__ flag) {
@@ -485,6 +487,13 @@ __global__ void __launch_bounds__(256) k_blk_factor(int nseg, int NBq, const int
       __syncthreads();
     }
     Pb[o + tid] = Dm[r][kBs + cc];
+    if (i > 0) {
+      const double2* Ai = Ab + o;
+      double2 qv = make_double2(0.0, 0.0);
+      for (int k = 0; k < kBs; ++k) qv = cadd(qv, cmul(Dm[r][kBs + k], Ai[k * kBs + cc]));
+      __syncthreads();                            // every column of A_i read before it is replaced
+      Ab[o + tid] = qv;
+    }
     if (i + 1 < N) {
       const double2* Ci = Cb + o;
       double2 g = make_double2(0.0, 0.0);
@@ -538,16 +547,46 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
   const int r = lane >> 1, hh = lane & 1;
   const double2 zero = make_double2(0.0, 0.0);
   for (int e = lane; e < kBs * N; e += 32) xs[e] = e < m ? x[e] : zero;
-  // forward: slot holds (A_i, P_i)
+  __syncwarp();
+  // t_i = P_i b_i for every block row: independent products, the next
+  // block's half row of P loaded while this one is used
+  {
+    double2 pn[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) pn[k] = Pb[b0 + r * kBs + 8 * hh + k];
+    for (int i = 0; i < N; ++i) {
+      double2 pc[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) pc[k] = pn[k];
+      if (i + 1 < N) {
+        const double2* Pn = Pb + b0 + (int64_t)(i + 1) * kBs * kBs + r * kBs + 8 * hh;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) pn[k] = Pn[k];
+      }
+      double2 a0 = zero, a1 = zero;
+#pragma unroll
+      for (int k = 0; k < 8; k += 2) {
+        const double2 y0 = xs[kBs * i + 8 * hh + k], y1 = xs[kBs * i + 8 * hh + k + 1];
+        a0.x += pc[k].x * y0.x - pc[k].y * y0.y;
+        a0.y += pc[k].x * y0.y + pc[k].y * y0.x;
+        a1.x += pc[k + 1].x * y1.x - pc[k + 1].y * y1.y;
+        a1.y += pc[k + 1].x * y1.y + pc[k + 1].y * y1.x;
+      }
+      a0.x += a1.x;
+      a0.y += a1.y;
+      a0.x += __shfl_xor_sync(0xffffffffu, a0.x, 1);
+      a0.y += __shfl_xor_sync(0xffffffffu, a0.y, 1);
+      __syncwarp();
+      if (hh == 0) xs[kBs * i + r] = a0;
+      __syncwarp();
+    }
+  }
+  // forward: y_i = t_i - Q_i y_{i-1}; the ring holds Q_i
   auto load_fwd = [&](int i) {
-    if (i >= 0 && i < N) {
+    if (i >= 1 && i < N) {
       const int64_t o = b0 + (int64_t)i * kBs * kBs;
       double2* d0 = ring[i % kBlkRing][0];
-      double2* d1 = ring[i % kBlkRing][1];
-      for (int e = lane; e < kBs * kBs; e += 32) {
-        cp_async16(d0 + e, Ab + o + e);
-        cp_async16(d1 + e, Pb + o + e);
-      }
+      for (int e = lane; e < kBs * kBs; e += 32) cp_async16(d0 + e, Ab + o + e);
     }
     cp_async_commit();
   };
@@ -556,36 +595,29 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
     load_fwd(i + kBlkRing - 1);
     cp_async_wait<kBlkRing - 1>();
     __syncwarp();
-    const double2* Ai = ring[i % kBlkRing][0];
-    const double2* Pi = ring[i % kBlkRing][1];
+    const double2* Qi = ring[i % kBlkRing][0];
     const int row = kBs * i + r;
-    const double2 bv = xs[row];
-    double2 acc = zero;
+    const double2 tv = xs[row];
+    double2 a0 = zero, a1 = zero;
     if (i > 0)
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const double2 a = Ai[r * kBs + 8 * hh + k], y = vv[8 * hh + k];
-        acc.x += a.x * y.x - a.y * y.y;
-        acc.y += a.x * y.y + a.y * y.x;
+      for (int k = 0; k < 8; k += 2) {
+        const double2 q0 = Qi[r * kBs + 8 * hh + k], y0 = vv[8 * hh + k];
+        const double2 q1 = Qi[r * kBs + 8 * hh + k + 1], y1 = vv[8 * hh + k + 1];
+        a0.x += q0.x * y0.x - q0.y * y0.y;
+        a0.y += q0.x * y0.y + q0.y * y0.x;
+        a1.x += q1.x * y1.x - q1.y * y1.y;
+        a1.y += q1.x * y1.y + q1.y * y1.x;
       }
-    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
-    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
-    __syncwarp();
-    if (hh == 0) tt[r] = csub(bv, acc);
-    __syncwarp();
-    double2 y2 = zero;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const double2 a = Pi[r * kBs + 8 * hh + k], t = tt[8 * hh + k];
-      y2.x += a.x * t.x - a.y * t.y;
-      y2.y += a.x * t.y + a.y * t.x;
-    }
-    y2.x += __shfl_xor_sync(0xffffffffu, y2.x, 1);
-    y2.y += __shfl_xor_sync(0xffffffffu, y2.y, 1);
+    a0.x += a1.x;
+    a0.y += a1.y;
+    a0.x += __shfl_xor_sync(0xffffffffu, a0.x, 1);
+    a0.y += __shfl_xor_sync(0xffffffffu, a0.y, 1);
     __syncwarp();
     if (hh == 0) {
-      vv[r] = y2;
-      xs[row] = y2;
+      const double2 y = csub(tv, a0);
+      vv[r] = y;
+      xs[row] = y;
     }
     __syncwarp();
   }
@@ -606,13 +638,18 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
     cp_async_wait<kBlkRing - 1>();
     __syncwarp();
     const double2* Gi = ring[i % kBlkRing][0];
-    double2 acc = zero;
+    double2 acc = zero, a1 = zero;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const double2 a = Gi[r * kBs + 8 * hh + k], y = vv[8 * hh + k];
-      acc.x += a.x * y.x - a.y * y.y;
-      acc.y += a.x * y.y + a.y * y.x;
+    for (int k = 0; k < 8; k += 2) {
+      const double2 g0 = Gi[r * kBs + 8 * hh + k], y0 = vv[8 * hh + k];
+      const double2 g1 = Gi[r * kBs + 8 * hh + k + 1], y1 = vv[8 * hh + k + 1];
+      acc.x += g0.x * y0.x - g0.y * y0.y;
+      acc.y += g0.x * y0.y + g0.y * y0.x;
+      a1.x += g1.x * y1.x - g1.y * y1.y;
+      a1.y += g1.x * y1.y + g1.y * y1.x;
     }
+    acc.x += a1.x;
+    acc.y += a1.y;
     acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
     acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
     const int row = kBs * i + r;
