@@ -99,6 +99,7 @@ struct IbState {
 // learned-preconditioner entry points used by the Schur solver (k_mlp.cu):
 // the band factors from the network's prediction at the current geometry,
 // and, while collection is on, a training set from each probed band
+int mlp_prepare_band(Handle* h);
 int mlp_build_band(Handle* h, double dt);
 bool mlp_collecting(const Handle* h);
 int mlp_add_probe_set(Handle* h);

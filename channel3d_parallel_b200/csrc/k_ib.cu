@@ -1485,9 +1485,10 @@ static int spread(Handle* h, int mode, int comp0, int ncomp, const double* f, do
 // zeros or values of earlier geometries that no banded reader touches)
 static int reg_all_band(Handle* h, int mode, const double* f, double dt, int jlo, int jhi) {
   IbState* s = h->ib;
-  int rc = spread(h, mode, 0, 3, f, dt, s->Ureg, s->Vreg, s->Wreg, jlo, jhi);
-  if (rc) return rc;
-  return launch_fill_ghosts3(h, s->Ureg, s->Vreg, s->Wreg);
+  // no ghost fill: the band divergence (k_xfft_fwd) folds the periodic x and
+  // z images and the wall faces itself, and the gathers read x-z interior
+  // points only
+  return spread(h, mode, 0, 3, f, dt, s->Ureg, s->Vreg, s->Wreg, jlo, jhi);
 }
 
 static int reg_all(Handle* h, int mode, const double* f, double dt) {
@@ -1740,6 +1741,9 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
   // (LEARNED) at every new geometry; timed as preconditioner builds
   const bool need_probe = mode == C3D_PRECOND_BAND && band_stale(h, dt);
   const bool need_learn = mode == C3D_PRECOND_LEARNED && !s->have_lrn;
+  // allocations out of the timed build
+  if (need_learn && (rc = mlp_prepare_band(h))) return rc;
+  if (need_probe && !s->prb && (rc = dev_alloc(h, &s->prb, 16 * (int64_t)s->nb))) return rc;
   if (need_probe || need_learn) {
     C3D_CUDA_TRY(h, cudaEventRecord(s->ev_a, h->stream));
     if (need_probe) {

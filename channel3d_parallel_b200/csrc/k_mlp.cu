@@ -813,20 +813,31 @@ static int upload_sigT(Handle* h) {
 
 // The network's band symbol at the current geometry, factored for the
 // solver (k_ib_band.cu).
-int mlp_build_band(Handle* h, double dt) {
-  IbState* s = h->ib;
+// the feature and output buffers of the predicted band (allocated once, out
+// of the timed build)
+int mlp_prepare_band(Handle* h) {
   int rc;
   if ((rc = mlp_ensure(h))) return rc;
   MlpState* S = h->mlp;
   const BandView v = band_view(h);
   if (v.lat == 0) { h->last_error = "learned preconditioner: unsupported marker lattice"; return C3D_ERR_UNSUPPORTED; }
-  if (!S->have_sigT) { h->last_error = "learned preconditioner: no training set (precond_probe / collect first)"; return C3D_ERR_PARAM; }
   const int64_t rows = lb_rows(v);
   if (S->q_rows < rows) {
     if ((rc = dev_alloc(h, &S->fq, rows * kF))) return rc;
     if ((rc = dev_alloc(h, &S->oq, rows * kO))) return rc;
     S->q_rows = (int)rows;
   }
+  return 0;
+}
+
+int mlp_build_band(Handle* h, double dt) {
+  IbState* s = h->ib;
+  int rc;
+  if ((rc = mlp_prepare_band(h))) return rc;
+  MlpState* S = h->mlp;
+  const BandView v = band_view(h);
+  if (!S->have_sigT) { h->last_error = "learned preconditioner: no training set (precond_probe / collect first)"; return C3D_ERR_PARAM; }
+  const int64_t rows = lb_rows(v);
   const LbArgs a = lb_args(h, v);
   const unsigned gb = (unsigned)std::min<int64_t>((rows + 255) / 256, 148 * 8);
   k_lb_features<<<gb, 256, 0, h->stream>>>(a, S->fq);
