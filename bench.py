@@ -39,6 +39,18 @@ DT = 1e-3
 WORKLOAD = "channel Re_tau=180 192x129x192 (nx_global=194, ny_global=129, nz_global=194), RK3, dt=1e-3"
 
 
+def max_over_ranks(x, pg=None, device="cuda"):
+    """The largest of a per-rank time over the process group (x itself
+    without one): a whole-job rate is the ranks' work over the slowest
+    rank's time."""
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -482,10 +494,8 @@ def run_ours(args):
     torch.cuda.synchronize()
     clk = clocks.stop()
     launches = ch.kernel_launches() - l0
+    ms_step = max_over_ranks(ms_step, pg)
     if pg:
-        t = torch.tensor([ms_step], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_step = float(t.item())
         pg.barrier()
     value = ws / (ms_step * 1e-3)
     div = ch.check_divergence()
@@ -554,10 +564,7 @@ def run_ours(args):
             cl, cu = L.box(lb, ub)
             L.check(ch._lib.c3d_download(ch.handle, L.FIELD[name], L.dptr(out), cl, cu), ch.handle)
     e2e_sec = (time.perf_counter() - t0) / e2e_steps
-    if pg:
-        t = torch.tensor([e2e_sec], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_sec = float(t.item())
+    e2e_sec = max_over_ranks(e2e_sec, pg)
     e2e_val = ws / e2e_sec
 
     extras = {}

@@ -302,16 +302,27 @@ __global__ void __launch_bounds__(256) k_band_fwd(int nb, int lat, int nzl, int 
   for (int qq = ql; qq < kFwdQ; qq += 8) {
     const int q = q0 + qq;
     if (q >= nq) break;
-    double re = 0.0, im = 0.0;
+    // two interleaved partial sums (even and odd iz): half-length FMA chains
+    double re0 = 0.0, im0 = 0.0, re1 = 0.0, im1 = 0.0;
     int k = 0;
-    for (int iz = 0; iz < nzl; ++iz) {
-      const double xv = xs[iz * 32 + mm];
-      re += xv * twc[k];
-      im -= xv * tws[k];
-      k += q;
+    int iz = 0;
+    for (; iz + 1 < nzl; iz += 2) {
+      const double x0 = xs[iz * 32 + mm], x1 = xs[(iz + 1) * 32 + mm];
+      int k1 = k + q;
+      if (k1 >= nzl) k1 -= nzl;
+      re0 += x0 * twc[k];
+      im0 -= x0 * tws[k];
+      re1 += x1 * twc[k1];
+      im1 -= x1 * tws[k1];
+      k = k1 + q;
       if (k >= nzl) k -= nzl;
     }
-    rhs[(int64_t)q * 4 * lat + row] = make_double2(re, im);
+    if (iz < nzl) {
+      const double x0 = xs[iz * 32 + mm];
+      re0 += x0 * twc[k];
+      im0 -= x0 * tws[k];
+    }
+    rhs[(int64_t)q * 4 * lat + row] = make_double2(re0 + re1, im0 + im1);
   }
 }
 
@@ -351,15 +362,24 @@ __global__ void __launch_bounds__(256) k_band_inv(int nb, int lat, int nzl, int 
   for (int zz = zl; zz < kInvZ; zz += 8) {
     const int iz = z0 + zz;
     if (iz >= nzl) break;
-    double acc = 0.0;
+    // two interleaved partial sums (even and odd q): half-length FMA chains
+    double acc0 = 0.0, acc1 = 0.0;
     int k = 0;
-    for (int q = 0; q < nq; ++q) {
-      const double2 xv = xs[q * 32 + mm];
-      acc += xv.x * twc[k] - xv.y * tws[k];
-      k += iz;
+    int q = 0;
+    for (; q + 1 < nq; q += 2) {
+      const double2 x0 = xs[q * 32 + mm], x1 = xs[(q + 1) * 32 + mm];
+      int k1 = k + iz;
+      if (k1 >= nzl) k1 -= nzl;
+      acc0 += x0.x * twc[k] - x0.y * tws[k];
+      acc1 += x1.x * twc[k1] - x1.y * tws[k1];
+      k = k1 + iz;
       if (k >= nzl) k -= nzl;
     }
-    v[(int64_t)c * nb + m0 + mm + (int64_t)lat * iz] = acc * inv;
+    if (q < nq) {
+      const double2 x0 = xs[q * 32 + mm];
+      acc0 += x0.x * twc[k] - x0.y * tws[k];
+    }
+    v[(int64_t)c * nb + m0 + mm + (int64_t)lat * iz] = (acc0 + acc1) * inv;
   }
 }
 
@@ -511,9 +531,9 @@ __global__ void __launch_bounds__(256) k_blk_factor(int nseg, int NBq, const int
 // shared-memory ring (cp.async, kBlkRing - 1 block rows ahead), and the
 // system's right-hand side sits in shared memory for the whole solve (no
 // global access inside the two sequential sweeps).
-constexpr int kBlkRing = 6;
+constexpr int kBlkRing = 16;    // one 16x16 block per stage: 15 blocks (60 KB) in flight
 static size_t blk_solve_smem(int nmax) {
-  return sizeof(double2) * ((size_t)kBlkRing * 2 * kBs * kBs + (size_t)kBs * nmax);
+  return sizeof(double2) * ((size_t)kBlkRing * kBs * kBs + (size_t)kBs * nmax);
 }
 __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, const int* __restrict__ segstart,
                                                   const int* __restrict__ seglen, const int* __restrict__ nblk,
@@ -535,8 +555,8 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
                                                   const double2* __restrict__ Pb, const double2* __restrict__ Gb,
                                                   double2* __restrict__ rhs) {
   extern __shared__ __align__(16) double2 bs_smem[];
-  double2 (*ring)[2][kBs * kBs] = reinterpret_cast<double2 (*)[2][kBs * kBs]>(bs_smem);
-  double2* xs = bs_smem + (size_t)kBlkRing * 2 * kBs * kBs;   // [kBs * N] right-hand side / solution
+  double2 (*ring)[kBs * kBs] = reinterpret_cast<double2 (*)[kBs * kBs]>(bs_smem);
+  double2* xs = bs_smem + (size_t)kBlkRing * kBs * kBs;   // [kBs * N] right-hand side / solution
   __shared__ double2 vv[kBs], tt[kBs];
   const int q = blockIdx.x / nseg, sg = blockIdx.x % nseg;
   const int N = nblk[sg];
@@ -548,44 +568,47 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
   const double2 zero = make_double2(0.0, 0.0);
   for (int e = lane; e < kBs * N; e += 32) xs[e] = e < m ? x[e] : zero;
   __syncwarp();
-  // t_i = P_i b_i for every block row: independent products, the next
-  // block's half row of P loaded while this one is used
-  {
-    double2 pn[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) pn[k] = Pb[b0 + r * kBs + 8 * hh + k];
-    for (int i = 0; i < N; ++i) {
-      double2 pc[8];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) pc[k] = pn[k];
-      if (i + 1 < N) {
-        const double2* Pn = Pb + b0 + (int64_t)(i + 1) * kBs * kBs + r * kBs + 8 * hh;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) pn[k] = Pn[k];
-      }
-      double2 a0 = zero, a1 = zero;
-#pragma unroll
-      for (int k = 0; k < 8; k += 2) {
-        const double2 y0 = xs[kBs * i + 8 * hh + k], y1 = xs[kBs * i + 8 * hh + k + 1];
-        a0.x += pc[k].x * y0.x - pc[k].y * y0.y;
-        a0.y += pc[k].x * y0.y + pc[k].y * y0.x;
-        a1.x += pc[k + 1].x * y1.x - pc[k + 1].y * y1.y;
-        a1.y += pc[k + 1].x * y1.y + pc[k + 1].y * y1.x;
-      }
-      a0.x += a1.x;
-      a0.y += a1.y;
-      a0.x += __shfl_xor_sync(0xffffffffu, a0.x, 1);
-      a0.y += __shfl_xor_sync(0xffffffffu, a0.y, 1);
-      __syncwarp();
-      if (hh == 0) xs[kBs * i + r] = a0;
-      __syncwarp();
+  // t_i = P_i b_i for every block row: independent products, P_i streamed
+  // through the ring
+  auto load_p = [&](int i) {
+    if (i < N) {
+      const int64_t o = b0 + (int64_t)i * kBs * kBs;
+      double2* d0 = ring[i % kBlkRing];
+      for (int e = lane; e < kBs * kBs; e += 32) cp_async16(d0 + e, Pb + o + e);
     }
+    cp_async_commit();
+  };
+  for (int i = 0; i < kBlkRing - 1; ++i) load_p(i);
+  for (int i = 0; i < N; ++i) {
+    load_p(i + kBlkRing - 1);
+    cp_async_wait<kBlkRing - 1>();
+    __syncwarp();
+    const double2* Pi = ring[i % kBlkRing];
+    double2 a0 = zero, a1 = zero;
+#pragma unroll
+    for (int k = 0; k < 8; k += 2) {
+      const double2 p0 = Pi[r * kBs + 8 * hh + k], y0 = xs[kBs * i + 8 * hh + k];
+      const double2 p1 = Pi[r * kBs + 8 * hh + k + 1], y1 = xs[kBs * i + 8 * hh + k + 1];
+      a0.x += p0.x * y0.x - p0.y * y0.y;
+      a0.y += p0.x * y0.y + p0.y * y0.x;
+      a1.x += p1.x * y1.x - p1.y * y1.y;
+      a1.y += p1.x * y1.y + p1.y * y1.x;
+    }
+    a0.x += a1.x;
+    a0.y += a1.y;
+    a0.x += __shfl_xor_sync(0xffffffffu, a0.x, 1);
+    a0.y += __shfl_xor_sync(0xffffffffu, a0.y, 1);
+    __syncwarp();
+    if (hh == 0) xs[kBs * i + r] = a0;
+    __syncwarp();
   }
+  cp_async_wait<0>();
+  __syncwarp();
   // forward: y_i = t_i - Q_i y_{i-1}; the ring holds Q_i
   auto load_fwd = [&](int i) {
     if (i >= 1 && i < N) {
       const int64_t o = b0 + (int64_t)i * kBs * kBs;
-      double2* d0 = ring[i % kBlkRing][0];
+      double2* d0 = ring[i % kBlkRing];
       for (int e = lane; e < kBs * kBs; e += 32) cp_async16(d0 + e, Ab + o + e);
     }
     cp_async_commit();
@@ -595,7 +618,7 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
     load_fwd(i + kBlkRing - 1);
     cp_async_wait<kBlkRing - 1>();
     __syncwarp();
-    const double2* Qi = ring[i % kBlkRing][0];
+    const double2* Qi = ring[i % kBlkRing];
     const int row = kBs * i + r;
     const double2 tv = xs[row];
     double2 a0 = zero, a1 = zero;
@@ -627,7 +650,7 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
   auto load_bwd = [&](int i) {
     if (i >= 0 && i < N - 1) {
       const int64_t o = b0 + (int64_t)i * kBs * kBs;
-      double2* d0 = ring[i % kBlkRing][0];
+      double2* d0 = ring[i % kBlkRing];
       for (int e = lane; e < kBs * kBs; e += 32) cp_async16(d0 + e, Gb + o + e);
     }
     cp_async_commit();
@@ -637,7 +660,7 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
     load_bwd(i - (kBlkRing - 1));
     cp_async_wait<kBlkRing - 1>();
     __syncwarp();
-    const double2* Gi = ring[i % kBlkRing][0];
+    const double2* Gi = ring[i % kBlkRing];
     double2 acc = zero, a1 = zero;
 #pragma unroll
     for (int k = 0; k < 8; k += 2) {
