@@ -729,9 +729,22 @@ __global__ void __launch_bounds__(256) k_sp_gather(SpGather g0, SpGather g1, SpG
     double acc = 0.0;
     for (int cb = lo; cb < hi; cb += kSpChunk) {
       const int m = min(kSpChunk, hi - cb);
-      for (int u = lane; u < m; u += 32) {
-        ws[u] = g.w[cb + u];
-        as[u] = a[g.ent[cb + u] >> 7];
+      // all loads of the chunk in flight before the marker amplitudes they
+      // index, then the stores
+      double wv[kSpChunk / 32], av[kSpChunk / 32];
+      uint32_t ev[kSpChunk / 32];
+#pragma unroll
+      for (int u = 0; u < kSpChunk / 32; ++u) {
+        const int e = lane + 32 * u;
+        wv[u] = e < m ? g.w[cb + e] : 0.0;
+        ev[u] = e < m ? g.ent[cb + e] : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < kSpChunk / 32; ++u) av[u] = lane + 32 * u < m ? a[ev[u] >> 7] : 0.0;
+#pragma unroll
+      for (int u = 0; u < kSpChunk / 32; ++u) {
+        ws[lane + 32 * u] = wv[u];
+        as[lane + 32 * u] = av[u];
       }
       __syncwarp();
       const int e1 = min(o + n, cb + m);

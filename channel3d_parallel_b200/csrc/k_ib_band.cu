@@ -39,6 +39,7 @@
 
 #include "c3d_internal.cuh"
 #include "ib_state.cuh"
+#include "bulk.cuh"
 
 namespace c3d {
 
@@ -290,9 +291,17 @@ __global__ void __launch_bounds__(256) k_band_fwd(int nb, int lat, int nzl, int 
   const int m0 = blockIdx.x * 32;
   const int q0 = blockIdx.z * kFwdQ;
   const int tid = threadIdx.x;
-  for (int e = tid; e < 32 * nzl; e += 256) {
-    const int iz = e >> 5, mm = e & 31;
-    xs[e] = (m0 + mm < lat) ? v[(int64_t)c * nb + m0 + mm + (int64_t)lat * iz] : 0.0;
+  // eight loads in flight per thread before any store
+  for (int e0 = tid; e0 < 32 * nzl; e0 += 8 * 256) {
+    double tv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + u * 256, iz = e >> 5, mm = e & 31;
+      tv[u] = (e < 32 * nzl && m0 + mm < lat) ? v[(int64_t)c * nb + m0 + mm + (int64_t)lat * iz] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (e0 + u * 256 < 32 * nzl) xs[e0 + u * 256] = tv[u];
   }
   for (int e = tid; e < nzl; e += 256) { twc[e] = tw[e]; tws[e] = tw[nzl + e]; }
   __syncthreads();
@@ -343,16 +352,23 @@ __global__ void __launch_bounds__(256) k_band_inv(int nb, int lat, int nzl, int 
   const int m0 = blockIdx.x * 32;
   const int z0 = blockIdx.z * kInvZ;
   const int tid = threadIdx.x;
-  for (int e = tid; e < 32 * nq; e += 256) {
-    const int q = e >> 5, mm = e & 31;
-    double2 xv = make_double2(0.0, 0.0);
-    if (m0 + mm < lat) {
-      xv = rhs[(int64_t)q * 4 * lat + 4 * pos[m0 + mm] + c];
-      const double w = (q == 0 || 2 * q == nzl) ? 1.0 : 2.0;
-      xv.x *= w;
-      xv.y *= w;
+  const int prow = (m0 + (tid & 31) < lat) ? 4 * pos[m0 + (tid & 31)] + c : 0;
+  // eight loads in flight per thread before any store
+  for (int e0 = tid; e0 < 32 * nq; e0 += 8 * 256) {
+    double2 tv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + u * 256, q = e >> 5;
+      tv[u] = (e < 32 * nq && m0 + (e & 31) < lat) ? rhs[(int64_t)q * 4 * lat + prow] : make_double2(0.0, 0.0);
     }
-    xs[e] = xv;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + u * 256, q = e >> 5;
+      if (e < 32 * nq) {
+        const double w = (q == 0 || 2 * q == nzl) ? 1.0 : 2.0;
+        xs[e] = make_double2(w * tv[u].x, w * tv[u].y);
+      }
+    }
   }
   for (int e = tid; e < nzl; e += 256) { twc[e] = tw[e]; tws[e] = tw[nzl + e]; }
   __syncthreads();
@@ -539,7 +555,7 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
                                                   const int* __restrict__ seglen, const int* __restrict__ nblk,
                                                   const int* __restrict__ blkoff, const double2* __restrict__ Ab,
                                                   const double2* __restrict__ Pb, const double2* __restrict__ Gb,
-                                                  double2* __restrict__ rhs);
+                                                  double2* __restrict__ rhs, int* __restrict__ flag);
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -553,11 +569,12 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
                                                   const int* __restrict__ seglen, const int* __restrict__ nblk,
                                                   const int* __restrict__ blkoff, const double2* __restrict__ Ab,
                                                   const double2* __restrict__ Pb, const double2* __restrict__ Gb,
-                                                  double2* __restrict__ rhs) {
-  extern __shared__ __align__(16) double2 bs_smem[];
+                                                  double2* __restrict__ rhs, int* __restrict__ flag) {
+  extern __shared__ __align__(128) double2 bs_smem[];
   double2 (*ring)[kBs * kBs] = reinterpret_cast<double2 (*)[kBs * kBs]>(bs_smem);
   double2* xs = bs_smem + (size_t)kBlkRing * kBs * kBs;   // [kBs * N] right-hand side / solution
-  __shared__ double2 vv[kBs], tt[kBs];
+  __shared__ double2 vv[kBs];
+  __shared__ __align__(8) uint64_t bar[kBlkRing];
   const int q = blockIdx.x / nseg, sg = blockIdx.x % nseg;
   const int N = nblk[sg];
   const int m = 4 * seglen[sg];
@@ -566,29 +583,42 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
   const int lane = threadIdx.x;
   const int r = lane >> 1, hh = lane & 1;
   const double2 zero = make_double2(0.0, 0.0);
+  if (lane == 0) {
+    for (int k = 0; k < kBlkRing; ++k) mbar_init(&bar[k], 1);
+    fence_mbar_init();
+  }
   for (int e = lane; e < kBs * N; e += 32) xs[e] = e < m ? x[e] : zero;
   __syncwarp();
-  // t_i = P_i b_i for every block row: independent products, P_i streamed
-  // through the ring
-  auto load_p = [&](int i) {
-    if (i < N) {
-      const int64_t o = b0 + (int64_t)i * kBs * kBs;
-      double2* d0 = ring[i % kBlkRing];
-      for (int e = lane; e < kBs * kBs; e += 32) cp_async16(d0 + e, Pb + o + e);
+  // Blocks stream through a ring of kBlkRing slots, one bulk copy (4 KB) per
+  // block on the slot's mbarrier; `issued` and `used` count blocks over all
+  // three passes, so slot and phase follow from them.
+  unsigned issued = 0, used = 0;
+  bool ok = true;
+  constexpr unsigned kBlkBytes = kBs * kBs * sizeof(double2);
+  auto issue = [&](const double2* src) {
+    const unsigned slot = issued % kBlkRing;
+    if (lane == 0) {
+      fence_async_shared();            // this warp's reads of the slot come first
+      mbar_arrive_expect_tx(&bar[slot], kBlkBytes);
+      bulk_load(ring[slot], src, kBlkBytes, &bar[slot]);
     }
-    cp_async_commit();
+    ++issued;
   };
-  for (int i = 0; i < kBlkRing - 1; ++i) load_p(i);
-  for (int i = 0; i < N; ++i) {
-    load_p(i + kBlkRing - 1);
-    cp_async_wait<kBlkRing - 1>();
-    __syncwarp();
-    const double2* Pi = ring[i % kBlkRing];
+  auto acquire = [&]() -> const double2* {
+    const unsigned slot = used % kBlkRing;
+    if (!mbar_wait(&bar[slot], (used / kBlkRing) & 1u, kWaitCycles)) ok = false;
+    ++used;
+    return ring[slot];
+  };
+  auto blk = [&](const double2* base, int i) { return base + b0 + (int64_t)i * kBs * kBs; };
+  // 16-term complex dot product of row r with a 16-vector in shared memory
+  // (two lanes, eight terms each, two partial sums)
+  auto rowdot = [&](const double2* M, const double2* v) {
     double2 a0 = zero, a1 = zero;
 #pragma unroll
     for (int k = 0; k < 8; k += 2) {
-      const double2 p0 = Pi[r * kBs + 8 * hh + k], y0 = xs[kBs * i + 8 * hh + k];
-      const double2 p1 = Pi[r * kBs + 8 * hh + k + 1], y1 = xs[kBs * i + 8 * hh + k + 1];
+      const double2 p0 = M[r * kBs + 8 * hh + k], y0 = v[8 * hh + k];
+      const double2 p1 = M[r * kBs + 8 * hh + k + 1], y1 = v[8 * hh + k + 1];
       a0.x += p0.x * y0.x - p0.y * y0.y;
       a0.y += p0.x * y0.y + p0.y * y0.x;
       a1.x += p1.x * y1.x - p1.y * y1.y;
@@ -598,96 +628,53 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
     a0.y += a1.y;
     a0.x += __shfl_xor_sync(0xffffffffu, a0.x, 1);
     a0.y += __shfl_xor_sync(0xffffffffu, a0.y, 1);
+    return a0;
+  };
+  // t_i = P_i b_i for every block row (independent products)
+  for (int i = 0; i < N && i < kBlkRing - 1; ++i) issue(blk(Pb, i));
+  for (int i = 0; i < N; ++i) {
+    if (i + kBlkRing - 1 < N) issue(blk(Pb, i + kBlkRing - 1));
+    const double2* Pi = acquire();
+    const double2 t = rowdot(Pi, xs + kBs * i);
     __syncwarp();
-    if (hh == 0) xs[kBs * i + r] = a0;
+    if (hh == 0) xs[kBs * i + r] = t;
     __syncwarp();
   }
-  cp_async_wait<0>();
-  __syncwarp();
-  // forward: y_i = t_i - Q_i y_{i-1}; the ring holds Q_i
-  auto load_fwd = [&](int i) {
-    if (i >= 1 && i < N) {
-      const int64_t o = b0 + (int64_t)i * kBs * kBs;
-      double2* d0 = ring[i % kBlkRing];
-      for (int e = lane; e < kBs * kBs; e += 32) cp_async16(d0 + e, Ab + o + e);
-    }
-    cp_async_commit();
-  };
-  for (int i = 0; i < kBlkRing - 1; ++i) load_fwd(i);
+  // forward: y_i = t_i - Q_i y_{i-1} (Q_i = P_i A_i, stored in place of A_i)
+  for (int i = 1; i < N && i < kBlkRing; ++i) issue(blk(Ab, i));
   for (int i = 0; i < N; ++i) {
-    load_fwd(i + kBlkRing - 1);
-    cp_async_wait<kBlkRing - 1>();
-    __syncwarp();
-    const double2* Qi = ring[i % kBlkRing];
+    if (i > 0 && i + kBlkRing - 1 < N) issue(blk(Ab, i + kBlkRing - 1));
     const int row = kBs * i + r;
-    const double2 tv = xs[row];
-    double2 a0 = zero, a1 = zero;
-    if (i > 0)
-#pragma unroll
-      for (int k = 0; k < 8; k += 2) {
-        const double2 q0 = Qi[r * kBs + 8 * hh + k], y0 = vv[8 * hh + k];
-        const double2 q1 = Qi[r * kBs + 8 * hh + k + 1], y1 = vv[8 * hh + k + 1];
-        a0.x += q0.x * y0.x - q0.y * y0.y;
-        a0.y += q0.x * y0.y + q0.y * y0.x;
-        a1.x += q1.x * y1.x - q1.y * y1.y;
-        a1.y += q1.x * y1.y + q1.y * y1.x;
-      }
-    a0.x += a1.x;
-    a0.y += a1.y;
-    a0.x += __shfl_xor_sync(0xffffffffu, a0.x, 1);
-    a0.y += __shfl_xor_sync(0xffffffffu, a0.y, 1);
+    double2 y = xs[row];
+    if (i > 0) {
+      const double2* Qi = acquire();
+      y = csub(y, rowdot(Qi, vv));
+    }
     __syncwarp();
     if (hh == 0) {
-      const double2 y = csub(tv, a0);
       vv[r] = y;
       xs[row] = y;
     }
     __syncwarp();
   }
-  cp_async_wait<0>();
-  __syncwarp();
   // backward: x_i = y_i - G_i x_{i+1}; vv holds x_{i+1}
-  auto load_bwd = [&](int i) {
-    if (i >= 0 && i < N - 1) {
-      const int64_t o = b0 + (int64_t)i * kBs * kBs;
-      double2* d0 = ring[i % kBlkRing];
-      for (int e = lane; e < kBs * kBs; e += 32) cp_async16(d0 + e, Gb + o + e);
-    }
-    cp_async_commit();
-  };
-  for (int k = 0; k < kBlkRing - 1; ++k) load_bwd(N - 2 - k);
+  for (int k = 0; k < kBlkRing - 1 && N - 2 - k >= 0; ++k) issue(blk(Gb, N - 2 - k));
   for (int i = N - 2; i >= 0; --i) {
-    load_bwd(i - (kBlkRing - 1));
-    cp_async_wait<kBlkRing - 1>();
-    __syncwarp();
-    const double2* Gi = ring[i % kBlkRing];
-    double2 acc = zero, a1 = zero;
-#pragma unroll
-    for (int k = 0; k < 8; k += 2) {
-      const double2 g0 = Gi[r * kBs + 8 * hh + k], y0 = vv[8 * hh + k];
-      const double2 g1 = Gi[r * kBs + 8 * hh + k + 1], y1 = vv[8 * hh + k + 1];
-      acc.x += g0.x * y0.x - g0.y * y0.y;
-      acc.y += g0.x * y0.y + g0.y * y0.x;
-      a1.x += g1.x * y1.x - g1.y * y1.y;
-      a1.y += g1.x * y1.y + g1.y * y1.x;
-    }
-    acc.x += a1.x;
-    acc.y += a1.y;
-    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
-    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+    if (i - (kBlkRing - 1) >= 0) issue(blk(Gb, i - (kBlkRing - 1)));
+    const double2* Gi = acquire();
+    const double2 a = rowdot(Gi, vv);
     const int row = kBs * i + r;
     const double2 yv = xs[row];
     __syncwarp();
     if (hh == 0) {
-      const double2 xr = csub(yv, acc);
+      const double2 xr = csub(yv, a);
       vv[r] = xr;
       xs[row] = xr;
     }
     __syncwarp();
   }
-  cp_async_wait<0>();
-  __syncwarp();
   for (int e = lane; e < m; e += 32) x[e] = xs[e];
+  if (!ok && lane == 0) atomicOr(flag + 3, 1);
 }
 
 // Forward and back substitution of one system (LAPACK zgbtrs, no transpose)
@@ -1101,7 +1088,7 @@ int band_apply(Handle* h, const double* in, double* out) {
   if (B->block) {
     k_blk_solve<<<nq * B->nseg, 32, blk_solve_smem(B->nblk_max), h->stream>>>(
         lat, B->nseg, B->NBq, B->segstart_d, B->seglen_d, B->nblk_d, B->blkoff_d, B->Ab_d, B->Pb_d, B->Gb_d,
-        B->rhs_d);
+        B->rhs_d, B->flag_d);
   } else {
     const size_t smem = solve_smem_bytes(lat);
     k_band_solve<<<nq * B->nseg, 32, smem, h->stream>>>(lat, B->nseg, B->segstart_d, B->seglen_d, B->AB_d,

@@ -719,9 +719,19 @@ __global__ void __launch_bounds__(256) k_spectral_band(BandYzArgs a) {
   for (int t = tid; t < Nz; t += nt) tw[t] = a.tw[t];
   pdl_wait();
   pdl_trigger();
-  for (int t = tid; t < nr * Nz; t += nt) {
-    const int r = t / Nz, c = t - r * Nz;
-    data[r * RS + c] = g[(int64_t)r * a.pz + c];
+  // eight loads in flight per thread before any store
+  for (int t0 = tid; t0 < nr * Nz; t0 += 8 * nt) {
+    double2 tv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = t0 + u * nt, r = t / Nz, c = t - r * Nz;
+      tv[u] = t < nr * Nz ? g[(int64_t)r * a.pz + c] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = t0 + u * nt, r = t / Nz, c = t - r * Nz;
+      if (t < nr * Nz) data[r * RS + c] = tv[u];
+    }
   }
   __syncthreads();
   fft_rows_dif<double, kYzMaxRWide>(data, nr, RS, tw, a.P);
