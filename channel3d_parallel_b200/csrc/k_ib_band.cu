@@ -449,96 +449,124 @@ __global__ void k_blk_pad(int nq, int nseg, int NBq, const int* __restrict__ seg
     if (kBs * i + rr >= m) Bb[o + rr * kBs + rr] = make_double2(1.0, 0.0);
 }
 
-// Block LU of one system: Delta_0 = B_0, Delta_i = B_i - A_i G_{i-1},
-// P_i = Delta_i^-1 (Gauss-Jordan, partial pivoting within the block),
-// G_i = P_i C_i, and Q_i = P_i A_i, which replaces A_i (the forward sweep
-// is then y_i = P_i b_i - Q_i y_{i-1}: one dependent product per block row).
-// A pivot below 1e-12 of the block's largest entry sets flag[1]: the caller
-// then uses the pivoted banded LU instead.
-__global__ void __launch_bounds__(256) k_blk_factor(int nseg, int NBq, const int* __restrict__ nblk,
-                                                    const int* __restrict__ blkoff, double2* __restrict__ Ab,
-                                                    const double2* __restrict__ Bb, const double2* __restrict__ Cb,
-                                                    double2* __restrict__ Pb, double2* __restrict__ Gb,
-                                                    int* __restrict__ flag) {
-  __shared__ double2 Dm[kBs][2 * kBs];
-  __shared__ double2 Gp[kBs][kBs];
-  __shared__ double2 fk[kBs];
-  __shared__ int s_piv;
-  __shared__ double s_dmax;
+// Block LU of one system by one warp: Delta_0 = B_0, Delta_i = B_i -
+// A_i G_{i-1}, P_i = Delta_i^-1, G_i = P_i C_i, and Q_i = P_i A_i, which
+// replaces A_i (the forward sweep is then y_i = P_i b_i - Q_i y_{i-1}: one
+// dependent product per block row).  The block products run over the 256
+// entries of a block in shared memory; the inverse is Gauss-Jordan with
+// partial pivoting on [Delta_i | I] held by columns in registers (lane c < 16
+// holds column c of Delta_i, lane 16 + c column c of the identity), a pivot
+// row being marked used rather than swapped, so that row perm[k] ends as row
+// k of the inverse.  A pivot below 1e-12 of the block's largest entry sets
+// flag[1]: the caller then uses the pivoted banded LU instead.
+__global__ void __launch_bounds__(32) k_blk_factor(int nseg, int NBq, const int* __restrict__ nblk,
+                                                   const int* __restrict__ blkoff, double2* __restrict__ Ab,
+                                                   const double2* __restrict__ Bb, const double2* __restrict__ Cb,
+                                                   double2* __restrict__ Pb, double2* __restrict__ Gb,
+                                                   int* __restrict__ flag) {
+  __shared__ double2 sA[kBs * kBs], sC[kBs * kBs], sP[kBs * kBs], sG[kBs * kBs], sD[kBs * kBs];
   const int q = blockIdx.x / nseg, sg = blockIdx.x % nseg;
   const int N = nblk[sg];
   const int64_t b0 = ((int64_t)q * NBq + blkoff[sg]) * (kBs * kBs);
-  const int tid = threadIdx.x;
-  const int r = tid / kBs, cc = tid % kBs;      // 256 threads: one per block entry
+  const int lane = threadIdx.x, c = lane & 15;
+  const bool left = lane < 16;
+  const double2 zero = make_double2(0.0, 0.0);
   for (int i = 0; i < N; ++i) {
     const int64_t o = b0 + (int64_t)i * kBs * kBs;
-    double2 v = Bb[o + tid];
-    if (i > 0) {
-      const double2* Ai = Ab + o + r * kBs;
-      for (int k = 0; k < kBs; ++k) v = csub(v, cmul(Ai[k], Gp[k][cc]));
+    for (int e = lane; e < kBs * kBs; e += 32) {
+      sA[e] = Ab[o + e];
+      sC[e] = (i + 1 < N) ? Cb[o + e] : zero;
     }
-    Dm[r][cc] = v;
-    Dm[r][kBs + cc] = make_double2(r == cc ? 1.0 : 0.0, 0.0);
-    __syncthreads();
-    if (tid < 32) {
-      double mx = 0.0;
-      for (int e = tid; e < kBs * kBs; e += 32) mx = fmax(mx, cabs1(Dm[e / kBs][e % kBs]));
-      for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (tid == 0) s_dmax = mx;
+    __syncwarp();
+    // Delta_i = B_i - A_i G_{i-1}
+    for (int e = lane; e < kBs * kBs; e += 32) {
+      const int rr = e / kBs, cc = e % kBs;
+      double2 d = Bb[o + e];
+      if (i > 0) {
+        double2 acc = zero;
+#pragma unroll
+        for (int k = 0; k < kBs; ++k) acc = cadd(acc, cmul(sA[rr * kBs + k], sG[k * kBs + cc]));
+        d = csub(d, acc);
+      }
+      sD[e] = d;
     }
-    __syncthreads();
+    __syncwarp();
+    double2 col[kBs];
+#pragma unroll
+    for (int rr = 0; rr < kBs; ++rr)
+      col[rr] = left ? sD[rr * kBs + c] : make_double2(rr == c ? 1.0 : 0.0, 0.0);
+    // largest entry of Delta_i (the small-pivot test)
+    double dmax = 0.0;
+    if (left)
+#pragma unroll
+      for (int rr = 0; rr < kBs; ++rr) dmax = fmax(dmax, cabs1(col[rr]));
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, s));
+    unsigned used = 0;
+    unsigned long long perm = 0;       // 4 bits per pivot step: the row it took
+#pragma unroll 1
     for (int k = 0; k < kBs; ++k) {
-      if (tid < 32) {
-        double best = -1.0;
-        int bi = k;
-        if (tid >= k && tid < kBs) { best = cabs1(Dm[tid][k]); bi = tid; }
-        for (int off = 16; off > 0; off >>= 1) {
-          const double ob = __shfl_xor_sync(0xffffffffu, best, off);
-          const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-          if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-        }
-        if (tid == 0) {
-          s_piv = bi;
-          if (!(best > 1e-12 * s_dmax)) atomicExch(flag + 1, 1);
-        }
+      // pivot of column k (lane k): the largest unused row, lowest index on ties
+      double best = -1.0;
+      int bp = 0;
+#pragma unroll
+      for (int rr = 0; rr < kBs; ++rr) {
+        const double v = cabs1(col[rr]);
+        if (!((used >> rr) & 1u) && v > best) { best = v; bp = rr; }
       }
-      __syncthreads();
-      const int p = s_piv;
-      if (p != k && tid < 2 * kBs) {
-        const double2 t = Dm[k][tid];
-        Dm[k][tid] = Dm[p][tid];
-        Dm[p][tid] = t;
+      const int p = __shfl_sync(0xffffffffu, bp, k);
+      const double bk = __shfl_sync(0xffffffffu, best, k);
+      if (lane == 0 && !(bk > 1e-12 * dmax)) atomicExch(flag + 1, 1);
+      double2 mine = zero;             // this lane's entry of the pivot row
+#pragma unroll
+      for (int rr = 0; rr < kBs; ++rr)
+        if (rr == p) mine = col[rr];
+      double2 pv;
+      pv.x = __shfl_sync(0xffffffffu, mine.x, k);
+      pv.y = __shfl_sync(0xffffffffu, mine.y, k);
+      const double2 rp = cabs1(pv) > 0.0 ? crcp(pv) : zero;
+      const double2 vp = cmul(mine, rp);
+#pragma unroll
+      for (int rr = 0; rr < kBs; ++rr) {
+        double2 m;
+        m.x = __shfl_sync(0xffffffffu, col[rr].x, k);
+        m.y = __shfl_sync(0xffffffffu, col[rr].y, k);
+        col[rr] = (rr == p) ? vp : csub(col[rr], cmul(m, vp));
       }
-      __syncthreads();
-      const double2 pv = Dm[k][k];
-      const double2 rp = cabs1(pv) > 0.0 ? crcp(pv) : make_double2(0.0, 0.0);
-      __syncthreads();
-      if (tid < 2 * kBs) Dm[k][tid] = cmul(Dm[k][tid], rp);
-      if (tid < kBs) fk[tid] = Dm[tid][k];
-      __syncthreads();
-      for (int e = tid; e < kBs * 2 * kBs; e += 256) {
-        const int rr = e / (2 * kBs), c2 = e % (2 * kBs);
-        if (rr != k) Dm[rr][c2] = csub(Dm[rr][c2], cmul(fk[rr], Dm[k][c2]));
+      used |= 1u << p;
+      perm |= (unsigned long long)p << (4 * k);
+    }
+    // P_i: row k of the inverse is row perm[k] of the right half
+    if (!left) {
+#pragma unroll 1
+      for (int k = 0; k < kBs; ++k) {
+        const int pk = (int)((perm >> (4 * k)) & 15u);
+        double2 v = zero;
+#pragma unroll
+        for (int rr = 0; rr < kBs; ++rr)
+          if (rr == pk) v = col[rr];
+        sP[k * kBs + c] = v;
+        Pb[o + k * kBs + c] = v;
       }
-      __syncthreads();
     }
-    Pb[o + tid] = Dm[r][kBs + cc];
-    if (i > 0) {
-      const double2* Ai = Ab + o;
-      double2 qv = make_double2(0.0, 0.0);
-      for (int k = 0; k < kBs; ++k) qv = cadd(qv, cmul(Dm[r][kBs + k], Ai[k * kBs + cc]));
-      __syncthreads();                            // every column of A_i read before it is replaced
-      Ab[o + tid] = qv;
+    __syncwarp();
+    // G_i = P_i C_i (kept for the next block row) and Q_i = P_i A_i
+    for (int e = lane; e < 2 * kBs * kBs; e += 32) {
+      const bool isg = e < kBs * kBs;
+      const int f = isg ? e : e - kBs * kBs;
+      const int rr = f / kBs, cc = f % kBs;
+      if (isg ? (i + 1 >= N) : (i == 0)) continue;
+      const double2* R = isg ? sC : sA;
+      double2 acc = zero;
+#pragma unroll
+      for (int k = 0; k < kBs; ++k) acc = cadd(acc, cmul(sP[rr * kBs + k], R[k * kBs + cc]));
+      if (isg) Gb[o + f] = acc;
+      else Ab[o + f] = acc;
+      if (isg) sD[f] = acc;            // staged; copied to sG below
     }
-    if (i + 1 < N) {
-      const double2* Ci = Cb + o;
-      double2 g = make_double2(0.0, 0.0);
-      for (int k = 0; k < kBs; ++k) g = cadd(g, cmul(Dm[r][kBs + k], Ci[k * kBs + cc]));
-      Gb[o + tid] = g;
-      __syncthreads();
-      Gp[r][cc] = g;
-    }
-    __syncthreads();
+    __syncwarp();
+    for (int e = lane; e < kBs * kBs; e += 32) sG[e] = sD[e];
+    __syncwarp();
   }
 }
 
@@ -581,13 +609,26 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
   const int64_t b0 = ((int64_t)q * NBq + blkoff[sg]) * (kBs * kBs);
   double2* x = rhs + (int64_t)q * 4 * lat + 4 * segstart[sg];
   const int lane = threadIdx.x;
-  const int r = lane >> 1, hh = lane & 1;
+  // lane = row r (0..15) + 16 * half hh: a quarter warp takes eight rows of
+  // one half, and the rotated column order below keeps its eight 16-byte
+  // reads of a 16 x 16 block in eight different bank groups
+  const int r = lane & 15, hh = lane >> 4;
   const double2 zero = make_double2(0.0, 0.0);
   if (lane == 0) {
     for (int k = 0; k < kBlkRing; ++k) mbar_init(&bar[k], 1);
     fence_mbar_init();
   }
-  for (int e = lane; e < kBs * N; e += 32) xs[e] = e < m ? x[e] : zero;
+  for (int e0 = lane; e0 < kBs * N; e0 += 8 * 32) {   // eight loads in flight
+    double2 tv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + 32 * u;
+      tv[u] = e < m ? x[e] : zero;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (e0 + 32 * u < kBs * N) xs[e0 + 32 * u] = tv[u];
+  }
   __syncwarp();
   // Blocks stream through a ring of kBlkRing slots, one bulk copy (4 KB) per
   // block on the slot's mbarrier; `issued` and `used` count blocks over all
@@ -612,13 +653,14 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
   };
   auto blk = [&](const double2* base, int i) { return base + b0 + (int64_t)i * kBs * kBs; };
   // 16-term complex dot product of row r with a 16-vector in shared memory
-  // (two lanes, eight terms each, two partial sums)
+  // (two lanes, eight terms each in a row-rotated order, two partial sums)
   auto rowdot = [&](const double2* M, const double2* v) {
     double2 a0 = zero, a1 = zero;
 #pragma unroll
     for (int k = 0; k < 8; k += 2) {
-      const double2 p0 = M[r * kBs + 8 * hh + k], y0 = v[8 * hh + k];
-      const double2 p1 = M[r * kBs + 8 * hh + k + 1], y1 = v[8 * hh + k + 1];
+      const int k0 = (k + r) & 7, k1 = (k + 1 + r) & 7;
+      const double2 p0 = M[r * kBs + 8 * hh + k0], y0 = v[8 * hh + k0];
+      const double2 p1 = M[r * kBs + 8 * hh + k1], y1 = v[8 * hh + k1];
       a0.x += p0.x * y0.x - p0.y * y0.y;
       a0.y += p0.x * y0.y + p0.y * y0.x;
       a1.x += p1.x * y1.x - p1.y * y1.y;
@@ -626,8 +668,8 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
     }
     a0.x += a1.x;
     a0.y += a1.y;
-    a0.x += __shfl_xor_sync(0xffffffffu, a0.x, 1);
-    a0.y += __shfl_xor_sync(0xffffffffu, a0.y, 1);
+    a0.x += __shfl_xor_sync(0xffffffffu, a0.x, 16);
+    a0.y += __shfl_xor_sync(0xffffffffu, a0.y, 16);
     return a0;
   };
   // t_i = P_i b_i for every block row (independent products)
@@ -992,8 +1034,8 @@ static int band_factor_that(Handle* h) {
   k_blk_pad<<<nq * B->nseg, 32, 0, h->stream>>>(nq, B->nseg, B->NBq, B->seglen_d, B->nblk_d, B->blkoff_d, B->Bb_d);
   C3D_LAUNCH_CHECK(h);
   C3D_CUDA_TRY(h, cudaMemsetAsync(B->flag_d, 0, 8, h->stream));
-  k_blk_factor<<<nq * B->nseg, 256, 0, h->stream>>>(B->nseg, B->NBq, B->nblk_d, B->blkoff_d, B->Ab_d, B->Bb_d,
-                                                    B->Cb_d, B->Pb_d, B->Gb_d, B->flag_d);
+  k_blk_factor<<<nq * B->nseg, 32, 0, h->stream>>>(B->nseg, B->NBq, B->nblk_d, B->blkoff_d, B->Ab_d, B->Bb_d,
+                                                   B->Cb_d, B->Pb_d, B->Gb_d, B->flag_d);
   C3D_LAUNCH_CHECK(h);
   int flag[2] = {0, 0};
   C3D_CUDA_TRY(h, cudaMemcpyAsync(flag, B->flag_d, 8, cudaMemcpyDeviceToHost, h->stream));
