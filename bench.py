@@ -312,7 +312,8 @@ def make_ib_channel(maxit, cfg="cfg2", tol=1e-10):
 def measure_ib(maxit=300, steps=2, modes=("none", "jacobi", "band", "learned"), cfgs=("cfg2",),
                band_maxit=600):
     """Schur BiCGSTAB of the IB projection at the 1e-10 tolerance for each
-    preconditioner: iterations and device ms per solve (3 solves per step),
+    preconditioner, after one untimed warm-up step (graph capture, first
+    preconditioner build): iterations and device ms per solve (3 solves per step),
     ms per iteration (two Schur applications), the residual reached, and for
     the band preconditioner its builds (probes of the Schur operator and the
     banded factorisations) in device ms."""
@@ -349,6 +350,7 @@ def measure_ib(maxit=300, steps=2, modes=("none", "jacobi", "band", "learned"), 
                     res["modes"][name] = learned_run(ch, run, steps)
                 else:
                     ch.set_mode(precond=mode_id[name])
+                    ch.compute_time_step_RK3(1)      # warm-up: graph capture, first builds
                     res["modes"][name] = run(ch, steps)
                     res["modes"][name]["cg_max_iter"] = cap
             except c3d.C3DError as e:
@@ -419,6 +421,7 @@ def learned_run(ch, run, steps):
     loss = ch.precond_train(epochs=400, lr=2e-3)
     t_train = time.perf_counter() - t0
     ch.set_mode(precond=L.PRECOND_LEARNED)
+    ch.compute_time_step_RK3(1)                  # warm-up: graph capture, buffers
     r = run(ch, steps)
     r.update({"train_loss": loss, "train_s": t_train, "probe_and_step_s": t_probe,
               "pairs": ch.precond_info()["pairs"]})

@@ -464,24 +464,47 @@ __global__ void __launch_bounds__(32) k_blk_factor(int nseg, int NBq, const int*
                                                    const double2* __restrict__ Bb, const double2* __restrict__ Cb,
                                                    double2* __restrict__ Pb, double2* __restrict__ Gb,
                                                    int* __restrict__ flag) {
-  __shared__ double2 sA[kBs * kBs], sC[kBs * kBs], sP[kBs * kBs], sG[kBs * kBs], sD[kBs * kBs];
+  // A_i, B_i, C_i of block row i arrive by bulk copies into buffer i & 1
+  // while block row i - 1 is factored
+  __shared__ __align__(128) double2 sIn[2][3][kBs * kBs];
+  __shared__ double2 sP[kBs * kBs], sG[kBs * kBs], sD[kBs * kBs];
+  __shared__ __align__(8) uint64_t bar[2];
   const int q = blockIdx.x / nseg, sg = blockIdx.x % nseg;
   const int N = nblk[sg];
   const int64_t b0 = ((int64_t)q * NBq + blkoff[sg]) * (kBs * kBs);
   const int lane = threadIdx.x, c = lane & 15;
   const bool left = lane < 16;
   const double2 zero = make_double2(0.0, 0.0);
+  constexpr unsigned kBlkBytes = kBs * kBs * sizeof(double2);
+  if (lane == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  auto fetch = [&](int i) {          // lane 0: block row i into buffer i & 1
+    const int64_t o = b0 + (int64_t)i * kBs * kBs;
+    uint64_t* b = &bar[i & 1];
+    fence_async_shared();
+    mbar_arrive_expect_tx(b, 3 * kBlkBytes);
+    bulk_load(sIn[i & 1][0], Ab + o, kBlkBytes, b);
+    bulk_load(sIn[i & 1][1], Bb + o, kBlkBytes, b);
+    bulk_load(sIn[i & 1][2], Cb + o, kBlkBytes, b);
+  };
+  if (lane == 0) fetch(0);
+  bool ok = true;
   for (int i = 0; i < N; ++i) {
     const int64_t o = b0 + (int64_t)i * kBs * kBs;
-    for (int e = lane; e < kBs * kBs; e += 32) {
-      sA[e] = Ab[o + e];
-      sC[e] = (i + 1 < N) ? Cb[o + e] : zero;
-    }
+    if (!mbar_wait(&bar[i & 1], (unsigned)(i >> 1) & 1u, kWaitCycles)) ok = false;
     __syncwarp();
+    if (lane == 0 && i + 1 < N) fetch(i + 1);
+    const double2* sA = sIn[i & 1][0];
+    const double2* sB = sIn[i & 1][1];
+    const double2* sC = sIn[i & 1][2];
     // Delta_i = B_i - A_i G_{i-1}
     for (int e = lane; e < kBs * kBs; e += 32) {
       const int rr = e / kBs, cc = e % kBs;
-      double2 d = Bb[o + e];
+      double2 d = sB[e];
       if (i > 0) {
         double2 acc = zero;
 #pragma unroll
@@ -568,6 +591,7 @@ __global__ void __launch_bounds__(32) k_blk_factor(int nseg, int NBq, const int*
     for (int e = lane; e < kBs * kBs; e += 32) sG[e] = sD[e];
     __syncwarp();
   }
+  if (!ok && lane == 0) atomicOr(flag + 3, 1);
 }
 
 // Block forward and back substitution of one system by one warp: lane 2r+h
