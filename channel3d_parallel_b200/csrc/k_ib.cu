@@ -640,11 +640,25 @@ __global__ void k_sp_sort(OpTables T, int c, int64_t npts, const int* __restrict
   const int n = cnt[p];
   if (n == 0) return;
   uint32_t* e = ent + off[p];
-  for (int a = 1; a < n; ++a) {
-    const uint32_t v = e[a];
-    int b = a - 1;
-    while (b >= 0 && e[b] > v) { e[b + 1] = e[b]; --b; }
-    e[b + 1] = v;
+  constexpr int kSortLocal = 64;
+  if (n <= kSortLocal) {
+    // a thread-local copy (registers / L1), sorted there, written back once
+    uint32_t t[kSortLocal];
+    for (int a = 0; a < n; ++a) t[a] = e[a];
+    for (int a = 1; a < n; ++a) {
+      const uint32_t v = t[a];
+      int b = a - 1;
+      while (b >= 0 && t[b] > v) { t[b + 1] = t[b]; --b; }
+      t[b + 1] = v;
+    }
+    for (int a = 0; a < n; ++a) e[a] = t[a];
+  } else {
+    for (int a = 1; a < n; ++a) {
+      const uint32_t v = e[a];
+      int b = a - 1;
+      while (b >= 0 && e[b] > v) { e[b + 1] = e[b]; --b; }
+      e[b + 1] = v;
+    }
   }
   double* wp = w + off[p];
   for (int a = 0; a < n; ++a) {
