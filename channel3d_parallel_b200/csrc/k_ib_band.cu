@@ -501,15 +501,19 @@ __global__ void __launch_bounds__(32) k_blk_factor(int nseg, int NBq, const int*
     const double2* sA = sIn[i & 1][0];
     const double2* sB = sIn[i & 1][1];
     const double2* sC = sIn[i & 1][2];
-    // Delta_i = B_i - A_i G_{i-1}
+    // Delta_i = B_i - A_i G_{i-1} (eight entries per lane, interleaved)
+#pragma unroll 4
     for (int e = lane; e < kBs * kBs; e += 32) {
       const int rr = e / kBs, cc = e % kBs;
       double2 d = sB[e];
       if (i > 0) {
-        double2 acc = zero;
+        double2 a0 = zero, a1 = zero;
 #pragma unroll
-        for (int k = 0; k < kBs; ++k) acc = cadd(acc, cmul(sA[rr * kBs + k], sG[k * kBs + cc]));
-        d = csub(d, acc);
+        for (int k = 0; k < kBs; k += 2) {
+          a0 = cadd(a0, cmul(sA[rr * kBs + k], sG[k * kBs + cc]));
+          a1 = cadd(a1, cmul(sA[rr * kBs + k + 1], sG[(k + 1) * kBs + cc]));
+        }
+        d = csub(d, cadd(a0, a1));
       }
       sD[e] = d;
     }
@@ -529,14 +533,22 @@ __global__ void __launch_bounds__(32) k_blk_factor(int nseg, int NBq, const int*
     unsigned long long perm = 0;       // 4 bits per pivot step: the row it took
 #pragma unroll 1
     for (int k = 0; k < kBs; ++k) {
-      // pivot of column k (lane k): the largest unused row, lowest index on ties
-      double best = -1.0;
-      int bp = 0;
+      // pivot of column k (lane k): the largest unused row, lowest index on
+      // ties, by a tournament over the 16 rows (depth 4)
+      double tv[kBs];
+      int ti[kBs];
 #pragma unroll
       for (int rr = 0; rr < kBs; ++rr) {
-        const double v = cabs1(col[rr]);
-        if (!((used >> rr) & 1u) && v > best) { best = v; bp = rr; }
+        tv[rr] = ((used >> rr) & 1u) ? -1.0 : cabs1(col[rr]);
+        ti[rr] = rr;
       }
+#pragma unroll
+      for (int w = 1; w < kBs; w *= 2)
+#pragma unroll
+        for (int rr = 0; rr < kBs; rr += 2 * w)
+          if (tv[rr + w] > tv[rr]) { tv[rr] = tv[rr + w]; ti[rr] = ti[rr + w]; }
+      const double best = tv[0];
+      const int bp = ti[0];
       const int p = __shfl_sync(0xffffffffu, bp, k);
       const double bk = __shfl_sync(0xffffffffu, best, k);
       if (lane == 0 && !(bk > 1e-12 * dmax)) atomicExch(flag + 1, 1);
@@ -574,15 +586,20 @@ __global__ void __launch_bounds__(32) k_blk_factor(int nseg, int NBq, const int*
     }
     __syncwarp();
     // G_i = P_i C_i (kept for the next block row) and Q_i = P_i A_i
+#pragma unroll 4
     for (int e = lane; e < 2 * kBs * kBs; e += 32) {
       const bool isg = e < kBs * kBs;
       const int f = isg ? e : e - kBs * kBs;
       const int rr = f / kBs, cc = f % kBs;
       if (isg ? (i + 1 >= N) : (i == 0)) continue;
       const double2* R = isg ? sC : sA;
-      double2 acc = zero;
+      double2 a0 = zero, a1 = zero;
 #pragma unroll
-      for (int k = 0; k < kBs; ++k) acc = cadd(acc, cmul(sP[rr * kBs + k], R[k * kBs + cc]));
+      for (int k = 0; k < kBs; k += 2) {
+        a0 = cadd(a0, cmul(sP[rr * kBs + k], R[k * kBs + cc]));
+        a1 = cadd(a1, cmul(sP[rr * kBs + k + 1], R[(k + 1) * kBs + cc]));
+      }
+      const double2 acc = cadd(a0, a1);
       if (isg) Gb[o + f] = acc;
       else Ab[o + f] = acc;
       if (isg) sD[f] = acc;            // staged; copied to sG below
