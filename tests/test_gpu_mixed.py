@@ -3,6 +3,9 @@ residual and one refinement projection) against the FP64 oracle.
 
 Bars (max-norm relative): before refinement 1e-6, after refinement 1e-10
 for U, V, W over 1 and 10 RK3 steps; max|div u| < 1e-12 after refinement.
+The pressure P after refinement within 1e-9 (the refined potential's
+residual error, one order above the velocity bar: P is not projected again),
+before refinement within 1e-5.
 """
 import math
 
@@ -55,6 +58,7 @@ def test_mixed_refined_matches_fp64_oracle(case, nsteps):
             co.compute_time_step_RK3(g, st, 1e-3)
         errs = {n: rel(ch.download(n), r[1:, 1:, 1:]) for n, r in (("U", st.U), ("V", st.V), ("W", st.W))}
         assert max(errs.values()) < 1e-10, errs
+        assert rel(ch.download("P"), st.P[1:, 1:, 1:]) < 1e-9
         assert ch.check_divergence() < 1e-12
         s = ch.stats()
         assert s["refinement_sweeps"] == 1
@@ -72,6 +76,7 @@ def test_mixed_unrefined_within_1e6(case):
         co.compute_time_step_RK3(g, st, 1e-3)
         errs = {n: rel(ch.download(n), r[1:, 1:, 1:]) for n, r in (("U", st.U), ("V", st.V), ("W", st.W))}
         assert max(errs.values()) < 1e-6, errs
+        assert rel(ch.download("P"), st.P[1:, 1:, 1:]) < 1e-5
         # and it is genuinely a lower-precision solve
         assert max(errs.values()) > 1e-12, errs
     finally:
