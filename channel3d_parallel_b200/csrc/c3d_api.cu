@@ -480,8 +480,7 @@ static int enqueue_step(Handle* h, double dt, double to) {
   // periodic, uniformly spaced x grid the bulk flux of d(phi)/dx telescopes
   // to zero, so the flux of the projected u is that of U* (up to rounding);
   // the stage-3 divergence kernel reduces it and the projection adds the shift.
-  const bool xflux = h->p.x_mass_cte == 1 && h->ib == nullptr && h->x_uniform &&
-                     h->poisson_mode == C3D_POISSON_FP64 && !h->write_pinterim;
+  const bool xflux = h->p.x_mass_cte == 1 && h->ib == nullptr && h->x_uniform && !h->write_pinterim;
   for (int s = 1; s <= 3; ++s) {
     const bool fx = xflux && s == 3;
     if ((rc = launch_rhs_stage(h, s, dt))) return rc;

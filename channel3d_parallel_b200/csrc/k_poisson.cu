@@ -1167,7 +1167,7 @@ static int set_limits(Handle* h, int smem_yz, int cs) {
   const int smx = xfft_smem<T>(d);
   C3D_CUDA_TRY(h, (raise_smem_limit<k_xfft_fwd<true, T>>(smx)));
   C3D_CUDA_TRY(h, (raise_smem_limit<k_xfft_fwd<false, T>>(smx)));
-  if (sizeof(T) == 8) C3D_CUDA_TRY(h, (raise_smem_limit<k_xfft_fwd<true, T, true>>(smx)));
+  C3D_CUDA_TRY(h, (raise_smem_limit<k_xfft_fwd<true, T, true>>(smx)));
   C3D_CUDA_TRY(h, (raise_smem_limit<k_xfft_inv<T>>(smx)));
   C3D_CUDA_TRY(h, (raise_smem_limit<k_spectral_yz<T, true>>(smem_yz)));
   C3D_CUDA_TRY(h, (raise_smem_limit<k_spectral_yz<T, false>>(smem_yz)));
@@ -1215,7 +1215,7 @@ static int run_spectral_t(Handle* h, bool from_div, const double* U, const doubl
     a.spec = spec; a.tw = twx; a.P = Px; a.pz = pz; a.rs = rsx; a.rbase = rbase; a.nlines = nlines;
     a.linesum = f32 ? S.linesum : nullptr;
     a.pos = S.posx;
-    if (flux_dt > 0.0 && !f32 && from_div && nlines == (int64_t)d.Ny * d.Nz) {
+    if (flux_dt > 0.0 && from_div && nlines == (int64_t)d.Ny * d.Nz) {
       // the x bulk flux of U reduced on the way (constant x mass flow)
       if (h->flux_part_len < (int64_t)nbx) {
         h->last_error = "x bulk-flux partials not allocated";
@@ -1492,9 +1492,11 @@ int launch_projection_step(Handle* h, int rk_step, double dt, const double* ushi
   int rc;
   double* phi = h->rhs_p;
   if (h->poisson_mode == C3D_POISSON_MIXED) {
+    // with ushift the first forward transform (of U*) also yields the x
+    // mass-flow correction: the flux of the refined projection is still U*'s
     const int sweeps = h->refine_sweeps;
     rc = run_spectral_t<float>(h, true, h->Us, h->Vs, h->Ws, nullptr, h->rhs_p,
-                               (stage1 && sweeps == 0) ? h->phi1 : nullptr, 0, 7);
+                               (stage1 && sweeps == 0) ? h->phi1 : nullptr, 0, 7, 0, -1, ushift ? dt : 0.0);
     if (rc) return rc;
     for (int sw = 1; sw <= sweeps; ++sw) {
       rc = launch_gradient_subtract(h, h->Us, h->Vs, h->Ws, h->rhs_p, dt, h->U, h->V, h->W, false, true);
