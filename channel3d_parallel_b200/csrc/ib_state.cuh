@@ -75,6 +75,10 @@ struct IbState {
   // BAND solves, and consecutive LEARNED solves that were slow against them
   double band_iters_ref = 0.0;
   int lrn_slow = 0;
+  // marker positions and dt when the network last predicted the band: like
+  // the probed band it is predicted again once a marker moved 0.03 dymin
+  std::vector<double> yb_at_lrn, xb_at_lrn;
+  double dt_at_lrn = 0.0;
   double* ext_part = nullptr;        // block partials of the extrapolation errors
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;   // Schur-solve timing
   // the BiCGSTAB iteration loop as a CUDA graph (a conditional WHILE node
@@ -99,6 +103,7 @@ struct IbState {
 // learned-preconditioner entry points used by the Schur solver (k_mlp.cu):
 // the band factors from the network's prediction at the current geometry,
 // and, while collection is on, a training set from each probed band
+bool learned_stale(Handle* h, double dt);
 int mlp_prepare_band(Handle* h);
 int mlp_build_band(Handle* h, double dt);
 bool mlp_collecting(const Handle* h);

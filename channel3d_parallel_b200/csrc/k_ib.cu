@@ -1365,7 +1365,6 @@ int ib_setup_operators(Handle* h) {
   C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   s->iy_lo = range[0];
   s->iy_hi = range[1];
-  s->have_lrn = false;
   return build_spread_maps(h);
 }
 
@@ -1742,6 +1741,19 @@ static int bcg_graph_ready(Handle* h, double* x, double dt, const double* blk, b
   return 0;
 }
 
+// the predicted band is redone when dt changed or a marker moved by more
+// than 0.03 dymin since the prediction (the probed band's rule)
+bool learned_stale(Handle* h, double dt) {
+  IbState* s = h->ib;
+  if (s->dt_at_lrn != dt || s->yb_at_lrn.size() != s->yb.size()) return true;
+  double mx = 0.0;
+  for (size_t k = 0; k < s->yb.size(); ++k) {
+    mx = std::max(mx, std::fabs(s->yb[k] - s->yb_at_lrn[k]));
+    mx = std::max(mx, std::fabs(s->xb[k] - s->xb_at_lrn[k]));
+  }
+  return mx > 0.03 * h->dymin;
+}
+
 void ib_rows(const Handle* h, int32_t rows[2]) {
   rows[0] = h->ib ? h->ib->iy_lo : 0;
   rows[1] = h->ib ? h->ib->iy_hi : 0;
@@ -1767,7 +1779,7 @@ int ib_bicgstab(Handle* h, const double* b, double dt) {
   // band factors: probed (BAND) when stale, or predicted by the network
   // (LEARNED) at every new geometry; timed as preconditioner builds
   const bool need_probe = mode == C3D_PRECOND_BAND && band_stale(h, dt);
-  const bool need_learn = mode == C3D_PRECOND_LEARNED && !s->have_lrn;
+  const bool need_learn = mode == C3D_PRECOND_LEARNED && (!s->have_lrn || learned_stale(h, dt));
   // allocations out of the timed build
   if (need_learn && (rc = mlp_prepare_band(h))) return rc;
   if (need_probe && !s->prb && (rc = dev_alloc(h, &s->prb, 16 * (int64_t)s->nb))) return rc;
@@ -2002,7 +2014,7 @@ int ib_precond_apply(Handle* h, const double* in, double* out, double dt) {
     return band_apply(h, in, out);
   }
   if (mode == C3D_PRECOND_LEARNED) {
-    if (!s->have_lrn && (rc = mlp_build_band(h, dt))) return rc;
+    if ((!s->have_lrn || learned_stale(h, dt)) && (rc = mlp_build_band(h, dt))) return rc;
     return band_apply(h, in, out);
   }
   if (mode == C3D_PRECOND_NONE) {
@@ -2106,7 +2118,6 @@ int ib_heaviside(Handle* h) {
   if ((rc = launch_fill_ghosts3(h, s->Hu, s->Hv, s->Hw))) return rc;              // :49
   if ((rc = gather_c(h, s->Hce, 1.0, s->E1nHc))) return rc;                       // :51
   if ((rc = gather3(h, G_E1N, s->Ut, s->Vt, s->Wt, s->E1nH))) return rc;          // :52
-  s->have_lrn = false;
   return 0;
 }
 

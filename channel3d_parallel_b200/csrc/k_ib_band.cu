@@ -1131,6 +1131,7 @@ int band_build(Handle* h, double dt) {
       B->probes++;
     }
   if ((rc = band_factor_from_T(h))) return rc;
+  s->have_lrn = false;                 // the factors in use are the probed band's now
   B->built = true;
   B->yb_at = s->yb;
   B->xb_at = s->xb;

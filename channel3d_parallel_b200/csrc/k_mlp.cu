@@ -848,6 +848,9 @@ int mlp_build_band(Handle* h, double dt) {
   if ((rc = check_mlp_err(h))) return rc;
   if ((rc = band_factor_symbol(h, dt))) return rc;
   s->have_lrn = true;
+  s->yb_at_lrn = s->yb;
+  s->xb_at_lrn = s->xb;
+  s->dt_at_lrn = dt;
   return 0;
 }
 
