@@ -325,6 +325,7 @@ def measure_ib(maxit=300, steps=2, modes=("none", "jacobi", "band", "learned"), 
     def run(ch, n):
         s0 = ch.stats()
         ch.compute_time_step_RK3(n)
+        step_ms = ch.last_step_time_ms()     # whole IB RK3 step, device timeline
         s1 = ch.stats()
         ns = s1["bicgstab_solves"] - s0["bicgstab_solves"]
         it = s1["bicgstab_iters"] - s0["bicgstab_iters"]
@@ -335,7 +336,8 @@ def measure_ib(maxit=300, steps=2, modes=("none", "jacobi", "band", "learned"), 
                 "total_ms_per_solve": (ms + bms) / ns, "iters_per_step": it / n,
                 "last_residual": s1["last_residual"], "converged": s1["last_residual"] < 1e-10,
                 "fallbacks": s1["precond_fallbacks"] - s0["precond_fallbacks"],
-                "max_div": ch.check_divergence(), "ib_rows": list(s1["ib_rows"])}
+                "max_div": ch.check_divergence(), "ib_rows": list(s1["ib_rows"]),
+                "ms_per_step": step_ms}
 
     out = {}
     for cfg in cfgs:

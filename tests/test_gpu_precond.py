@@ -68,20 +68,25 @@ def count_iters(case, mode, nsteps, warm=0):
         ch.close()
 
 
-@pytest.mark.parametrize("case,ratio", [("wall_standing_wave", 0.5), ("traveling_wave_x", None)])
-def test_learned_band_trains_and_beats_jacobi(case, ratio):
+@pytest.mark.parametrize("case,ratio,warm", [("wall_standing_wave", 0.5, 0), ("traveling_wave_x", None, 0)])
+def test_learned_band_trains_and_beats_jacobi(case, ratio, warm):
     """Training sets: the band probed at five geometries 2 steps apart (the
     solver's unit corrections and their Schur responses); then three steps
     with the network's band and the learned warm start, which must converge
-    to 1e-14 with no hand-over to the probed band where the geometries
-    repeat closely (the standing wave: at most half the Jacobi iterations),
-    and match the oracle."""
+    to 1e-14 and match the oracle; for the standing wave with no hand-over
+    to the probed band and at most half the Jacobi iterations.  The
+    travelling wave is trained during its 10-step amplitude ramp and run
+    after it (outside the training geometries; its test flow diverges after
+    about 13 steps in every preconditioner mode alike, so the run cannot
+    train after the ramp): reported, not asserted."""
     import channel3d_parallel_b200 as c3d
     L = c3d.lib
     p, g, st, ib, ch = build(case, cg_tol=TOL, cg_max_iter=600)
     dt = -p["cfl"]
     try:
         ch.set_mode(precond=L.PRECOND_BAND)
+        if warm:
+            ch.compute_time_step_RK3(warm)
         ch.precond_collect(True, max_sets=8)
         for _ in range(5):
             ch.precond_probe()
@@ -97,15 +102,15 @@ def test_learned_band_trains_and_beats_jacobi(case, ratio):
         s1 = ch.stats()
         it_lrn = iters_per_solve(s0, s1)
         assert s1["last_residual"] < TOL
-        for _ in range(13):
+        for _ in range(warm + 13):
             ibo.compute_time_step_RK3_ib(g, st, ib, dt)
         errs = {name: rel(ch.download(name), ref[1:, 1:, 1:])
                 for name, ref in (("U", st.U), ("V", st.V), ("W", st.W))}
         assert max(errs.values()) < 1e-10, errs
     finally:
         ch.close()
-    it_jac = count_iters(case, L.PRECOND_JACOBI, 3, warm=10)
-    it_band = count_iters(case, L.PRECOND_BAND, 3, warm=10)
+    it_jac = count_iters(case, L.PRECOND_JACOBI, 3, warm=warm + 10)
+    it_band = count_iters(case, L.PRECOND_BAND, 3, warm=warm + 10)
     print(f"{case}: iterations per solve jacobi {it_jac:.1f}, probed band {it_band:.1f}, "
           f"learned {it_lrn:.1f}, loss {loss:.4f}, hand-overs {s1['precond_fallbacks'] - s0['precond_fallbacks']}")
     if ratio is not None:
