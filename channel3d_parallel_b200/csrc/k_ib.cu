@@ -518,62 +518,175 @@ __device__ __forceinline__ int64_t lin(int n1, int n2, int i, int j, int k, int 
 
 // Gather of grid values to the markers, E (src/immersed_boundary_operators.f90
 // regT) and E1n (regT_1n, weights times the stencil point's offset along the
-// normal), with LANES threads per (marker, component): thread r of the group
-// walks the stencil rows (qj, qk) with qj + 5 qk = r, r+LANES, ... (25/LANES
-// rounds of five loads instead of 25), and the group adds its partial sums
-// by a fixed shuffle tree.  Rows of zero weight are skipped.
-constexpr int kGatherLanes = 8;
-template <int LANES>
-__global__ void __launch_bounds__(128) k_ib_gather8(GatherArgs a) {
-  constexpr int kGatherLanes = LANES;
+// normal), with the field box of a tile of markers staged in shared memory: a
+// CTA takes kTileMarkers consecutive markers of one component (one thread
+// each), finds the box of grid points their stencils touch (periodic x and z
+// indices unwrapped around the tile's first marker), copies that box from the
+// field once (consecutive threads along x, eight loads in flight) and gathers
+// from shared memory.  Per stencil row (qj, qk) the thread forms the row sums
+// s0 = sum_qi wx v and, for E1n, s1 = sum_qi wx ox v, and adds
+// scale wy wz (s1 + (oy + oz) s0) -- the regT / regT_1n sums
+// (src/immersed_boundary_operators.f90) regrouped by rows.  A stencil point of
+// zero weight reads a point inside the box and adds an exact zero.  A tile
+// whose box does not fit gathers from the field directly.
+constexpr int kTileMarkers = 64;
+constexpr int kTileBox = 3072;     // doubles of shared memory for the box (24 KB)
+template <bool E1N>
+__global__ void __launch_bounds__(kTileMarkers) k_ib_gather_tile(GatherArgs a) {
+  __shared__ double box[kTileBox];
+  __shared__ int s_ref[2], s_lo[3], s_hi[3];
   const int nb = a.T.nb;
-  const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int sub = (int)(gt & (kGatherLanes - 1));
-  const int64_t gid = gt / kGatherLanes;
-  const bool valid = gid < (int64_t)nb * a.ncomp;   // every lane joins the shuffles
-  const int c = valid ? (int)(gid / nb) : 0;
-  const int l = valid ? (int)(gid - (int64_t)c * nb) : 0;
+  const int c = blockIdx.y;
+  const int tid = threadIdx.x;
+  const int l = blockIdx.x * kTileMarkers + tid;
+  const bool valid = l < nb;
   const int t = a.type[c];
   const OpTables& T = a.T;
   const GField& g = a.f[c];
-  const bool e1n = a.mode == G_E1N;
-  double acc = 0.0;
-  if (valid) {
-    int ix[5];
-    double wx[5], ox[5];
-    double nx_ = 0.0, ny_ = 0.0, nz_ = 0.0;
-    if (e1n) { nx_ = T.nrm[l]; ny_ = T.nrm[nb + l]; nz_ = T.nrm[2 * nb + l]; }
+  const int px = a.d.Nx, pz = a.d.Nz;        // index periods of x and z (indices 2 .. N+1)
+  if (tid == 0) {
+    const int l0 = blockIdx.x * kTileMarkers;
+    s_ref[0] = T.idx[tslot(nb, t, 0, 2, l0)];
+    s_ref[1] = T.idx[tslot(nb, t, 2, 2, l0)];
+#pragma unroll
+    for (int a3 = 0; a3 < 3; ++a3) { s_lo[a3] = INT_MAX; s_hi[a3] = INT_MIN; }
+  }
+  __syncthreads();
+  const int rx = s_ref[0], rz = s_ref[1];
+  auto unwrap = [](int i, int r, int p) {
+    if (i - r > p / 2) return i - p;
+    if (r - i > p / 2) return i + p;
+    return i;
+  };
+  int ix[5], iy[5], iz[5];
+  double wx[5], wy[5], wz[5];
+  int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    ix[q] = iy[q] = iz[q] = 0;
+    wx[q] = wy[q] = wz[q] = 0.0;
+    if (valid) {
+      ix[q] = unwrap(T.idx[tslot(nb, t, 0, q, l)], rx, px);
+      iy[q] = T.idx[tslot(nb, t, 1, q, l)];
+      iz[q] = unwrap(T.idx[tslot(nb, t, 2, q, l)], rz, pz);
+      wx[q] = T.w1[tslot(nb, t, 0, q, l)];
+      wy[q] = T.w1[tslot(nb, t, 1, q, l)];
+      wz[q] = T.w1[tslot(nb, t, 2, q, l)];
+    }
+    if (wx[q] != 0.0) { lo[0] = min(lo[0], ix[q]); hi[0] = max(hi[0], ix[q]); }
+    if (wy[q] != 0.0) { lo[1] = min(lo[1], iy[q]); hi[1] = max(hi[1], iy[q]); }
+    if (wz[q] != 0.0) { lo[2] = min(lo[2], iz[q]); hi[2] = max(hi[2], iz[q]); }
+  }
+#pragma unroll
+  for (int a3 = 0; a3 < 3; ++a3) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[a3] = min(lo[a3], __shfl_xor_sync(0xffffffffu, lo[a3], o));
+      hi[a3] = max(hi[a3], __shfl_xor_sync(0xffffffffu, hi[a3], o));
+    }
+    if ((tid & 31) == 0) { atomicMin(&s_lo[a3], lo[a3]); atomicMax(&s_hi[a3], hi[a3]); }
+  }
+  __syncthreads();
+  const int bx0 = s_lo[0], by0 = s_lo[1], bz0 = s_lo[2];
+  const bool any = s_hi[0] >= bx0 && s_hi[1] >= by0 && s_hi[2] >= bz0;
+  const int bx = any ? s_hi[0] - bx0 + 1 : 0, by = any ? s_hi[1] - by0 + 1 : 0,
+            bz = any ? s_hi[2] - bz0 + 1 : 0;
+  const bool staged = any && (int64_t)bx * by * bz <= kTileBox;
+  auto field = [&](int i, int j, int k) {
+    const int ia = 2 + ((i - 2) % px + px) % px, ka = 2 + ((k - 2) % pz + pz) % pz;
+    return g.F[lin(g.n1, g.n2, ia, j, ka, g.rhsp)];
+  };
+  if (staged) {
+    const int vol = bx * by * bz;
+    for (int e0 = tid; e0 < vol; e0 += 8 * kTileMarkers) {
+      double tv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int e = e0 + u * kTileMarkers;
+        tv[u] = 0.0;
+        if (e < vol) {
+          const int r = e / bx;
+          tv[u] = field(bx0 + (e - r * bx), by0 + r % by, bz0 + r / by);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (e0 + u * kTileMarkers < vol) box[e0 + u * kTileMarkers] = tv[u];
+    }
+  }
+  __syncthreads();
+  if (!valid) return;
+  double ox[5], oy[5], oz[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) ox[q] = oy[q] = oz[q] = 0.0;
+  if (E1N) {
+    const double nx_ = T.nrm[l], ny_ = T.nrm[nb + l], nz_ = T.nrm[2 * nb + l];
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
-      ix[q] = T.idx[tslot(nb, t, 0, q, l)];
-      wx[q] = T.w1[tslot(nb, t, 0, q, l)];
-      ox[q] = e1n ? nx_ * T.off[tslot(nb, t, 0, q, l)] : 0.0;
+      ox[q] = nx_ * T.off[tslot(nb, t, 0, q, l)];
+      oy[q] = ny_ * T.off[tslot(nb, t, 1, q, l)];
+      oz[q] = nz_ * T.off[tslot(nb, t, 2, q, l)];
     }
-    for (int rr = sub; rr < 25; rr += kGatherLanes) {
-      const int qj = rr % 5, qk = rr / 5;
-      const double wy = T.w1[tslot(nb, t, 1, qj, l)], wz = T.w1[tslot(nb, t, 2, qk, l)];
-      if (wy == 0.0 || wz == 0.0) continue;            // the row adds exactly nothing
-      const int iy = T.idx[tslot(nb, t, 1, qj, l)], iz = T.idx[tslot(nb, t, 2, qk, l)];
-      const double wjk = T.scale * wy * wz;
-      const double oyz = e1n ? ny_ * T.off[tslot(nb, t, 1, qj, l)] + nz_ * T.off[tslot(nb, t, 2, qk, l)] : 0.0;
+  }
+  double acc = 0.0;
+  if (staged) {
+    int offx[5], offy[5], offz[5];
 #pragma unroll
-      for (int qi = 0; qi < 5; ++qi) {
-        const double v = g.F[lin(g.n1, g.n2, ix[qi], iy, iz, g.rhsp)] * g.mul;
-        double term = wjk * wx[qi] * v;
-        if (e1n) term *= ox[qi] + oyz;
-        acc += term;
+    for (int q = 0; q < 5; ++q) {        // zero-weight points read the box's first point
+      offx[q] = wx[q] != 0.0 ? ix[q] - bx0 : 0;
+      offy[q] = wy[q] != 0.0 ? bx * (iy[q] - by0) : 0;
+      offz[q] = wz[q] != 0.0 ? bx * by * (iz[q] - bz0) : 0;
+    }
+#pragma unroll
+    for (int qk = 0; qk < 5; ++qk) {
+#pragma unroll
+      for (int qj = 0; qj < 5; ++qj) {
+        const double* row = box + offy[qj] + offz[qk];
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int qi = 0; qi < 5; ++qi) {
+          const double wv = wx[qi] * row[offx[qi]];
+          s0 += wv;
+          if (E1N) s1 = fma(wv, ox[qi], s1);
+        }
+        const double wjk = T.scale * wy[qj] * wz[qk];
+        acc = fma(wjk, E1N ? fma(oy[qj] + oz[qk], s0, s1) : s0, acc);
       }
     }
-  }
+  } else {
+#pragma unroll 1
+    for (int r = 0; r < 25; ++r) {
+      const int qj = r % 5, qk = r / 5;
+      double wyq = 0.0, wzq = 0.0, oyz = 0.0;
+      int jy = 0, kz = 0;
 #pragma unroll
-  for (int o = kGatherLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if (valid && sub == 0) {
-    double r = a.sign * acc;
-    const int i = c * nb + l;
-    if (a.sub) r -= a.sub[i] * a.subv[i];
-    if (a.addv) r += a.addv[i];
-    a.out[i] = r;
+      for (int q = 0; q < 5; ++q) {
+        if (q == qj) { wyq = wy[q]; jy = iy[q]; oyz += oy[q]; }
+        if (q == qk) { wzq = wz[q]; kz = iz[q]; oyz += oz[q]; }
+      }
+      if (wyq == 0.0 || wzq == 0.0) continue;
+      double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+      for (int qi = 0; qi < 5; ++qi) {
+        if (wx[qi] == 0.0) continue;
+        const double wv = wx[qi] * field(ix[qi], jy, kz);
+        s0 += wv;
+        if (E1N) s1 = fma(wv, ox[qi], s1);
+      }
+      acc = fma(T.scale * wyq * wzq, E1N ? fma(oyz, s0, s1) : s0, acc);
+    }
   }
+  double r = a.sign * (acc * g.mul);
+  const int i = c * nb + l;
+  if (a.sub) r -= a.sub[i] * a.subv[i];
+  if (a.addv) r += a.addv[i];
+  a.out[i] = r;
+}
+
+static void launch_gather_tile(const GatherArgs& a, cudaStream_t st) {
+  const dim3 grid((a.T.nb + kTileMarkers - 1) / kTileMarkers, a.ncomp);
+  if (a.mode == G_E1N) k_ib_gather_tile<true><<<grid, kTileMarkers, 0, st>>>(a);
+  else k_ib_gather_tile<false><<<grid, kTileMarkers, 0, st>>>(a);
 }
 
 enum SpreadMode { S_RAW = 0, S_JUMP = 1, S_NORMAL = 2 };
@@ -1414,7 +1527,7 @@ static int gather3(Handle* h, int mode, const double* U, const double* V, const 
   a.f[0] = gf_u(h->d, U); a.f[1] = gf_v(h->d, V); a.f[2] = gf_w(h->d, W);
   a.type[0] = 0; a.type[1] = 1; a.type[2] = 2;
   a.ncomp = 3; a.mode = mode; a.out = out; a.sign = sign; a.sub = sub; a.subv = subv; a.addv = addv;
-  k_ib_gather8<kGatherLanes><<<thread_blocks(3 * kGatherLanes * (int64_t)h->ib->nb), 128, 0, h->stream>>>(a);
+  launch_gather_tile(a, h->stream);
   C3D_LAUNCH_CHECK(h);
   return 0;
 }
@@ -1425,7 +1538,7 @@ static int gather_c(Handle* h, const double* P, double mul, double* out, double 
   a.f[0] = GField{P, h->d.nxg - 2, h->d.nyg - 2, 1, mul};
   a.type[0] = 3;
   a.ncomp = 1; a.mode = G_E1N; a.out = out; a.sign = sign;
-  k_ib_gather8<kGatherLanes><<<thread_blocks(kGatherLanes * (int64_t)h->ib->nb), 128, 0, h->stream>>>(a);
+  launch_gather_tile(a, h->stream);
   C3D_LAUNCH_CHECK(h);
   return 0;
 }
