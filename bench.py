@@ -11,9 +11,12 @@ larger than L2, so no flush is needed between steps.
 
 value : steps/s from CUDA events on the library's stream around K steps
         (fields resident in HBM), max over ranks, summed over ranks (replicas).
-e2e   : the same metric through the C-ABI with host buffers: every step
-        uploads U, V, W from pinned host memory, advances one step and
-        downloads U, V, W.
+e2e   : the same metric through the C-ABI with the fields in pinned host
+        arrays (c3d_time_step_rk3_host): every step uploads U, V, W, advances
+        one step and downloads U, V, W into the same arrays; the download of
+        one step and the upload of the next overlap slab by slab.
+        e2e.blocking_calls_value: the same round trip as blocking
+        upload / step / download calls.
 --impl reference: the C++/OpenMP restatement of the reference's FP64 step
         (oracle/cpu_rk3.cpp; the Fortran/MPI/FFTW reference cannot be built
         on this host) with all host threads, one full RK3 step of the same
@@ -540,7 +543,10 @@ def run_ours(args):
         except Exception:
             traffic = None
 
-    # ---- end to end through the C-ABI with pinned host buffers
+    # ---- end to end through the C-ABI with pinned host buffers: the fields
+    # live in the caller's arrays and every step uploads U, V, W, advances one
+    # step and downloads them into the same arrays (c3d_time_step_rk3_host,
+    # whose slabbed copies let step n's download overlap step n+1's upload)
     pin = {}
     for name in ("U", "V", "W"):
         a = ch.download(name)
@@ -549,12 +555,17 @@ def run_ours(args):
         pin[name] = (t, t.numpy().reshape(a.shape, order="F"))
     nbytes = sum(v[1].nbytes for v in pin.values())
     e2e_steps = max(3, min(args.steps, 20))
-    for _ in range(2):
-        for name in ("U", "V", "W"):
-            ch.upload(name, pin[name][1])
-        ch.compute_time_step_RK3(1)
-        for name in ("U", "V", "W"):
-            ch.download(name)
+    hU, hV, hW = (pin[n][1] for n in ("U", "V", "W"))
+    ch.compute_time_step_RK3_host(hU, hV, hW, 2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ch.compute_time_step_RK3_host(hU, hV, hW, e2e_steps)
+    e2e_sec = (time.perf_counter() - t0) / e2e_steps
+    e2e_sec = max_over_ranks(e2e_sec, pg)
+    e2e_val = ws / e2e_sec
+    # the same round trip as one blocking call per copy and per step
+    # (upload U, V, W; one step; download U, V, W), without the overlap
+    from channel3d_parallel_b200 import lib as L
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
@@ -562,15 +573,9 @@ def run_ours(args):
             ch.upload(name, pin[name][1])
         ch.compute_time_step_RK3(1)
         for name in ("U", "V", "W"):
-            out = pin[name][1]
-            lb, ub = ch.bounds(name)
-            import ctypes
-            from channel3d_parallel_b200 import lib as L
-            cl, cu = L.box(lb, ub)
-            L.check(ch._lib.c3d_download(ch.handle, L.FIELD[name], L.dptr(out), cl, cu), ch.handle)
-    e2e_sec = (time.perf_counter() - t0) / e2e_steps
-    e2e_sec = max_over_ranks(e2e_sec, pg)
-    e2e_val = ws / e2e_sec
+            cl, cu = L.box(*ch.bounds(name))
+            L.check(ch._lib.c3d_download(ch.handle, L.FIELD[name], L.dptr(pin[name][1]), cl, cu), ch.handle)
+    e2e_sync_sec = max_over_ranks((time.perf_counter() - t0) / e2e_steps, pg)
 
     extras = {}
     if ws == 1 and not args.no_extras:
@@ -606,7 +611,8 @@ def run_ours(args):
         "kernel_ms": prof,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_val, "unit": "steps/s", "h2d_bytes_per_step": nbytes,
-                "d2h_bytes_per_step": nbytes},
+                "d2h_bytes_per_step": nbytes, "entry": "c3d_time_step_rk3_host",
+                "blocking_calls_value": ws / e2e_sync_sec},
         "gpu_launches": launches,
         "clocks": clk,
         "max_div": div,

@@ -170,6 +170,20 @@ class Channel:
         """compute_dt + compute_time_step_RK3 (src/time_integration.f90:86-267)."""
         return self._check(self._lib.c3d_time_step_rk3(self.handle, int(nsteps)))
 
+    def compute_time_step_RK3_host(self, U, V, W, nsteps=1):
+        """compute_time_step_RK3 with u, v, w kept in the caller's arrays
+        (app/main.f90:101-117): each step uploads U, V, W, advances one step
+        and writes them back in place.  The arrays must be float64,
+        Fortran-contiguous and of the full field extents; page-locked memory
+        (e.g. numpy views of pinned torch tensors) lets the copies overlap."""
+        for name, a in (("U", U), ("V", V), ("W", W)):
+            shape = self.bounds(name)[1]
+            if (not isinstance(a, np.ndarray) or a.dtype != np.float64 or a.shape != tuple(shape)
+                    or not a.flags.f_contiguous or not a.flags.writeable):
+                raise ValueError(f"{name} must be a writeable Fortran-ordered float64 array of shape {shape}")
+        return self._check(self._lib.c3d_time_step_rk3_host(self.handle, L.dptr(U), L.dptr(V), L.dptr(W),
+                                                            int(nsteps)))
+
     def compute_time_step_Euler(self, nsteps=1):
         """compute_dt + compute_time_step_Euler (src/time_integration.f90:25-81)."""
         return self._check(self._lib.c3d_time_step_euler(self.handle, int(nsteps)))

@@ -264,6 +264,13 @@ static void free_handle(Handle* h) {
   mixed_free(h);
   if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
   for (void* p : h->allocations) cudaFree(p);
+  if (h->h2d) cudaStreamSynchronize(h->h2d);
+  if (h->d2h) cudaStreamSynchronize(h->d2h);
+  for (cudaEvent_t e : h->ev_slab) cudaEventDestroy(e);
+  if (h->ev_up) cudaEventDestroy(h->ev_up);
+  if (h->ev_done) cudaEventDestroy(h->ev_done);
+  if (h->h2d) cudaStreamDestroy(h->h2d);
+  if (h->d2h) cudaStreamDestroy(h->d2h);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -582,6 +589,80 @@ static int run_steps(Handle* h, int nsteps, bool euler = false) {
 
 Handle* lookup_handle(int id) { return lookup(id); }
 
+// ---- stepping with u, v, w resident in host arrays -----------------------
+// Every step uploads the three arrays, advances one RK3 step and downloads
+// them back into the same arrays.  The copies go in slabs of kHostSlab bytes
+// on two copy streams: the upload of a slab for step n+1 waits only for the
+// download of that slab in step n, so one slab's download and the previous
+// slab's upload use the two directions of the host link at once.  The step
+// itself waits for all uploads, and the downloads for the step.
+constexpr size_t kHostSlab = size_t(4) << 20;
+
+static int host_copy_setup(Handle* h, size_t nslab) {
+  if (!h->h2d) C3D_CUDA_TRY(h, cudaStreamCreateWithFlags(&h->h2d, cudaStreamNonBlocking));
+  if (!h->d2h) C3D_CUDA_TRY(h, cudaStreamCreateWithFlags(&h->d2h, cudaStreamNonBlocking));
+  if (!h->ev_up) C3D_CUDA_TRY(h, cudaEventCreateWithFlags(&h->ev_up, cudaEventDisableTiming));
+  if (!h->ev_done) C3D_CUDA_TRY(h, cudaEventCreateWithFlags(&h->ev_done, cudaEventDisableTiming));
+  while (h->ev_slab.size() < nslab) {
+    cudaEvent_t e = nullptr;
+    C3D_CUDA_TRY(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    h->ev_slab.push_back(e);
+  }
+  return 0;
+}
+
+static int run_steps_host(Handle* h, double* const host[3], int nsteps) {
+  const int ids[3] = {C3D_FIELD_U, C3D_FIELD_V, C3D_FIELD_W};
+  double* dev[3];
+  size_t bytes[3], nsl[3], total = 0;
+  for (int a = 0; a < 3; ++a) {
+    FieldRef f{};
+    if (!field_ref(h, ids[a], f)) { h->last_error = "velocity field not allocated"; return C3D_ERR_PARAM; }
+    dev[a] = f.ptr;
+    bytes[a] = (size_t)(f.n[0] * f.n[1] * f.n[2]) * sizeof(double);
+    nsl[a] = (bytes[a] + kHostSlab - 1) / kHostSlab;
+    total += nsl[a];
+  }
+  int rc = host_copy_setup(h, total);
+  if (rc) return rc;
+  // the first uploads follow whatever the caller queued on the step stream
+  C3D_CUDA_TRY(h, cudaEventRecord(h->ev_done, h->stream));
+  C3D_CUDA_TRY(h, cudaStreamWaitEvent(h->h2d, h->ev_done, 0));
+  int warn = 0;
+  for (int n = 0; n < nsteps && rc >= 0; ++n) {
+    size_t e = 0;
+    for (int a = 0; a < 3; ++a)
+      for (size_t s = 0; s < nsl[a]; ++s) {
+        const size_t off = s * kHostSlab, len = std::min(kHostSlab, bytes[a] - off);
+        if (n > 0) C3D_CUDA_TRY(h, cudaStreamWaitEvent(h->h2d, h->ev_slab[e + s], 0));
+        C3D_CUDA_TRY(h, cudaMemcpyAsync(reinterpret_cast<char*>(dev[a]) + off,
+                                        reinterpret_cast<const char*>(host[a]) + off, len,
+                                        cudaMemcpyHostToDevice, h->h2d));
+      }
+    C3D_CUDA_TRY(h, cudaEventRecord(h->ev_up, h->h2d));
+    C3D_CUDA_TRY(h, cudaStreamWaitEvent(h->stream, h->ev_up, 0));
+    rc = run_steps(h, 1);
+    if (rc > 0) warn = rc;
+    if (rc < 0) break;
+    C3D_CUDA_TRY(h, cudaEventRecord(h->ev_done, h->stream));
+    C3D_CUDA_TRY(h, cudaStreamWaitEvent(h->d2h, h->ev_done, 0));
+    e = 0;
+    for (int a = 0; a < 3; ++a) {
+      for (size_t s = 0; s < nsl[a]; ++s) {
+        const size_t off = s * kHostSlab, len = std::min(kHostSlab, bytes[a] - off);
+        C3D_CUDA_TRY(h, cudaMemcpyAsync(reinterpret_cast<char*>(host[a]) + off,
+                                        reinterpret_cast<const char*>(dev[a]) + off, len,
+                                        cudaMemcpyDeviceToHost, h->d2h));
+        C3D_CUDA_TRY(h, cudaEventRecord(h->ev_slab[e + s], h->d2h));
+      }
+      e += nsl[a];
+    }
+  }
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->h2d));
+  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->d2h));
+  return rc < 0 ? rc : warn;
+}
+
 }  // namespace c3d
 
 using namespace c3d;
@@ -717,6 +798,13 @@ int c3d_time_step_rk3(int id, int nsteps) {
   GET_HANDLE(id);
   if (nsteps < 0) return C3D_ERR_PARAM;
   RET(h, run_steps(h, nsteps));
+}
+
+int c3d_time_step_rk3_host(int id, double* U, double* V, double* W, int nsteps) {
+  GET_HANDLE(id);
+  if (nsteps < 0 || !U || !V || !W) return C3D_ERR_PARAM;
+  double* const host[3] = {U, V, W};
+  RET(h, run_steps_host(h, host, nsteps));
 }
 
 int c3d_time_step_euler(int id, int nsteps) {

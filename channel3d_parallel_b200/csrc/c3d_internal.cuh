@@ -193,6 +193,10 @@ struct Handle {
   std::string last_error;
   int64_t launches = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // host-resident stepping: copy streams and per-slab download events
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t ev_up = nullptr, ev_done = nullptr;
+  std::vector<cudaEvent_t> ev_slab;
   double last_step_ms = 0;
   IbState* ib = nullptr;
   MixedState* mixed = nullptr;

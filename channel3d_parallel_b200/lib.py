@@ -67,6 +67,7 @@ PROTOTYPES = {
     "c3d_set_scalars": [_INT, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double],
     "c3d_synchronize": [_INT],
     "c3d_time_step_rk3": [_INT, _INT],
+    "c3d_time_step_rk3_host": [_INT, _D, _D, _D, _INT],
     "c3d_time_step_euler": [_INT, _INT],
     "c3d_write_snapshot": [_INT, C.c_char_p, _INT],
     "c3d_read_snapshot": [_INT, C.c_char_p],

@@ -13,13 +13,15 @@
  *    nothing calls exit().
  *  - Fields live in device memory owned by the library for the lifetime of
  *    the handle; they move to and from the host only through
- *    c3d_upload / c3d_download.  Host buffers are caller-owned, FP64,
+ *    c3d_upload / c3d_download (and, for U, V, W, c3d_time_step_rk3_host).
+ *    Host buffers are caller-owned, FP64,
  *    Fortran (column-major) order, and hold exactly the box lb..ub (inclusive,
  *    Fortran indices of the field, see C3D_FIELD_* below).
  *  - The domain is the reference's global array set for one z slab:
  *    nx = nx_global, ny = ny_global, nz = nz_global, nxg = nx+1, nyg = ny+1,
  *    nzg = nz+1 (src/initialization.f90:60-94 with nprocs = 1).
- *  - One host thread per handle; each handle owns one CUDA stream.
+ *  - One host thread per handle; each handle owns one CUDA stream for its
+ *    kernels (and two copy streams once c3d_time_step_rk3_host is used).
  */
 #ifndef C3D_H
 #define C3D_H
@@ -147,6 +149,14 @@ int c3d_synchronize(int handle);
 /* compute_time_step_RK3, src/time_integration.f90:86-213; nsteps steps, each
  * preceded by compute_dt (src/time_integration.f90:219-267).               */
 int c3d_time_step_rk3(int handle, int nsteps);
+/* compute_time_step_RK3 for a driver whose u, v, w stay in its own arrays, as
+ * the reference's time loop keeps them (app/main.f90:101-117): every one of
+ * the nsteps steps uploads U(nx,nyg,nzg), V(nxg,ny,nzg) and W(nxg,nyg,nz)
+ * (whole Fortran arrays, lower bounds 1), advances one step and writes the
+ * fields back into the same arrays.  With page-locked arrays the download of
+ * step n and the upload of step n+1 overlap slab by slab; returns when the
+ * last download has landed.                                                  */
+int c3d_time_step_rk3_host(int handle, double* U, double* V, double* W, int nsteps);
 /* compute_time_step_Euler, src/time_integration.f90:25-81 (explicit Euler,
  * non-IB projection, x and y constant-flux corrections); nsteps steps, each
  * preceded by compute_dt.                                                   */
