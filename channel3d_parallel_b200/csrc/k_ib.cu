@@ -496,19 +496,24 @@ struct GField {
 
 enum GatherMode { G_E = 0, G_E1N = 1 };
 
+// one component of a gather: its field, stencil table and epilogue
+// out[c*nb + l] = sign * gathered - sub[i] * subv[i] + addv[i], i = c*nb + l
+struct GComp {
+  GField f;
+  int type;           // table type: 0 u, 1 v, 2 w, 3 centre
+  int mode;           // G_E or G_E1N
+  double sign;
+  const double* sub;  // optional (with subv)
+  const double* subv;
+  const double* addv; // optional
+};
+
 struct GatherArgs {
   OpTables T;
   Dims d;
-  Metric m;
-  GField f[3];        // per component
-  int type[3];        // table type per component
+  GComp comp[4];      // blockIdx.y picks the component
   int ncomp;
-  int mode;
-  double* out;        // out[c*nb + l]
-  const double* sub;  // optional: out = gathered - sub_mul*sub[c*nb+l]*subv[c*nb+l]
-  const double* subv;
-  double sign;        // out = sign*gather + ...
-  const double* addv; // optional: out += addv[c*nb + l]
+  double* out;
 };
 
 __device__ __forceinline__ int64_t lin(int n1, int n2, int i, int j, int k, int rhsp) {
@@ -531,18 +536,18 @@ __device__ __forceinline__ int64_t lin(int n1, int n2, int i, int j, int k, int 
 // whose box does not fit gathers from the field directly.
 constexpr int kTileMarkers = 64;
 constexpr int kTileBox = 3072;     // doubles of shared memory for the box (24 KB)
+// Components of both variants may share one launch (the Schur operator's
+// E1n of phi beside the three E components); each CTA runs one variant.
 template <bool E1N>
-__global__ void __launch_bounds__(kTileMarkers) k_ib_gather_tile(GatherArgs a) {
-  __shared__ double box[kTileBox];
-  __shared__ int s_ref[2], s_lo[3], s_hi[3];
+__device__ __forceinline__ void gather_tile(const GatherArgs& a, const GComp& cp, int c, double* box,
+                                            int* s_ref, int* s_lo, int* s_hi) {
   const int nb = a.T.nb;
-  const int c = blockIdx.y;
   const int tid = threadIdx.x;
   const int l = blockIdx.x * kTileMarkers + tid;
   const bool valid = l < nb;
-  const int t = a.type[c];
+  const int t = cp.type;
   const OpTables& T = a.T;
-  const GField& g = a.f[c];
+  const GField& g = cp.f;
   const int px = a.d.Nx, pz = a.d.Nz;        // index periods of x and z (indices 2 .. N+1)
   if (tid == 0) {
     const int l0 = blockIdx.x * kTileMarkers;
@@ -591,27 +596,42 @@ __global__ void __launch_bounds__(kTileMarkers) k_ib_gather_tile(GatherArgs a) {
   const bool any = s_hi[0] >= bx0 && s_hi[1] >= by0 && s_hi[2] >= bz0;
   const int bx = any ? s_hi[0] - bx0 + 1 : 0, by = any ? s_hi[1] - by0 + 1 : 0,
             bz = any ? s_hi[2] - bz0 + 1 : 0;
-  const bool staged = any && (int64_t)bx * by * bz <= kTileBox;
-  auto field = [&](int i, int j, int k) {
-    const int ia = 2 + ((i - 2) % px + px) % px, ka = 2 + ((k - 2) % pz + pz) % pz;
-    return g.F[lin(g.n1, g.n2, ia, j, ka, g.rhsp)];
+  const bool staged = any && bx <= 2 * kTileMarkers && (int64_t)bx * by * bz <= kTileBox;
+  // periodic index back into 2 .. p+1 (one period away after the unwrap)
+  auto wrap = [](int i, int p) {
+    i = i < 2 ? i + p : (i > p + 1 ? i - p : i);
+    if (i < 2 || i > p + 1) i = 2 + ((i - 2) % p + p) % p;
+    return i;
   };
+  auto field = [&](int i, int j, int k) { return g.F[lin(g.n1, g.n2, wrap(i, px), j, wrap(k, pz), g.rhsp)]; };
   if (staged) {
-    const int vol = bx * by * bz;
-    for (int e0 = tid; e0 < vol; e0 += 8 * kTileMarkers) {
-      double tv[8];
+    // the box row by row (j fastest, then k), four rows per round with two
+    // x points per thread and row: eight loads in flight
+    const int nrow = by * bz;
+    const int xa = wrap(bx0 + tid, px), xb = wrap(bx0 + tid + kTileMarkers, px);
+    const bool ha = tid < bx, hb = tid + kTileMarkers < bx;
+    int jj = 0, kk = 0;
+    for (int r0 = 0; r0 < nrow; r0 += 4) {
+      double ta[4], tb[4];
+      int cj = jj, ck = kk;
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int e = e0 + u * kTileMarkers;
-        tv[u] = 0.0;
-        if (e < vol) {
-          const int r = e / bx;
-          tv[u] = field(bx0 + (e - r * bx), by0 + r % by, bz0 + r / by);
+      for (int u = 0; u < 4; ++u) {
+        ta[u] = tb[u] = 0.0;
+        if (r0 + u < nrow) {
+          const int j = by0 + cj, k = wrap(bz0 + ck, pz);
+          if (ha) ta[u] = g.F[lin(g.n1, g.n2, xa, j, k, g.rhsp)];
+          if (hb) tb[u] = g.F[lin(g.n1, g.n2, xb, j, k, g.rhsp)];
+        }
+        if (++cj == by) { cj = 0; ++ck; }
+      }
+      jj = cj; kk = ck;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (r0 + u < nrow) {
+          if (ha) box[tid + bx * (r0 + u)] = ta[u];
+          if (hb) box[tid + kTileMarkers + bx * (r0 + u)] = tb[u];
         }
       }
-#pragma unroll
-      for (int u = 0; u < 8; ++u)
-        if (e0 + u * kTileMarkers < vol) box[e0 + u * kTileMarkers] = tv[u];
     }
   }
   __syncthreads();
@@ -676,17 +696,25 @@ __global__ void __launch_bounds__(kTileMarkers) k_ib_gather_tile(GatherArgs a) {
       acc = fma(T.scale * wyq * wzq, E1N ? fma(oyz, s0, s1) : s0, acc);
     }
   }
-  double r = a.sign * (acc * g.mul);
+  double r = cp.sign * (acc * g.mul);
   const int i = c * nb + l;
-  if (a.sub) r -= a.sub[i] * a.subv[i];
-  if (a.addv) r += a.addv[i];
+  if (cp.sub) r -= cp.sub[i] * cp.subv[i];
+  if (cp.addv) r += cp.addv[i];
   a.out[i] = r;
+}
+
+__global__ void __launch_bounds__(kTileMarkers) k_ib_gather_tile(GatherArgs a) {
+  __shared__ double box[kTileBox];
+  __shared__ int s_ref[2], s_lo[3], s_hi[3];
+  const int c = blockIdx.y;
+  const GComp& cp = a.comp[c];
+  if (cp.mode == G_E1N) gather_tile<true>(a, cp, c, box, s_ref, s_lo, s_hi);
+  else gather_tile<false>(a, cp, c, box, s_ref, s_lo, s_hi);
 }
 
 static void launch_gather_tile(const GatherArgs& a, cudaStream_t st) {
   const dim3 grid((a.T.nb + kTileMarkers - 1) / kTileMarkers, a.ncomp);
-  if (a.mode == G_E1N) k_ib_gather_tile<true><<<grid, kTileMarkers, 0, st>>>(a);
-  else k_ib_gather_tile<false><<<grid, kTileMarkers, 0, st>>>(a);
+  k_ib_gather_tile<<<grid, kTileMarkers, 0, st>>>(a);
 }
 
 enum SpreadMode { S_RAW = 0, S_JUMP = 1, S_NORMAL = 2 };
@@ -1523,10 +1551,10 @@ static int gather3(Handle* h, int mode, const double* U, const double* V, const 
                    double sign = 1.0, const double* sub = nullptr, const double* subv = nullptr,
                    const double* addv = nullptr) {
   GatherArgs a{};
-  a.T = tables(h); a.d = h->d; a.m = h->m;
-  a.f[0] = gf_u(h->d, U); a.f[1] = gf_v(h->d, V); a.f[2] = gf_w(h->d, W);
-  a.type[0] = 0; a.type[1] = 1; a.type[2] = 2;
-  a.ncomp = 3; a.mode = mode; a.out = out; a.sign = sign; a.sub = sub; a.subv = subv; a.addv = addv;
+  a.T = tables(h); a.d = h->d;
+  const GField fs[3] = {gf_u(h->d, U), gf_v(h->d, V), gf_w(h->d, W)};
+  for (int c = 0; c < 3; ++c) a.comp[c] = GComp{fs[c], c, mode, sign, sub, subv, addv};
+  a.ncomp = 3; a.out = out;
   launch_gather_tile(a, h->stream);
   C3D_LAUNCH_CHECK(h);
   return 0;
@@ -1534,10 +1562,9 @@ static int gather3(Handle* h, int mode, const double* U, const double* V, const 
 
 static int gather_c(Handle* h, const double* P, double mul, double* out, double sign = 1.0) {
   GatherArgs a{};
-  a.T = tables(h); a.d = h->d; a.m = h->m;
-  a.f[0] = GField{P, h->d.nxg - 2, h->d.nyg - 2, 1, mul};
-  a.type[0] = 3;
-  a.ncomp = 1; a.mode = G_E1N; a.out = out; a.sign = sign;
+  a.T = tables(h); a.d = h->d;
+  a.comp[0] = GComp{GField{P, h->d.nxg - 2, h->d.nyg - 2, 1, mul}, 3, G_E1N, sign, nullptr, nullptr, nullptr};
+  a.ncomp = 1; a.out = out;
   launch_gather_tile(a, h->stream);
   C3D_LAUNCH_CHECK(h);
   return 0;
@@ -1683,17 +1710,24 @@ int ib_schur(Handle* h, const double* f, double* Sf, double dt) {
   const int jlo = s->iy_lo - 1, jhi = s->iy_hi + 1;
   if ((rc = reg_all_band(h, S_JUMP, f, dt, jlo - 1, jhi + 1))) return rc;
   if ((rc = launch_poisson_of_div_band(h, s->Ureg, s->Vreg, s->Wreg, h->rhs_p, jlo, jhi))) return rc;
-  // Sf(p) = -E1n_c(phi/dt); mean removal; -E1nHc_ext*p_jump        :123-126
-  if ((rc = gather_c(h, h->rhs_p, 1.0 / dt, Sf + 3 * nb, -1.0))) return rc;
-  if ((rc = remove_mean(h, Sf + 3 * nb, f + 3 * nb))) return rc;
   // Sf(u) = E(G phi - U_reg) - E1nH_ext*dudn                          :129-140
-  // (G phi - U_reg formed once on the stencil rows, then gathered)
+  // (G phi - U_reg formed once on the stencil rows, then gathered) and
+  // Sf(p) = -E1n_c(phi/dt), gathered in the same launch;
+  // then the mean removal and -E1nHc_ext*p_jump                       :123-126
   const Dims& d = h->d;
   const int64_t npts = (int64_t)d.Nx * (s->iy_hi - s->iy_lo + 1) * d.Nz;
   k_grad_minus_reg<<<(unsigned)std::min<int64_t>((npts + 255) / 256, 148 * 8), 256, 0, h->stream>>>(
       d, h->m, h->rhs_p, s->Ureg, s->Vreg, s->Wreg, s->Ut, s->Vt, s->Wt, s->iy_lo, s->iy_hi);
   C3D_LAUNCH_CHECK(h);
-  return gather3(h, G_E, s->Ut, s->Vt, s->Wt, Sf, 1.0, s->E1nH, f);
+  GatherArgs a{};
+  a.T = tables(h); a.d = d;
+  const GField fs[3] = {gf_u(d, s->Ut), gf_v(d, s->Vt), gf_w(d, s->Wt)};
+  for (int c = 0; c < 3; ++c) a.comp[c] = GComp{fs[c], c, G_E, 1.0, s->E1nH, f, nullptr};
+  a.comp[3] = GComp{GField{h->rhs_p, d.nxg - 2, d.nyg - 2, 1, 1.0 / dt}, 3, G_E1N, -1.0, nullptr, nullptr, nullptr};
+  a.ncomp = 4; a.out = Sf;
+  launch_gather_tile(a, h->stream);
+  C3D_LAUNCH_CHECK(h);
+  return remove_mean(h, Sf + 3 * nb, f + 3 * nb);
 }
 
 static int dot(Handle* h, const double* a, const double* b, const double* c, const double* e, int op,
