@@ -40,6 +40,7 @@
 #include "c3d_internal.cuh"
 #include "ib_state.cuh"
 #include "bulk.cuh"
+#include "fft.cuh"
 
 namespace c3d {
 
@@ -99,6 +100,11 @@ struct BandState {
   double2 *Pb_d = nullptr, *Gb_d = nullptr;                    // Delta^-1 and Delta^-1 C
   bool block = false;              // the factors in use are the block ones
   double* tw_d = nullptr;          // [2][nzl] cos, sin of 2 pi k / nzl
+  // z transforms by FFT when nzl = 2^a 3^b (else the direct DFTs)
+  bool fft = false;
+  FftPasses fftP{};
+  double2* ftw_d = nullptr;        // [nzl] exp(-2 pi i m / nzl)
+  int* fpos_d = nullptr;           // [nzl] digit-reversed position of coefficient m
   int* flag_d = nullptr;           // [0] zero pivot seen
   bool built = false;
   std::vector<double> yb_at, xb_at;
@@ -332,6 +338,100 @@ __global__ void __launch_bounds__(256) k_band_fwd(int nb, int lat, int nzl, int 
       im0 -= x0 * tws[k];
     }
     rhs[(int64_t)q * 4 * lat + row] = make_double2(re0 + re1, im0 + im1);
+  }
+}
+
+// The same two transforms with the shared-memory FFT engine (nzl = 2^a 3^b):
+// two real columns of one component share a complex row, z = a + i b, and a
+// CTA transforms kFftRows rows (2 kFftRows lattice columns).  Forward: the
+// half spectra A = (Z[q] + conj Z[N-q]) / 2 and B = (Z[q] - conj Z[N-q]) / 2i
+// are written to the block rows of the columns, as k_band_fwd writes them.
+// Inverse: Z[k] = A[k] + i B[k] on the whole circle from the Hermitian half
+// spectra (imaginary parts at q = 0 and q = N/2 dropped, the real part
+// k_band_inv takes), one inverse FFT, a = Re z / N and b = Im z / N.
+constexpr int kFftRows = 4;
+constexpr int kFftThreads = 64;
+static size_t fft_smem_bytes(int nzl) { return sizeof(double2) * kFftRows * (size_t)(nzl | 1); }
+
+__global__ void __launch_bounds__(kFftThreads) k_band_fwd_fft(int nb, int lat, int nzl, int nq, FftPasses P,
+                                                              const double2* __restrict__ tw,
+                                                              const int* __restrict__ fpos,
+                                                              const int* __restrict__ pos,
+                                                              const double* __restrict__ v,
+                                                              double2* __restrict__ rhs) {
+  extern __shared__ double2 zs[];   // [kFftRows][nzl | 1]
+  const int rs = nzl | 1;
+  const int c = blockIdx.y, m0 = blockIdx.x * 2 * kFftRows;
+  const int tid = threadIdx.x;
+  const int tot = 2 * kFftRows * nzl;   // e = iz * 2 kFftRows + column
+  for (int e0 = tid; e0 < tot; e0 += 8 * kFftThreads) {
+    double tv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + u * kFftThreads, iz = e / (2 * kFftRows), mm = e % (2 * kFftRows);
+      tv[u] = (e < tot && m0 + mm < lat) ? v[(int64_t)c * nb + m0 + mm + (int64_t)lat * iz] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + u * kFftThreads, iz = e / (2 * kFftRows), mm = e % (2 * kFftRows);
+      if (e < tot) reinterpret_cast<double*>(zs + (mm >> 1) * rs + iz)[mm & 1] = tv[u];
+    }
+  }
+  __syncthreads();
+  fft_rows_dif<double, 16>(zs, kFftRows, rs, tw, P);
+  for (int e = tid; e < kFftRows * nq; e += kFftThreads) {
+    const int r = e / nq, q = e - r * nq;
+    const double2 zq = zs[r * rs + fpos[q]];
+    const double2 zn = zs[r * rs + fpos[q == 0 ? 0 : nzl - q]];
+    const int ma = m0 + 2 * r, mb = ma + 1;
+    if (ma < lat) rhs[(int64_t)q * 4 * lat + 4 * pos[ma] + c] = make_double2(0.5 * (zq.x + zn.x), 0.5 * (zq.y - zn.y));
+    if (mb < lat) rhs[(int64_t)q * 4 * lat + 4 * pos[mb] + c] = make_double2(0.5 * (zq.y + zn.y), -0.5 * (zq.x - zn.x));
+  }
+}
+
+__global__ void __launch_bounds__(kFftThreads) k_band_inv_fft(int nb, int lat, int nzl, int nq, FftPasses P,
+                                                              const double2* __restrict__ tw,
+                                                              const int* __restrict__ fpos,
+                                                              const int* __restrict__ pos,
+                                                              const double2* __restrict__ rhs,
+                                                              double* __restrict__ v) {
+  extern __shared__ double2 zs[];   // [kFftRows][nzl | 1]
+  const int rs = nzl | 1;
+  const int c = blockIdx.y, m0 = blockIdx.x * 2 * kFftRows;
+  const int tid = threadIdx.x;
+  const double2 zero = make_double2(0.0, 0.0);
+  for (int e0 = tid; e0 < kFftRows * nq; e0 += 4 * kFftThreads) {
+    double2 A[4], B[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + u * kFftThreads;
+      A[u] = B[u] = zero;
+      if (e < kFftRows * nq) {
+        const int r = e / nq, q = e - r * nq;
+        const int ma = m0 + 2 * r, mb = ma + 1;
+        if (ma < lat) A[u] = rhs[(int64_t)q * 4 * lat + 4 * pos[ma] + c];
+        if (mb < lat) B[u] = rhs[(int64_t)q * 4 * lat + 4 * pos[mb] + c];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + u * kFftThreads;
+      if (e >= kFftRows * nq) break;
+      const int r = e / nq, q = e - r * nq;
+      const bool edge = q == 0 || 2 * q == nzl;
+      if (edge) { A[u].y = 0.0; B[u].y = 0.0; }
+      zs[r * rs + fpos[q]] = make_double2(A[u].x - B[u].y, A[u].y + B[u].x);
+      if (!edge) zs[r * rs + fpos[nzl - q]] = make_double2(A[u].x + B[u].y, -A[u].y + B[u].x);
+    }
+  }
+  __syncthreads();
+  fft_rows_dit_inv<double, 16>(zs, kFftRows, rs, tw, P);
+  const double inv = 1.0 / nzl;
+  const int tot = 2 * kFftRows * nzl;
+  for (int e = tid; e < tot; e += kFftThreads) {
+    const int iz = e / (2 * kFftRows), mm = e % (2 * kFftRows);
+    if (m0 + mm < lat)
+      v[(int64_t)c * nb + m0 + mm + (int64_t)lat * iz] = inv * reinterpret_cast<const double*>(zs + (mm >> 1) * rs + iz)[mm & 1];
   }
 }
 
@@ -1020,6 +1120,20 @@ static int band_setup(Handle* h) {
   if ((rc = dev_alloc(h, &B->Gb_d, nbe))) return rc;
   if ((rc = dev_alloc(h, &B->tw_d, 2 * (int64_t)nzl))) return rc;
   if ((rc = dev_alloc(h, &B->flag_d, 4))) return rc;
+  B->fft = make_fft_passes(nzl, B->fftP, 16) && fft_smem_bytes(nzl) <= 48 * 1024;
+  std::vector<double2> ftw;
+  std::vector<int> fpos;
+  if (B->fft) {
+    if ((rc = dev_alloc(h, &B->ftw_d, nzl))) return rc;
+    if ((rc = dev_alloc(h, &B->fpos_d, nzl))) return rc;
+    ftw.resize(nzl);
+    fpos.resize(nzl);
+    for (int m = 0; m < nzl; ++m) {
+      const long double a = -2.0L * 3.141592653589793238462643383279503L * (long double)m / (long double)nzl;
+      ftw[m] = make_double2((double)std::cos(a), (double)std::sin(a));
+      fpos[m] = dif_k_to_position(m, B->fftP);
+    }
+  }
   std::vector<double> tw(2 * (size_t)nzl);
   for (int k = 0; k < nzl; ++k) {
     const long double a = 2.0L * 3.141592653589793238462643383279503L * (long double)k / (long double)nzl;
@@ -1034,6 +1148,10 @@ static int band_setup(Handle* h) {
   C3D_CUDA_TRY(h, cudaMemcpyAsync(B->seglen_d, B->seg_len.data(), 4 * B->nseg, cudaMemcpyHostToDevice, st));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(B->colour_d, col.data(), 4 * col.size(), cudaMemcpyHostToDevice, st));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(B->tw_d, tw.data(), 8 * tw.size(), cudaMemcpyHostToDevice, st));
+  if (B->fft) {
+    C3D_CUDA_TRY(h, cudaMemcpyAsync(B->ftw_d, ftw.data(), sizeof(double2) * nzl, cudaMemcpyHostToDevice, st));
+    C3D_CUDA_TRY(h, cudaMemcpyAsync(B->fpos_d, fpos.data(), sizeof(int) * nzl, cudaMemcpyHostToDevice, st));
+  }
   C3D_CUDA_TRY(h, cudaMemcpyAsync(B->nblk_d, B->nblk.data(), 4 * B->nseg, cudaMemcpyHostToDevice, st));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(B->blkoff_d, B->blkoff.data(), 4 * B->nseg, cudaMemcpyHostToDevice, st));
   C3D_CUDA_TRY(h, cudaStreamSynchronize(st));
@@ -1166,8 +1284,13 @@ int band_apply(Handle* h, const double* in, double* out) {
   BandState* B = s->band;
   const int lat = B->lat, nzl = B->nzl, nq = B->nq, nb = s->nb;
   const unsigned nmc = (unsigned)((lat + 31) / 32);
-  k_band_fwd<<<dim3(nmc, 4, (unsigned)((nq + kFwdQ - 1) / kFwdQ)), 256, fwd_smem_bytes(nzl), h->stream>>>(
-      nb, lat, nzl, nq, B->tw_d, B->pos_d, in, B->rhs_d);
+  const unsigned nfc = (unsigned)((lat + 2 * kFftRows - 1) / (2 * kFftRows));
+  if (B->fft)
+    k_band_fwd_fft<<<dim3(nfc, 4), kFftThreads, fft_smem_bytes(nzl), h->stream>>>(
+        nb, lat, nzl, nq, B->fftP, B->ftw_d, B->fpos_d, B->pos_d, in, B->rhs_d);
+  else
+    k_band_fwd<<<dim3(nmc, 4, (unsigned)((nq + kFwdQ - 1) / kFwdQ)), 256, fwd_smem_bytes(nzl), h->stream>>>(
+        nb, lat, nzl, nq, B->tw_d, B->pos_d, in, B->rhs_d);
   C3D_LAUNCH_CHECK(h);
   if (B->block) {
     k_blk_solve<<<nq * B->nseg, 32, blk_solve_smem(B->nblk_max), h->stream>>>(
@@ -1179,8 +1302,12 @@ int band_apply(Handle* h, const double* in, double* out) {
                                                         B->ipiv_d, B->rhs_d);
   }
   C3D_LAUNCH_CHECK(h);
-  k_band_inv<<<dim3(nmc, 4, (unsigned)((nzl + kInvZ - 1) / kInvZ)), 256, inv_smem_bytes(nzl, nq), h->stream>>>(
-      nb, lat, nzl, nq, B->tw_d, B->pos_d, B->rhs_d, out);
+  if (B->fft)
+    k_band_inv_fft<<<dim3(nfc, 4), kFftThreads, fft_smem_bytes(nzl), h->stream>>>(
+        nb, lat, nzl, nq, B->fftP, B->ftw_d, B->fpos_d, B->pos_d, B->rhs_d, out);
+  else
+    k_band_inv<<<dim3(nmc, 4, (unsigned)((nzl + kInvZ - 1) / kInvZ)), 256, inv_smem_bytes(nzl, nq), h->stream>>>(
+        nb, lat, nzl, nq, B->tw_d, B->pos_d, B->rhs_d, out);
   C3D_LAUNCH_CHECK(h);
   return 0;
 }

@@ -65,9 +65,10 @@ def rel(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-def build(case, cg_tol=1e-12, cg_max_iter=200, x_mass_cte=1):
+def build(case, cg_tol=1e-12, cg_max_iter=200, x_mass_cte=1, extra=None):
     import channel3d_parallel_b200 as c3d
     kw = dict(CASES[case])
+    kw.update(extra or {})
     nx, ny, nz = kw.pop("nx_global"), kw.pop("ny_global"), kw.pop("nz_global")
     lx, lz = kw.pop("Lxp"), kw.pop("Lzp")
     gt, al = kw.pop("grid_type"), kw.pop("alpha_stretch")
