@@ -711,20 +711,29 @@ __global__ void __launch_bounds__(32) k_blk_factor(int nseg, int NBq, const int*
   if (!ok && lane == 0) atomicOr(flag + 3, 1);
 }
 
-// Block forward and back substitution of one system by one warp: lane 2r+h
-// forms half (8 terms) of row r's products; the blocks stream through a
-// shared-memory ring (cp.async, kBlkRing - 1 block rows ahead), and the
-// system's right-hand side sits in shared memory for the whole solve (no
-// global access inside the two sequential sweeps).
+// Block forward and back substitution of one system by one CTA of four
+// warps: thread (r, p) = (tid / 8, tid % 8) forms the terms of columns p and
+// p + 8 of row r of each 16 x 16 product (a quarter warp reads 128
+// consecutive bytes of a block row: no bank conflicts), eight threads add
+// them by shuffles, and one barrier per block row publishes the new 16-vector
+// (double-buffered).  The blocks stream through a shared-memory ring of bulk
+// copies (kBlkRing - 1 block rows ahead, issued by thread 0), and the
+// system's right-hand side and solution sit in shared memory for the whole
+// solve.
 constexpr int kBlkRing = 16;    // one 16x16 block per stage: 15 blocks (60 KB) in flight
+constexpr int kBlkThreads = 128;
 static size_t blk_solve_smem(int nmax) {
-  return sizeof(double2) * ((size_t)kBlkRing * kBs * kBs + (size_t)kBs * nmax);
+  return sizeof(double2) * ((size_t)kBlkRing * kBs * kBs + 2 * (size_t)kBs * nmax);
 }
-__global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, const int* __restrict__ segstart,
-                                                  const int* __restrict__ seglen, const int* __restrict__ nblk,
-                                                  const int* __restrict__ blkoff, const double2* __restrict__ Ab,
-                                                  const double2* __restrict__ Pb, const double2* __restrict__ Gb,
-                                                  double2* __restrict__ rhs, int* __restrict__ flag);
+__global__ void __launch_bounds__(kBlkThreads) k_blk_solve(int lat, int nseg, int NBq,
+                                                           const int* __restrict__ segstart,
+                                                           const int* __restrict__ seglen,
+                                                           const int* __restrict__ nblk,
+                                                           const int* __restrict__ blkoff,
+                                                           const double2* __restrict__ Ab,
+                                                           const double2* __restrict__ Pb,
+                                                           const double2* __restrict__ Gb,
+                                                           double2* __restrict__ rhs, int* __restrict__ flag);
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -734,57 +743,73 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-__global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, const int* __restrict__ segstart,
-                                                  const int* __restrict__ seglen, const int* __restrict__ nblk,
-                                                  const int* __restrict__ blkoff, const double2* __restrict__ Ab,
-                                                  const double2* __restrict__ Pb, const double2* __restrict__ Gb,
-                                                  double2* __restrict__ rhs, int* __restrict__ flag) {
+__global__ void __launch_bounds__(kBlkThreads) k_blk_solve(int lat, int nseg, int NBq,
+                                                           const int* __restrict__ segstart,
+                                                           const int* __restrict__ seglen,
+                                                           const int* __restrict__ nblk,
+                                                           const int* __restrict__ blkoff,
+                                                           const double2* __restrict__ Ab,
+                                                           const double2* __restrict__ Pb,
+                                                           const double2* __restrict__ Gb,
+                                                           double2* __restrict__ rhs, int* __restrict__ flag) {
   extern __shared__ __align__(128) double2 bs_smem[];
   double2 (*ring)[kBs * kBs] = reinterpret_cast<double2 (*)[kBs * kBs]>(bs_smem);
-  double2* xs = bs_smem + (size_t)kBlkRing * kBs * kBs;   // [kBs * N] right-hand side / solution
-  __shared__ double2 vv[kBs];
-  __shared__ __align__(8) uint64_t bar[kBlkRing];
   const int q = blockIdx.x / nseg, sg = blockIdx.x % nseg;
   const int N = nblk[sg];
   const int m = 4 * seglen[sg];
+  double2* xs = bs_smem + (size_t)kBlkRing * kBs * kBs;   // [kBs * N] right-hand side b
+  double2* ys = xs + (size_t)kBs * N;                     // [kBs * N] t, then y, then x
+  __shared__ double2 vv[2][kBs];
+  __shared__ __align__(8) uint64_t bar[kBlkRing];
   const int64_t b0 = ((int64_t)q * NBq + blkoff[sg]) * (kBs * kBs);
   double2* x = rhs + (int64_t)q * 4 * lat + 4 * segstart[sg];
-  const int lane = threadIdx.x;
-  // lane = row r (0..15) + 16 * half hh: a quarter warp takes eight rows of
-  // one half, and the rotated column order below keeps its eight 16-byte
-  // reads of a 16 x 16 block in eight different bank groups
-  const int r = lane & 15, hh = lane >> 4;
+  const int tid = threadIdx.x;
+  const int r = tid >> 3, pp = tid & 7;
   const double2 zero = make_double2(0.0, 0.0);
-  if (lane == 0) {
+  if (tid == 0) {
     for (int k = 0; k < kBlkRing; ++k) mbar_init(&bar[k], 1);
     fence_mbar_init();
   }
-  for (int e0 = lane; e0 < kBs * N; e0 += 8 * 32) {   // eight loads in flight
-    double2 tv[8];
+  for (int e0 = tid; e0 < kBs * N; e0 += 4 * kBlkThreads) {   // four loads in flight
+    double2 tv[4];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int e = e0 + 32 * u;
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + kBlkThreads * u;
       tv[u] = e < m ? x[e] : zero;
     }
 #pragma unroll
-    for (int u = 0; u < 8; ++u)
-      if (e0 + 32 * u < kBs * N) xs[e0 + 32 * u] = tv[u];
+    for (int u = 0; u < 4; ++u)
+      if (e0 + kBlkThreads * u < kBs * N) xs[e0 + kBlkThreads * u] = tv[u];
   }
-  __syncwarp();
-  // Blocks stream through a ring of kBlkRing slots, one bulk copy (4 KB) per
-  // block on the slot's mbarrier; `issued` and `used` count blocks over all
-  // three passes, so slot and phase follow from them.
-  unsigned issued = 0, used = 0;
+  __syncthreads();
+  // `used` counts the blocks consumed (uniform across the CTA); slot and
+  // phase follow from it.
+  unsigned used = 0;
   bool ok = true;
   constexpr unsigned kBlkBytes = kBs * kBs * sizeof(double2);
-  auto issue = [&](const double2* src) {
-    const unsigned slot = issued % kBlkRing;
-    if (lane == 0) {
-      fence_async_shared();            // this warp's reads of the slot come first
-      mbar_arrive_expect_tx(&bar[slot], kBlkBytes);
-      bulk_load(ring[slot], src, kBlkBytes, &bar[slot]);
+  auto blk = [&](const double2* base, int i) { return base + b0 + (int64_t)i * kBs * kBs; };
+  // The three passes consume one sequence of blocks, g = 0 .. 3N-3: P_0 ..
+  // P_{N-1}, then Q_1 .. Q_{N-1}, then G_{N-2} .. G_0; block g goes to slot
+  // g % kBlkRing.  The first kBlkRing are issued at g = 0, and at every
+  // g = 4, 8, ... the four blocks g+12 .. g+15, into the slots of g-4 .. g-1,
+  // which the barriers of their block rows have released (one proxy fence
+  // per group), so each pass's first blocks arrive during the previous one.
+  const int total = 3 * N - 2;
+  auto src = [&](int g) -> const double2* {
+    if (g < N) return blk(Pb, g);
+    if (g < 2 * N - 1) return blk(Ab, g - N + 1);
+    return blk(Gb, N - 2 - (g - (2 * N - 1)));
+  };
+  auto refill = [&](int g) {
+    const int lo = g == 0 ? 0 : g + kBlkRing - 4, hi = min(total, g + kBlkRing);
+    if (tid == 0 && lo < hi) {
+      fence_async_shared();            // the CTA's reads of the slots come first
+      for (int k = lo; k < hi; ++k) {
+        const unsigned slot = (unsigned)k % kBlkRing;
+        mbar_arrive_expect_tx(&bar[slot], kBlkBytes);
+        bulk_load(ring[slot], src(k), kBlkBytes, &bar[slot]);
+      }
     }
-    ++issued;
   };
   auto acquire = [&]() -> const double2* {
     const unsigned slot = used % kBlkRing;
@@ -792,72 +817,87 @@ __global__ void __launch_bounds__(32) k_blk_solve(int lat, int nseg, int NBq, co
     ++used;
     return ring[slot];
   };
-  auto blk = [&](const double2* base, int i) { return base + b0 + (int64_t)i * kBs * kBs; };
-  // 16-term complex dot product of row r with a 16-vector in shared memory
-  // (two lanes, eight terms each in a row-rotated order, two partial sums)
+  // row r of M times v: columns pp and pp + 8 here, the other six pairs in
+  // the seven neighbouring threads (shuffle sum over the group of eight)
   auto rowdot = [&](const double2* M, const double2* v) {
-    double2 a0 = zero, a1 = zero;
+    const double2 p0 = M[r * kBs + pp], y0 = v[pp];
+    const double2 p1 = M[r * kBs + pp + 8], y1 = v[pp + 8];
+    double2 a;
+    a.x = p0.x * y0.x - p0.y * y0.y;
+    a.y = p0.x * y0.y + p0.y * y0.x;
+    a.x = fma(p1.x, y1.x, fma(-p1.y, y1.y, a.x));
+    a.y = fma(p1.x, y1.y, fma(p1.y, y1.x, a.y));
 #pragma unroll
-    for (int k = 0; k < 8; k += 2) {
-      const int k0 = (k + r) & 7, k1 = (k + 1 + r) & 7;
-      const double2 p0 = M[r * kBs + 8 * hh + k0], y0 = v[8 * hh + k0];
-      const double2 p1 = M[r * kBs + 8 * hh + k1], y1 = v[8 * hh + k1];
-      a0.x += p0.x * y0.x - p0.y * y0.y;
-      a0.y += p0.x * y0.y + p0.y * y0.x;
-      a1.x += p1.x * y1.x - p1.y * y1.y;
-      a1.y += p1.x * y1.y + p1.y * y1.x;
+    for (int o = 1; o < 8; o <<= 1) {
+      a.x += __shfl_xor_sync(0xffffffffu, a.x, o);
+      a.y += __shfl_xor_sync(0xffffffffu, a.y, o);
     }
-    a0.x += a1.x;
-    a0.y += a1.y;
-    a0.x += __shfl_xor_sync(0xffffffffu, a0.x, 16);
-    a0.y += __shfl_xor_sync(0xffffffffu, a0.y, 16);
-    return a0;
+    return a;
   };
-  // t_i = P_i b_i for every block row (independent products)
-  for (int i = 0; i < N && i < kBlkRing - 1; ++i) issue(blk(Pb, i));
-  for (int i = 0; i < N; ++i) {
-    if (i + kBlkRing - 1 < N) issue(blk(Pb, i + kBlkRing - 1));
-    const double2* Pi = acquire();
-    const double2 t = rowdot(Pi, xs + kBs * i);
-    __syncwarp();
-    if (hh == 0) xs[kBs * i + r] = t;
-    __syncwarp();
+  // t_i = P_i b_i for every block row (independent products): four block
+  // rows per step, one per warp; lane (r2, hh) forms half (eight terms, in a
+  // row-rotated order) of row r2.  P_i is block g = i of the sequence.
+  {
+    const int warp = tid >> 5, lane = tid & 31, r2 = lane & 15, hh = lane >> 4;
+    for (int s4 = 0; s4 < N; s4 += 4) {
+      refill(s4);
+      const int i = s4 + warp;
+      if (i < N) {
+        if (!mbar_wait(&bar[i % kBlkRing], (unsigned)(i / kBlkRing) & 1u, kWaitCycles)) ok = false;
+        const double2* Pi = ring[i % kBlkRing];
+        const double2* v = xs + kBs * i;
+        double2 a0 = zero, a1 = zero;
+#pragma unroll
+        for (int k = 0; k < 8; k += 2) {
+          const int k0 = (k + r2) & 7, k1 = (k + 1 + r2) & 7;
+          const double2 p0 = Pi[r2 * kBs + 8 * hh + k0], y0 = v[8 * hh + k0];
+          const double2 p1 = Pi[r2 * kBs + 8 * hh + k1], y1 = v[8 * hh + k1];
+          a0.x += p0.x * y0.x - p0.y * y0.y;
+          a0.y += p0.x * y0.y + p0.y * y0.x;
+          a1.x += p1.x * y1.x - p1.y * y1.y;
+          a1.y += p1.x * y1.y + p1.y * y1.x;
+        }
+        a0.x += a1.x;
+        a0.y += a1.y;
+        a0.x += __shfl_xor_sync(0xffffffffu, a0.x, 16);
+        a0.y += __shfl_xor_sync(0xffffffffu, a0.y, 16);
+        if (hh == 0) ys[kBs * i + r2] = a0;
+      }
+      __syncthreads();
+    }
+    used = (unsigned)N;
   }
-  // forward: y_i = t_i - Q_i y_{i-1} (Q_i = P_i A_i, stored in place of A_i)
-  for (int i = 1; i < N && i < kBlkRing; ++i) issue(blk(Ab, i));
+  // forward: y_i = t_i - Q_i y_{i-1} (Q_i = P_i A_i, stored in place of A_i);
+  // vv[i & 1] carries y_i to the next block row
   for (int i = 0; i < N; ++i) {
-    if (i > 0 && i + kBlkRing - 1 < N) issue(blk(Ab, i + kBlkRing - 1));
+    if (i > 0 && ((N + i - 1) & 3) == 0) refill(N + i - 1);
     const int row = kBs * i + r;
-    double2 y = xs[row];
+    double2 y = ys[row];
     if (i > 0) {
       const double2* Qi = acquire();
-      y = csub(y, rowdot(Qi, vv));
+      y = csub(y, rowdot(Qi, vv[(i - 1) & 1]));
     }
-    __syncwarp();
-    if (hh == 0) {
-      vv[r] = y;
-      xs[row] = y;
+    if (pp == 0) {
+      vv[i & 1][r] = y;
+      ys[row] = y;
     }
-    __syncwarp();
+    __syncthreads();
   }
-  // backward: x_i = y_i - G_i x_{i+1}; vv holds x_{i+1}
-  for (int k = 0; k < kBlkRing - 1 && N - 2 - k >= 0; ++k) issue(blk(Gb, N - 2 - k));
+  // backward: x_i = y_i - G_i x_{i+1}; vv[(i + 1) & 1] holds x_{i+1}
   for (int i = N - 2; i >= 0; --i) {
-    if (i - (kBlkRing - 1) >= 0) issue(blk(Gb, i - (kBlkRing - 1)));
+    if (((3 * N - 3 - i) & 3) == 0) refill(3 * N - 3 - i);
     const double2* Gi = acquire();
-    const double2 a = rowdot(Gi, vv);
+    const double2 a = rowdot(Gi, vv[(i + 1) & 1]);
     const int row = kBs * i + r;
-    const double2 yv = xs[row];
-    __syncwarp();
-    if (hh == 0) {
-      const double2 xr = csub(yv, a);
-      vv[r] = xr;
-      xs[row] = xr;
+    if (pp == 0) {
+      const double2 xr = csub(ys[row], a);
+      vv[i & 1][r] = xr;
+      ys[row] = xr;
     }
-    __syncwarp();
+    __syncthreads();
   }
-  for (int e = lane; e < m; e += 32) x[e] = xs[e];
-  if (!ok && lane == 0) atomicOr(flag + 3, 1);
+  for (int e = tid; e < m; e += kBlkThreads) x[e] = ys[e];
+  if (!ok && tid == 0) atomicOr(flag + 3, 1);
 }
 
 // Forward and back substitution of one system (LAPACK zgbtrs, no transpose)
@@ -1293,7 +1333,7 @@ int band_apply(Handle* h, const double* in, double* out) {
         nb, lat, nzl, nq, B->tw_d, B->pos_d, in, B->rhs_d);
   C3D_LAUNCH_CHECK(h);
   if (B->block) {
-    k_blk_solve<<<nq * B->nseg, 32, blk_solve_smem(B->nblk_max), h->stream>>>(
+    k_blk_solve<<<nq * B->nseg, kBlkThreads, blk_solve_smem(B->nblk_max), h->stream>>>(
         lat, B->nseg, B->NBq, B->segstart_d, B->seglen_d, B->nblk_d, B->blkoff_d, B->Ab_d, B->Pb_d, B->Gb_d,
         B->rhs_d, B->flag_d);
   } else {
