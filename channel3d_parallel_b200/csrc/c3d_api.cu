@@ -747,6 +747,7 @@ int c3d_set_grid(int id, const double* x, const double* y, const double* z) {
   if (rc) RET(h, rc);
   if (h->step_exec) { cudaGraphExecDestroy(h->step_exec); h->step_exec = nullptr; }
   if (h->ib) {
+    ib_grids_changed(h);
     rc = ib_setup_geometry(h, h->t);
     if (!rc) rc = ib_setup_operators(h);
   }

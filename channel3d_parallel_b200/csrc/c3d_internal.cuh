@@ -315,6 +315,7 @@ void ib_free(Handle* h);
 void mlp_free(Handle* h);
 int ib_setup_geometry(Handle* h, double t);
 int ib_setup_operators(Handle* h);
+void ib_grids_changed(Handle* h);   // the next operator set-up re-uploads the grids
 int ib_heaviside(Handle* h);
 int ib_projection(Handle* h, double dt, int rk_step);
 int ib_regT(Handle* h, const double* U, const double* V, const double* W, double* Eu_dev);

@@ -23,8 +23,14 @@ struct IbState {
   double *xb_d = nullptr, *yb_d = nullptr, *zb_d = nullptr, *ub_d = nullptr, *nrm_d = nullptr, *sb_d = nullptr;
   int *yref_d = nullptr, *body_d = nullptr;
   double* binv_d = nullptr;          // 1/markers per body
+  // page-locked staging of the geometry uploads; stage_ev marks the end of
+  // the last upload from it
+  char* stage_h = nullptr;
+  size_t stage_bytes = 0;
+  cudaEvent_t stage_ev = nullptr;
   // 1-D grids (Fortran-indexed) for the weight kernel
   double *x_d = nullptr, *y_d = nullptr, *z_d = nullptr, *xm_d = nullptr, *ym_d = nullptr, *zm_d = nullptr;
+  bool grids_current = false;      // the device grids match the handle's (set_grid clears it)
   // operator tables: [type(4)][axis(3)][a(5)][nb]
   int* idx_d = nullptr;
   double* w1_d = nullptr;

@@ -35,13 +35,35 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
   const Params& p = h->p;
   const int nxb = p.nxb, nzb = p.nzb;
   const double Lxp = h->Lxp, Lzp = h->Lzp;
+  // every body type writes the same entries at every time, so the arrays
+  // are cleared only when their size changes
   auto resize = [&](int nb) {
-    s->nb = nb;
-    s->xb.assign(nb, 0); s->yb.assign(nb, 0); s->zb.assign(nb, 0);
-    s->ub.assign(3 * nb, 0); s->nrm.assign(3 * nb, 0); s->sb.assign(nb, 0);
-    s->tan1.assign(3 * nb, 0); s->tan2.assign(3 * nb, 0);
-    s->yref.assign(nb, 1); s->body.assign(nb, 0);
+    if (s->nb != nb || (int)s->xb.size() != nb) {
+      s->nb = nb;
+      s->xb.assign(nb, 0); s->yb.assign(nb, 0); s->zb.assign(nb, 0);
+      s->ub.assign(3 * nb, 0); s->nrm.assign(3 * nb, 0); s->sb.assign(nb, 0);
+      s->tan1.assign(3 * nb, 0); s->tan2.assign(3 * nb, 0);
+      s->yref.assign(nb, 1); s->body.assign(nb, 0);
+    }
     s->lat_nx = nb;
+  };
+  // Lattices whose markers differ from row to row only in z (every value
+  // but zb depends on the x index and the time): the first row is computed
+  // and copied to the others, zb set per row.
+  auto replicate_rows = [&](int rl, int nrows, double dzb) {
+    const int nb = s->nb;
+    for (int j = 2; j <= nrows; ++j) {
+      const int o = rl * (j - 1);
+      std::copy(s->xb.begin(), s->xb.begin() + rl, s->xb.begin() + o);
+      std::copy(s->yb.begin(), s->yb.begin() + rl, s->yb.begin() + o);
+      std::copy(s->sb.begin(), s->sb.begin() + rl, s->sb.begin() + o);
+      std::copy(s->yref.begin(), s->yref.begin() + rl, s->yref.begin() + o);
+      std::copy(s->body.begin(), s->body.begin() + rl, s->body.begin() + o);
+      for (int c = 0; c < 3; ++c)
+        for (std::vector<double>* v : {&s->ub, &s->nrm, &s->tan1, &s->tan2})
+          std::copy(v->begin() + (size_t)c * nb, v->begin() + (size_t)c * nb + rl, v->begin() + (size_t)c * nb + o);
+      for (int e = 0; e < rl; ++e) s->zb[o + e] = ((double)j - 0.5) * dzb;
+    }
   };
   if (s->kind == "center_wall") {                                     // :80-115
     if (p.grid_type != 0) { err = "Error: body type is incompatible with grid type"; return C3D_ERR_PARAM; }
@@ -77,7 +99,7 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
     const double dxb = Lxp / nxb, dzb = Lzp / nzb;
     const double A = p.body_param_1, om = p.body_param_2, b3 = p.body_param_3;
     const double y0 = two ? 0.0 : p.body_param_4;
-    for (int j = 1; j <= nzb; ++j)
+    for (int j = 1; j <= 1; ++j)   // the first row (replicate_rows copies it)
       for (int i = 1; i <= nxb; ++i) {
         const int k = i + nw * nxb * (j - 1) - 1;
         const double x = ((double)i - 0.5) * dxb;
@@ -94,7 +116,7 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
           s->body[k + nxb] = 1;
         }
       }
-    for (int j = 1; j <= nzb; ++j)
+    for (int j = 1; j <= 1; ++j)   // the first row (replicate_rows copies it)
       for (int i = 1; i <= nxb; ++i) {
         const int k = i + nw * nxb * (j - 1) - 1;
         const double phase = 2.0 * kPiIb * b3 * s->xb[k] / Lxp;
@@ -117,7 +139,7 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
           s->tan2[2 * nb + k + nxb] = 1.0;
         }
       }
-    for (int j = 1; j <= nzb; ++j)
+    for (int j = 1; j <= 1; ++j)   // the first row (replicate_rows copies it)
       for (int i = 1; i <= nxb; ++i) {
         const int k = i + nw * nxb * (j - 1) - 1;
         const int first = nw * nxb * (j - 1), last = nxb - 1 + nw * nxb * (j - 1);
@@ -137,6 +159,7 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
         s->sb[k] = dzb * (0.5 * a1 + 0.5 * a2);
         if (two) s->sb[k + nxb] = dzb * (0.5 * a1 + 0.5 * a2);
       }
+    replicate_rows(nw * nxb, nzb, dzb);
     s->nbodies = nw;
   } else if (s->kind == "traveling_wave_x") {                          // :271-390
     const int nb = 2 * nxb * nzb;
@@ -151,7 +174,7 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
       damp = b1 * 0.5 * (kPiIb / tr) * std::sin(kPiIb * tau);
     } else { amp = b1; damp = 0.0; }
     const double phi = kPiIb;
-    for (int j = 1; j <= nzb; ++j)
+    for (int j = 1; j <= 1; ++j)   // the first row (replicate_rows copies it)
       for (int i = 1; i <= nxb; ++i) {
         const int k = i + 2 * nxb * (j - 1) - 1;
         const double x = ((double)i - 0.5) * dxb;
@@ -173,7 +196,7 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
         s->tan1[nb + k] = tby; s->tan1[nb + k + nxb] = tty;
         s->tan2[2 * nb + k] = 1.0; s->tan2[2 * nb + k + nxb] = 1.0;
       }
-    for (int j = 1; j <= nzb; ++j)
+    for (int j = 1; j <= 1; ++j)   // the first row (replicate_rows copies it)
       for (int i = 1; i <= nxb; ++i)
         for (int wall = 0; wall < 2; ++wall) {
           const int k = i + wall * nxb + 2 * nxb * (j - 1) - 1;
@@ -193,6 +216,7 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
           }
           s->sb[k] = dzb * (0.5 * a1 + 0.5 * a2);
         }
+    replicate_rows(2 * nxb, nzb, dzb);
     s->nbodies = 2;
   } else if (s->kind == "double_cylinders_z") {                         // :117-174
     if (p.grid_type != 0) { err = "Error: body type is incompatible with grid type"; return C3D_ERR_PARAM; }
@@ -300,16 +324,20 @@ static int geometry_host(Handle* h, IbState* s, double t, std::string& err) {
       z ^= z >> 31;
       ph = 2.0 * kPiIb * (double)(z >> 11) * (1.0 / 9007199254740992.0);
     }
+    std::vector<double> psn(nxb * nzb), pcs(nxb * nzb);   // per plate: sin, cos(omega t + phi)
+    for (int e = 0; e < nxb * nzb; ++e) {
+      psn[e] = std::sin(om * t + phase[e]);
+      pcs[e] = std::cos(om * t + phase[e]);
+    }
     for (int pj = 1; pj <= nzb; ++pj)
       for (int m = 1; m <= mz; ++m)
         for (int pi = 1; pi <= nxb; ++pi)
           for (int kk = 1; kk <= my; ++kk) {
             const int ix = (pi - 1) * my + kk - 1, iz = (pj - 1) * mz + m - 1;
             const int k = ix + s->lat_nx * iz;
-            const double ph = phase[(pi - 1) + nxb * (pj - 1)];
             const double y0 = 3.0 * h->dymin;
             const double y = y0 + (kk - 1) * (hh - y0) / (my - 1), eta = y / hh;
-            const double sn = std::sin(om * t + ph), cs = std::cos(om * t + ph);
+            const double sn = psn[(pi - 1) + nxb * (pj - 1)], cs = pcs[(pi - 1) + nxb * (pj - 1)];
             s->xb[k] = (pi - 0.5) * pitchx + amp * eta * eta * sn;
             s->yb[k] = y;
             s->zb[k] = (pj - 0.5) * pitchz + ((double)m - 0.5 - 0.5 * mz) * (wz / mz);
@@ -1355,19 +1383,38 @@ static unsigned thread_blocks(int64_t n) { return (unsigned)((n + 127) / 128); }
 static int upload_geometry(Handle* h) {
   IbState* s = h->ib;
   cudaStream_t st = h->stream;
-  const int nb = s->nb;
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->xb_d, s->xb.data(), 8 * nb, cudaMemcpyHostToDevice, st));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->yb_d, s->yb.data(), 8 * nb, cudaMemcpyHostToDevice, st));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->zb_d, s->zb.data(), 8 * nb, cudaMemcpyHostToDevice, st));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->ub_d, s->ub.data(), 8 * 3 * nb, cudaMemcpyHostToDevice, st));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->nrm_d, s->nrm.data(), 8 * 3 * nb, cudaMemcpyHostToDevice, st));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->sb_d, s->sb.data(), 8 * nb, cudaMemcpyHostToDevice, st));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->yref_d, s->yref.data(), 4 * nb, cudaMemcpyHostToDevice, st));
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->body_d, s->body.data(), 4 * nb, cudaMemcpyHostToDevice, st));
+  const size_t nb = (size_t)s->nb;
   std::vector<double> binv(s->nbodies);
   for (int b = 0; b < s->nbodies; ++b) binv[b] = 1.0 / (double)s->body_count[b];
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->binv_d, binv.data(), 8 * s->nbodies, cudaMemcpyHostToDevice, st));
-  C3D_CUDA_TRY(h, cudaStreamSynchronize(st));   // host vectors may change before the next call
+  struct Part { void* dst; const void* src; size_t bytes; };
+  const Part parts[] = {
+      {s->xb_d, s->xb.data(), 8 * nb},          {s->yb_d, s->yb.data(), 8 * nb},
+      {s->zb_d, s->zb.data(), 8 * nb},          {s->ub_d, s->ub.data(), 24 * nb},
+      {s->nrm_d, s->nrm.data(), 24 * nb},       {s->sb_d, s->sb.data(), 8 * nb},
+      {s->yref_d, s->yref.data(), 4 * nb},      {s->body_d, s->body.data(), 4 * nb},
+      {s->binv_d, binv.data(), 8 * binv.size()}};
+  size_t total = 0;
+  for (const Part& q : parts) total += (q.bytes + 15) & ~size_t(15);
+  if (s->stage_bytes < total) {
+    if (s->stage_h) {
+      C3D_CUDA_TRY(h, cudaEventSynchronize(s->stage_ev));
+      cudaFreeHost(s->stage_h);
+      s->stage_h = nullptr;
+    }
+    C3D_CUDA_TRY(h, cudaMallocHost(reinterpret_cast<void**>(&s->stage_h), total));
+    s->stage_bytes = total;
+  }
+  if (!s->stage_ev) C3D_CUDA_TRY(h, cudaEventCreateWithFlags(&s->stage_ev, cudaEventDisableTiming));
+  else C3D_CUDA_TRY(h, cudaEventSynchronize(s->stage_ev));   // the last upload has left the staging
+  // the host vectors go to page-locked staging, and from there
+  // asynchronously to the device (the host may change them at once)
+  size_t o = 0;
+  for (const Part& q : parts) {
+    std::memcpy(s->stage_h + o, q.src, q.bytes);
+    C3D_CUDA_TRY(h, cudaMemcpyAsync(q.dst, s->stage_h + o, q.bytes, cudaMemcpyHostToDevice, st));
+    o += (q.bytes + 15) & ~size_t(15);
+  }
+  C3D_CUDA_TRY(h, cudaEventRecord(s->stage_ev, st));
   return 0;
 }
 
@@ -1381,7 +1428,12 @@ static int upload_grids(Handle* h) {
   C3D_CUDA_TRY(h, cudaMemcpyAsync(s->ym_d, h->ym.data(), 8 * h->ym.size(), cudaMemcpyHostToDevice, st));
   C3D_CUDA_TRY(h, cudaMemcpyAsync(s->zm_d, h->zm.data(), 8 * h->zm.size(), cudaMemcpyHostToDevice, st));
   C3D_CUDA_TRY(h, cudaStreamSynchronize(st));
+  s->grids_current = true;
   return 0;
+}
+
+void ib_grids_changed(Handle* h) {
+  if (h->ib) h->ib->grids_current = false;
 }
 
 int ib_create(Handle* h) {
@@ -1445,7 +1497,14 @@ int ib_create(Handle* h) {
 }
 
 void ib_free(Handle* h) {
-  if (h->ib) band_free(h->ib);
+  if (h->ib) {
+    band_free(h->ib);
+    if (h->ib->stage_ev) {
+      cudaEventSynchronize(h->ib->stage_ev);
+      cudaEventDestroy(h->ib->stage_ev);
+    }
+    if (h->ib->stage_h) cudaFreeHost(h->ib->stage_h);
+  }
   delete h->ib;
   h->ib = nullptr;
 }
@@ -1481,7 +1540,7 @@ int ib_setup_operators(Handle* h) {
   IbState* s = h->ib;
   if (!s) return C3D_ERR_UNSUPPORTED;
   if (s->x_d == nullptr) return 0;
-  int rc = upload_grids(h);
+  int rc = s->grids_current ? 0 : upload_grids(h);
   if (rc) return rc;
   IbGeomArgs a{};
   a.d = h->d; a.nb = s->nb;
@@ -1489,23 +1548,21 @@ int ib_setup_operators(Handle* h) {
   a.x = s->x_d; a.y = s->y_d; a.z = s->z_d; a.xm = s->xm_d; a.ym = s->ym_d; a.zm = s->zm_d;
   a.dx = h->dx; a.dz = h->dz; a.dymin = h->dymin; a.Lxp = h->Lxp; a.Lzp = h->Lzp;
   a.idx = s->idx_d; a.w1 = s->w1_d; a.off = s->off_d; a.flag = s->flag_d;
-  C3D_CUDA_TRY(h, cudaMemsetAsync(s->flag_d, 0, 4, h->stream));
+  // flag_d[0]: a stencil left the grid; flag_d[1..2]: the y rows the
+  // stencils touch (the Schur complement's spread field and the rows of its
+  // potential read by the gathers lie in [iy_lo - 1, iy_hi + 1]); one
+  // read-back for both
+  int fr[3] = {0, 1 << 30, -(1 << 30)};
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->flag_d, fr, sizeof(fr), cudaMemcpyHostToDevice, h->stream));
   k_ib_weights<<<(s->nb + 127) / 128, 128, 0, h->stream>>>(a);
   C3D_LAUNCH_CHECK(h);
-  int flag = 0;
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(&flag, s->flag_d, 4, cudaMemcpyDeviceToHost, h->stream));
-  C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  if (flag) { h->last_error = "Error: zi_supp out of range (marker stencil outside the grid)"; return C3D_ERR_PARAM; }
-  // y rows the stencils touch: the Schur complement's spread field and the
-  // rows of its potential read by the gathers lie in [iy_lo - 1, iy_hi + 1]
-  int range[2] = {1 << 30, -(1 << 30)};
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(s->flag_d + 1, range, 8, cudaMemcpyHostToDevice, h->stream));
   k_iy_range<<<std::min(148, (s->nb + 255) / 256), 256, 0, h->stream>>>(s->idx_d, s->nb, s->flag_d + 1);
   C3D_LAUNCH_CHECK(h);
-  C3D_CUDA_TRY(h, cudaMemcpyAsync(range, s->flag_d + 1, 8, cudaMemcpyDeviceToHost, h->stream));
+  C3D_CUDA_TRY(h, cudaMemcpyAsync(fr, s->flag_d, sizeof(fr), cudaMemcpyDeviceToHost, h->stream));
   C3D_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  s->iy_lo = range[0];
-  s->iy_hi = range[1];
+  if (fr[0]) { h->last_error = "Error: zi_supp out of range (marker stencil outside the grid)"; return C3D_ERR_PARAM; }
+  s->iy_lo = fr[1];
+  s->iy_hi = fr[2];
   return build_spread_maps(h);
 }
 
