@@ -1,7 +1,7 @@
 // Bulk asynchronous copies between global and shared memory (sm_90+ copy
 // engine, `cp.async.bulk`, no tensor map) completed on a shared-memory
 // mbarrier.  Loads use the `.shared::cluster` destination form with this
-// CTA's own shared address; none use cluster multicast.
+// CTA's own shared address; each copy goes to this one CTA only.
 //
 // Every wait is bounded: mbar_wait gives up after a number of SM clock
 // cycles and returns false, so a kernel can record an error and finish.
